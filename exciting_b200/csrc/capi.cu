@@ -1,0 +1,632 @@
+// C ABI of libexcfv (include/excfv.h): handle lifetime, per-SCF-iteration
+// data upload, workspace, and the drop-ins for match / hamiltonandoverlapsetup
+// / solvewithlapack / seceqnfv / seceqn.
+#include <cstdarg>
+#include <cstring>
+#include <vector>
+#include <chrono>
+
+#include "handle.cuh"
+
+int match_compute_zdinv(DevStatic& st, const double* d_sprwin, const double* d_apwfrwin,
+                        cudaStream_t s);
+int mirror_upper(cudaStream_t s, int n, cplx* M, long long ld);
+size_t tridiag_eig_scratch_doubles(int n, int k);
+int tridiag_workspace_doubles();
+int tridiag_nb();
+
+namespace {
+thread_local char g_err[512] = "";
+
+template <typename T>
+int dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    excfv_set_error("cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    *p = nullptr;
+    return EXCFV_ERR_ALLOC;
+  }
+  return EXCFV_OK;
+}
+
+template <typename T>
+int upload(T** p, const void* host, size_t count) {
+  int rc = dalloc(p, count);
+  if (rc) return rc;
+  if (host) {
+    cudaError_t e = cudaMemcpy(*p, host, count * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      excfv_set_error("upload: %s", cudaGetErrorString(e));
+      return EXCFV_ERR_CUDA;
+    }
+  } else {
+    cudaMemset(*p, 0, count * sizeof(T));
+  }
+  return EXCFV_OK;
+}
+
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+void excfv_set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+void free_static(DevStatic& st) {
+  dfree(st.idxis); dfree(st.rmt); dfree(st.apword); dfree(st.flist); dfree(st.fofl);
+  dfree(st.lo_atom); dfree(st.lo_local); dfree(st.lo_lm); dfree(st.lo_ilo);
+  dfree(st.aa); dfree(st.loa); dfree(st.lolo); dfree(st.oalo); dfree(st.ololo); dfree(st.h1aa);
+  dfree(st.ivg); dfree(st.ivgig); dfree(st.veffig); dfree(st.xig); dfree(st.cfunig);
+  dfree(st.m2effig); dfree(st.zdinv);
+}
+
+void free_workspace(Workspace& ws) {
+  dfree(ws.H); dfree(ws.O); dfree(ws.Ui); dfree(ws.T); dfree(ws.Apk); dfree(ws.Zpk);
+  dfree(ws.ylm); dfree(ws.djl); dfree(ws.apwalm); dfree(ws.igpig); dfree(ws.vgpc); dfree(ws.gpc);
+  dfree(ws.tpgpc); dfree(ws.sfacgp); dfree(ws.gk_iv); dfree(ws.d); dfree(ws.e); dfree(ws.tau);
+  dfree(ws.Wp); dfree(ws.red); dfree(ws.w); dfree(ws.stein_ws); dfree(ws.icl); dfree(ws.ybuf);
+  dfree(ws.Z); dfree(ws.Z2); dfree(ws.Gk); dfree(ws.Gki); dfree(ws.Tf); dfree(ws.Xs);
+  dfree(ws.status); dfree(ws.bar);
+  ws.nmatmax = ws.ngkmax = ws.kmax = 0;
+}
+
+int stage_set_static(excfv_handle* h, const excfv_static* s) {
+  DevStatic& st = h->st;
+  free_static(st);
+  h->have_static = false;
+  if (!s || s->natmtot <= 0 || s->nspecies <= 0 || s->lmaxapw < 0 || s->apwordmax <= 0 ||
+      s->maxaa <= 0 || s->ngvec <= 0 || s->ngrtot < s->ngvec || s->nstfv <= 0 || !s->idxis ||
+      !s->rmt || !s->apword || !s->aa || !s->ivg || !s->ivgig || !s->veffig || !s->cfunig ||
+      !s->sprwin || !s->apwfrwin || s->npmatch <= 0) {
+    excfv_set_error("excfv_set_static: missing or inconsistent arguments");
+    return EXCFV_ERR_ARG;
+  }
+  if (s->lmaxmat > s->lmaxapw) {
+    excfv_set_error("excfv_set_static: lmaxmat > lmaxapw");
+    return EXCFV_ERR_ARG;
+  }
+  st.natmtot = s->natmtot; st.nspecies = s->nspecies; st.lmaxapw = s->lmaxapw;
+  st.lmaxmat = s->lmaxmat; st.lmmaxapw = (s->lmaxapw + 1) * (s->lmaxapw + 1);
+  st.apwordmax = s->apwordmax; st.nlomax = s->nlomax; st.lolmmax = (s->lolmax + 1) * (s->lolmax + 1);
+  st.nlotot = s->nlotot; st.maxaa = s->maxaa; st.maxnlo = s->maxnlo; st.ngvec = s->ngvec;
+  st.ngrtot = s->ngrtot; st.h1on = s->h1on; st.vrel = s->valence_relativity;
+  st.npmatch = s->npmatch; st.omega = s->omega; st.nstfv = s->nstfv; st.evaltol = s->evaltol;
+  for (int i = 0; i < 6; ++i) st.intgv[i] = s->intgv[i];
+  const int na = st.natmtot, ns = st.nspecies;
+  int rc;
+  // species (0-based)
+  std::vector<int> idxis(na);
+  for (int a = 0; a < na; ++a) {
+    idxis[a] = s->idxis[a] - 1;
+    if (idxis[a] < 0 || idxis[a] >= ns) {
+      excfv_set_error("excfv_set_static: idxis out of range");
+      return EXCFV_ERR_ARG;
+    }
+  }
+  // packed APW function list per species (hamiltonsetup.f90:62-71)
+  const int L1 = st.lmaxapw + 1;
+  std::vector<int> flist((size_t)st.maxaa * ns, -1), fofl((size_t)st.lmmaxapw * st.apwordmax * ns, -1);
+  for (int is = 0; is < ns; ++is) {
+    int f = 0;
+    for (int l = 0; l <= st.lmaxmat; ++l)
+      for (int m = -l; m <= l; ++m) {
+        const int lm = l * (l + 1) + m;
+        const int nap = s->apword[l + L1 * is];
+        if (nap > st.apwordmax || nap < 0) {
+          excfv_set_error("excfv_set_static: apword > apwordmax");
+          return EXCFV_ERR_ARG;
+        }
+        for (int io = 0; io < nap; ++io) {
+          if (f >= st.maxaa) {
+            excfv_set_error("excfv_set_static: maxaa too small for apword/lmaxmat");
+            return EXCFV_ERR_ARG;
+          }
+          flist[f + (size_t)st.maxaa * is] = lm * st.apwordmax + io;
+          fofl[(lm * st.apwordmax + io) + (size_t)st.lmmaxapw * st.apwordmax * is] = f;
+          ++f;
+        }
+      }
+  }
+  // local-orbital maps (genidxlo.f90:32-44)
+  std::vector<int> lo_atom(std::max(1, st.nlotot), -1), lo_local(std::max(1, st.nlotot), -1);
+  std::vector<int> lo_lm((size_t)std::max(1, st.maxnlo) * na, -1), lo_ilo((size_t)std::max(1, st.maxnlo) * na, -1);
+  if (st.nlotot > 0) {
+    if (!s->nlorb || !s->lorbl || !s->idxlo || !s->losize || !s->loa || !s->lolo || !s->oalo ||
+        !s->ololo) {
+      excfv_set_error("excfv_set_static: local-orbital arrays missing");
+      return EXCFV_ERR_ARG;
+    }
+    for (int a = 0; a < na; ++a) {
+      const int is = idxis[a];
+      int first = -1;
+      for (int ilo = 0; ilo < s->nlorb[is]; ++ilo) {
+        const int l = s->lorbl[ilo + st.nlomax * is];
+        for (int m = -l; m <= l; ++m) {
+          const int lm = l * (l + 1) + m;
+          const int g = s->idxlo[lm + st.lolmmax * (ilo + (size_t)st.nlomax * a)] - 1;
+          if (g < 0 || g >= st.nlotot) {
+            excfv_set_error("excfv_set_static: idxlo out of range");
+            return EXCFV_ERR_ARG;
+          }
+          if (first < 0 || g < first) first = g;
+        }
+      }
+      for (int ilo = 0; ilo < s->nlorb[is]; ++ilo) {
+        const int l = s->lorbl[ilo + st.nlomax * is];
+        for (int m = -l; m <= l; ++m) {
+          const int lm = l * (l + 1) + m;
+          const int g = s->idxlo[lm + st.lolmmax * (ilo + (size_t)st.nlomax * a)] - 1;
+          const int jj = g - first;
+          if (jj >= st.maxnlo) {
+            excfv_set_error("excfv_set_static: LO block larger than maxnlo");
+            return EXCFV_ERR_ARG;
+          }
+          lo_atom[g] = a;
+          lo_local[g] = jj;
+          lo_lm[jj + (size_t)st.maxnlo * a] = lm;
+          lo_ilo[jj + (size_t)st.maxnlo * a] = ilo;
+        }
+      }
+    }
+    for (int g = 0; g < st.nlotot; ++g)
+      if (lo_atom[g] < 0) {
+        excfv_set_error("excfv_set_static: idxlo does not cover 1..nlotot");
+        return EXCFV_ERR_ARG;
+      }
+  }
+  // overlap radial integrals with the IORA* terms folded in
+  const size_t noalo = (size_t)st.apwordmax * std::max(1, st.nlomax) * na;
+  const size_t nololo = (size_t)std::max(1, st.nlomax) * std::max(1, st.nlomax) * na;
+  std::vector<double> oalo(noalo, 0.0), ololo(nololo, 0.0);
+  if (st.nlotot > 0) {
+    for (size_t i = 0; i < noalo; ++i) oalo[i] = s->oalo[i] + (s->h1loa ? s->h1loa[i] : 0.0);
+    for (size_t i = 0; i < nololo; ++i) ololo[i] = s->ololo[i] + (s->h1lolo ? s->h1lolo[i] : 0.0);
+  }
+  st.have_h1aa = false;
+  const size_t nh1 = (size_t)st.apwordmax * st.apwordmax * L1 * na;
+  if (s->h1aa)
+    for (size_t i = 0; i < nh1; ++i)
+      if (s->h1aa[i] != 0.0) { st.have_h1aa = true; break; }
+  const int e1 = s->intgv[3] - s->intgv[0] + 1, e2 = s->intgv[4] - s->intgv[1] + 1,
+            e3 = s->intgv[5] - s->intgv[2] + 1;
+  if (e1 <= 0 || e2 <= 0 || e3 <= 0) {
+    excfv_set_error("excfv_set_static: empty intgv box");
+    return EXCFV_ERR_ARG;
+  }
+  const size_t nbox = (size_t)e1 * e2 * e3;
+  const size_t maxnlo1 = std::max(1, st.maxnlo);
+  if ((rc = upload(&st.idxis, idxis.data(), na))) return rc;
+  if ((rc = upload(&st.rmt, s->rmt, ns))) return rc;
+  if ((rc = upload(&st.apword, s->apword, (size_t)L1 * ns))) return rc;
+  if ((rc = upload(&st.flist, flist.data(), flist.size()))) return rc;
+  if ((rc = upload(&st.fofl, fofl.data(), fofl.size()))) return rc;
+  if ((rc = upload(&st.lo_atom, lo_atom.data(), lo_atom.size()))) return rc;
+  if ((rc = upload(&st.lo_local, lo_local.data(), lo_local.size()))) return rc;
+  if ((rc = upload(&st.lo_lm, lo_lm.data(), lo_lm.size()))) return rc;
+  if ((rc = upload(&st.lo_ilo, lo_ilo.data(), lo_ilo.size()))) return rc;
+  if ((rc = upload(&st.aa, s->aa, (size_t)st.maxaa * st.maxaa * na))) return rc;
+  if ((rc = upload(&st.loa, st.nlotot ? s->loa : nullptr, maxnlo1 * st.maxaa * na))) return rc;
+  if ((rc = upload(&st.lolo, st.nlotot ? s->lolo : nullptr, maxnlo1 * maxnlo1 * na))) return rc;
+  if ((rc = upload(&st.oalo, oalo.data(), noalo))) return rc;
+  if ((rc = upload(&st.ololo, ololo.data(), nololo))) return rc;
+  if (st.have_h1aa && (rc = upload(&st.h1aa, s->h1aa, nh1))) return rc;
+  if ((rc = upload(&st.ivg, s->ivg, (size_t)3 * st.ngrtot))) return rc;
+  if ((rc = upload(&st.ivgig, s->ivgig, nbox))) return rc;
+  if ((rc = upload(&st.veffig, s->veffig, st.ngvec))) return rc;
+  const double* xsrc = (st.vrel != 0) ? s->meffig : s->cfunig;
+  if (!xsrc) {
+    excfv_set_error("excfv_set_static: meffig required when valence_relativity != 0");
+    return EXCFV_ERR_ARG;
+  }
+  if ((rc = upload(&st.xig, xsrc, st.ngvec))) return rc;
+  if ((rc = upload(&st.cfunig, s->cfunig, st.ngvec))) return rc;
+  if (st.h1on && !s->m2effig) {
+    excfv_set_error("excfv_set_static: m2effig required when h1on");
+    return EXCFV_ERR_ARG;
+  }
+  if ((rc = upload(&st.m2effig, st.h1on ? s->m2effig : nullptr, st.ngvec))) return rc;
+  if ((rc = dalloc(&st.zdinv, (size_t)st.apwordmax * st.apwordmax * L1 * na))) return rc;
+  double *d_spr = nullptr, *d_apwfr = nullptr;
+  if ((rc = upload(&d_spr, s->sprwin, (size_t)st.npmatch * ns))) return rc;
+  if ((rc = upload(&d_apwfr, s->apwfrwin, (size_t)st.npmatch * st.apwordmax * L1 * na))) return rc;
+  rc = match_compute_zdinv(st, d_spr, d_apwfr, h->stream);
+  cudaStreamSynchronize(h->stream);
+  cudaFree(d_spr);
+  cudaFree(d_apwfr);
+  if (rc) return rc;
+  h->have_static = true;
+  return EXCFV_OK;
+}
+
+int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax) {
+  Workspace& ws = h->ws;
+  if (!h->have_static) {
+    excfv_set_error("excfv_set_static must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  if (nmatmax <= ws.nmatmax && ngkmax <= ws.ngkmax && kmax <= ws.kmax && ws.H) return EXCFV_OK;
+  nmatmax = std::max(nmatmax, ws.nmatmax);
+  ngkmax = std::max(ngkmax, ws.ngkmax);
+  kmax = std::max(kmax, ws.kmax);
+  cudaStreamSynchronize(h->stream);
+  free_workspace(ws);
+  const DevStatic& st = h->st;
+  const size_t n = nmatmax, n2 = n * n, AM = (size_t)st.natmtot * st.maxaa;
+  const size_t K = kmax;
+  int rc;
+  if ((rc = dalloc(&ws.H, n2)) || (rc = dalloc(&ws.O, n2)) || (rc = dalloc(&ws.Ui, n2)) ||
+      (rc = dalloc(&ws.T, n2)) || (rc = dalloc(&ws.Apk, AM * ngkmax)) ||
+      (rc = dalloc(&ws.Zpk, AM * ngkmax)) || (rc = dalloc(&ws.ylm, (size_t)st.lmmaxapw * ngkmax)) ||
+      (rc = dalloc(&ws.djl, (size_t)ngkmax * (st.lmaxapw + 1) * st.apwordmax * st.nspecies)) ||
+      (rc = dalloc(&ws.apwalm, (size_t)ngkmax * st.apwordmax * st.lmmaxapw * st.natmtot)) ||
+      (rc = dalloc(&ws.igpig, (size_t)ngkmax)) || (rc = dalloc(&ws.vgpc, (size_t)3 * ngkmax)) ||
+      (rc = dalloc(&ws.gpc, (size_t)ngkmax)) || (rc = dalloc(&ws.tpgpc, (size_t)2 * ngkmax)) ||
+      (rc = dalloc(&ws.sfacgp, (size_t)ngkmax * st.natmtot)) ||
+      (rc = dalloc(&ws.gk_iv, (size_t)3 * ngkmax)) || (rc = dalloc(&ws.d, n)) ||
+      (rc = dalloc(&ws.e, n)) || (rc = dalloc(&ws.tau, n)) ||
+      (rc = dalloc(&ws.Wp, n * tridiag_nb())) ||
+      (rc = dalloc(&ws.red, (size_t)tridiag_workspace_doubles())) || (rc = dalloc(&ws.w, n)) ||
+      (rc = dalloc(&ws.stein_ws, tridiag_eig_scratch_doubles((int)n, (int)K))) ||
+      (rc = dalloc(&ws.icl, K)) || (rc = dalloc(&ws.ybuf, 2 * n)) || (rc = dalloc(&ws.Z, n * K)) ||
+      (rc = dalloc(&ws.Z2, n * K)) || (rc = dalloc(&ws.Gk, K * K)) || (rc = dalloc(&ws.Gki, K * K)) ||
+      (rc = dalloc(&ws.Tf, ((n + 31) / 32 + 1) * 32 * 32)) || (rc = dalloc(&ws.Xs, 2 * 32 * K)) ||
+      (rc = dalloc(&ws.status, (size_t)ST_NWORDS)) || (rc = dalloc(&ws.bar, (size_t)4))) {
+    free_workspace(ws);
+    return rc;
+  }
+  CUDA_TRY(cudaMemset(ws.status, 0, ST_NWORDS * sizeof(int)));
+  CUDA_TRY(cudaMemset(ws.bar, 0, 4 * sizeof(unsigned)));
+  ws.nmatmax = (int)nmatmax;
+  ws.ngkmax = (int)ngkmax;
+  ws.kmax = (int)kmax;
+  return EXCFV_OK;
+}
+
+// ---------------------------------------------------------------------------
+// exported C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* excfv_last_error(void) { return g_err; }
+
+int excfv_create(int device, excfv_handle** out) {
+  if (!out) return EXCFV_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    excfv_set_error("excfv_create: no CUDA device %d", device);
+    return EXCFV_ERR_CUDA;
+  }
+  DeviceGuard g(device);
+  cudaDeviceProp prop;
+  CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) {
+    excfv_set_error("excfv_create: device %d is sm_%d%d; libexcfv is built for sm_100a", device,
+                    prop.major, prop.minor);
+    return EXCFV_ERR_UNSUPPORTED;
+  }
+  excfv_handle* h = new excfv_handle();
+  h->device = device;
+  h->nsm = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    excfv_set_error("excfv_create: stream creation failed");
+    return EXCFV_ERR_CUDA;
+  }
+  h->stream = h->own_stream;
+  *out = h;
+  return EXCFV_OK;
+}
+
+int excfv_destroy(excfv_handle* h) {
+  if (!h) return EXCFV_OK;
+  DeviceGuard g(h->device);
+  cudaStreamSynchronize(h->stream);
+  free_workspace(h->ws);
+  free_static(h->st);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+  return EXCFV_OK;
+}
+
+int excfv_set_precision(excfv_handle* h, int prec) {
+  if (!h) return EXCFV_ERR_ARG;
+  if (prec != EXCFV_PREC_FP64 && prec != EXCFV_PREC_MIXED) return EXCFV_ERR_ARG;
+  h->prec = prec;
+  return EXCFV_OK;
+}
+
+int excfv_set_stream(excfv_handle* h, void* stream) {
+  if (!h) return EXCFV_ERR_ARG;
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return EXCFV_OK;
+}
+
+int excfv_reserve(excfv_handle* h, int32_t nmatmax, int32_t ngkmax) {
+  if (!h || nmatmax <= 0 || ngkmax <= 0) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  return stage_reserve(h, nmatmax, ngkmax, std::max(1, std::min(h->st.nstfv, nmatmax)));
+}
+
+int excfv_set_static(excfv_handle* h, const excfv_static* s) {
+  if (!h) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  return stage_set_static(h, s);
+}
+
+static int check_k(excfv_handle* h, int nmatp, int ngp, int ngkmax) {
+  if (!h) return EXCFV_ERR_ARG;
+  if (!h->have_static) {
+    excfv_set_error("excfv_set_static must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  if (ngp <= 0 || ngp > ngkmax || nmatp != ngp + h->st.nlotot) {
+    excfv_set_error("inconsistent sizes: nmatp=%d ngp=%d ngkmax=%d nlotot=%d", nmatp, ngp, ngkmax,
+                    h->st.nlotot);
+    return EXCFV_ERR_ARG;
+  }
+  return EXCFV_OK;
+}
+
+int excfv_match(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc,
+                const double* tpgpc, const double* sfacgp, double* apwalm) {
+  if (!h || !gpc || !tpgpc || !sfacgp || !apwalm) return EXCFV_ERR_ARG;
+  int rc = check_k(h, ngp + h->st.nlotot, ngp, ngkmax);
+  if (rc) return rc;
+  DeviceGuard g(h->device);
+  if ((rc = stage_reserve(h, ngp + h->st.nlotot, ngkmax, std::max(1, h->st.nstfv)))) return rc;
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  if (ngkmax != ws.ngkmax) {
+    // staged arrays use the workspace leading dimension; re-reserve exactly
+    free_workspace(ws);
+    if ((rc = stage_reserve(h, ngp + h->st.nlotot, ngkmax, std::max(1, h->st.nstfv)))) return rc;
+  }
+  CUDA_TRY(cudaMemcpyAsync(ws.gpc, gpc, sizeof(double) * ngkmax, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.tpgpc, tpgpc, sizeof(double) * 2 * ngkmax, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.sfacgp, sfacgp, sizeof(cplx) * (size_t)ngkmax * h->st.natmtot,
+                           cudaMemcpyHostToDevice, s));
+  if ((rc = stage_match(h, ngp, ngkmax, ws.apwalm))) return rc;
+  const size_t na = (size_t)ngkmax * h->st.apwordmax * h->st.lmmaxapw * h->st.natmtot;
+  CUDA_TRY(cudaMemcpyAsync(apwalm, ws.apwalm, sizeof(cplx) * na, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return EXCFV_OK;
+}
+
+// G+k arrays (host) -> workspace, ld = ws.ngkmax
+static int stage_gk_host(excfv_handle* h, int ngp, int ngkmax, const int32_t* igpig,
+                         const double* vgpc) {
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  CUDA_TRY(cudaMemcpyAsync(ws.igpig, igpig, sizeof(int) * ngp, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.vgpc, vgpc, sizeof(double) * 3 * ngp, cudaMemcpyHostToDevice, s));
+  (void)ngkmax;
+  return EXCFV_OK;
+}
+
+int excfv_hamiltonandoverlapsetup(excfv_handle* h, int32_t nmatp, int32_t ngp, int32_t ngkmax,
+                                  const double* apwalm, const int32_t* igpig, const double* vgpc,
+                                  double* hmat, double* omat) {
+  int rc = check_k(h, nmatp, ngp, ngkmax);
+  if (rc) return rc;
+  if (!apwalm || !igpig || !vgpc || !hmat || !omat) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  if ((rc = stage_reserve(h, nmatp, ngkmax, std::max(1, h->st.nstfv)))) return rc;
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  const size_t na = (size_t)ngkmax * h->st.apwordmax * h->st.lmmaxapw * h->st.natmtot;
+  if (ngkmax > ws.ngkmax) return EXCFV_ERR_STATE;
+  CUDA_TRY(cudaMemcpyAsync(ws.apwalm, apwalm, sizeof(cplx) * na, cudaMemcpyHostToDevice, s));
+  if ((rc = stage_gk_host(h, ngp, ngkmax, igpig, vgpc))) return rc;
+  if ((rc = stage_pack_apwalm(h, ngp, ngkmax, ws.apwalm))) return rc;
+  if ((rc = stage_setup(h, nmatp, ngp, true))) return rc;
+  const size_t nn = (size_t)nmatp * nmatp;
+  CUDA_TRY(cudaMemcpyAsync(hmat, ws.H, sizeof(cplx) * nn, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(omat, ws.O, sizeof(cplx) * nn, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return EXCFV_OK;
+}
+
+int excfv_solvewithlapack(excfv_handle* h, int32_t nmatp, const double* hmat, const double* omat,
+                          int32_t nstfv, double evaltol, double* evalfv, double* evecfv,
+                          int32_t ldevec) {
+  if (!h || nmatp <= 0 || !hmat || !omat || !evalfv || !evecfv || nstfv < 1 || nstfv > nmatp ||
+      ldevec < nmatp)
+    return EXCFV_ERR_ARG;
+  if (!h->have_static) {
+    excfv_set_error("excfv_set_static must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  DeviceGuard g(h->device);
+  int rc = stage_reserve(h, nmatp, std::max(1, h->ws.ngkmax), std::max(nstfv, h->st.nstfv));
+  if (rc) return rc;
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  const double t0 = now_s();
+  const size_t nn = (size_t)nmatp * nmatp;
+  CUDA_TRY(cudaMemcpyAsync(ws.H, hmat, sizeof(cplx) * nn, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.O, omat, sizeof(cplx) * nn, cudaMemcpyHostToDevice, s));
+  // ZHEGVX('U') reads the upper triangles only
+  if ((rc = mirror_upper(s, nmatp, ws.H, nmatp))) return rc;
+  cplx* outv = nullptr;
+  double* outw = nullptr;
+  if ((rc = dalloc(&outv, (size_t)nmatp * nstfv))) return rc;
+  if ((rc = dalloc(&outw, (size_t)nstfv))) {
+    cudaFree(outv);
+    return rc;
+  }
+  rc = stage_solve(h, nmatp, nstfv, evaltol, outw, outv, nmatp);
+  if (rc == 0) {
+    CUDA_TRY(cudaMemcpy2DAsync(evecfv, sizeof(cplx) * ldevec, outv, sizeof(cplx) * nmatp,
+                               sizeof(cplx) * nmatp, nstfv, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(evalfv, outw, sizeof(double) * nstfv, cudaMemcpyDeviceToHost, s));
+    rc = stage_status(h, nmatp);
+  }
+  cudaStreamSynchronize(s);
+  cudaFree(outv);
+  cudaFree(outw);
+  h->timings[2] = now_s() - t0;
+  return rc;
+}
+
+// evalfv/evecfv device outputs for the seceqn paths
+static int solve_into(excfv_handle* h, int nmatp, double* d_eval, cplx* d_evec, long long ld) {
+  return stage_solve(h, nmatp, h->st.nstfv, h->st.evaltol, d_eval, d_evec, ld);
+}
+
+int excfv_seceqnfv(excfv_handle* h, int32_t ispn, int32_t ik, int32_t nmatp, int32_t ngp,
+                   int32_t ngkmax, const int32_t* igpig, const double* vgpc, const double* apwalm,
+                   int32_t nmatmax, double* evalfv, double* evecfv) {
+  (void)ik;
+  if (ispn != 1) {
+    excfv_set_error("excfv_seceqnfv: only one first-variational spin (ispn = 1) is supported");
+    return EXCFV_ERR_UNSUPPORTED;
+  }
+  int rc = check_k(h, nmatp, ngp, ngkmax);
+  if (rc) return rc;
+  if (!igpig || !vgpc || !apwalm || !evalfv || !evecfv || nmatmax < nmatp) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  if ((rc = stage_reserve(h, nmatp, ngkmax, std::max(1, h->st.nstfv)))) return rc;
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  const int k = h->st.nstfv;
+  if (k > nmatp) return EXCFV_ERR_ARG;
+  const double t0 = now_s();
+  const size_t na = (size_t)ngkmax * h->st.apwordmax * h->st.lmmaxapw * h->st.natmtot;
+  if (ngkmax > ws.ngkmax) return EXCFV_ERR_STATE;
+  CUDA_TRY(cudaMemcpyAsync(ws.apwalm, apwalm, sizeof(cplx) * na, cudaMemcpyHostToDevice, s));
+  if ((rc = stage_gk_host(h, ngp, ngkmax, igpig, vgpc))) return rc;
+  if ((rc = stage_pack_apwalm(h, ngp, ngkmax, ws.apwalm))) return rc;
+  if ((rc = stage_setup(h, nmatp, ngp, false))) return rc;
+  // outputs staged in Z2 (n x k, overwritten only by the Cholesky-QR before the
+  // final product) -> use Ui-sized T buffer region past the solve instead
+  cplx* outv = ws.apwalm;  // free after packing; holds >= n*k complex? check below
+  const size_t need = (size_t)nmatp * k;
+  bool own = false;
+  if (need > na) {
+    if ((rc = dalloc(&outv, need))) return rc;
+    own = true;
+  }
+  if ((rc = solve_into(h, nmatp, ws.w + 0, outv, nmatp))) { if (own) cudaFree(outv); return rc; }
+  CUDA_TRY(cudaMemcpy2DAsync(evecfv, sizeof(cplx) * nmatmax, outv, sizeof(cplx) * nmatp,
+                             sizeof(cplx) * nmatp, k, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(evalfv, ws.w, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
+  rc = stage_status(h, nmatp);
+  if (own) cudaFree(outv);
+  h->timings[2] = now_s() - t0;
+  return rc;
+}
+
+int excfv_seceqn_dev(excfv_handle* h, int32_t nmatp, int32_t ngp, int32_t ngkmax, const double* gpc,
+                     const double* tpgpc, const double* sfacgp, const int32_t* igpig,
+                     const double* vgpc, int32_t nmatmax, double* evalfv, double* evecfv) {
+  int rc = check_k(h, nmatp, ngp, ngkmax);
+  if (rc) return rc;
+  if (!gpc || !tpgpc || !sfacgp || !igpig || !vgpc || !evalfv || !evecfv || nmatmax < nmatp)
+    return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  if ((rc = stage_reserve(h, nmatp, ngkmax, std::max(1, h->st.nstfv)))) return rc;
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  if (ngkmax != ws.ngkmax) {
+    excfv_set_error("excfv_seceqn_dev: ngkmax must equal the reserved ngkmax (%d)", ws.ngkmax);
+    return EXCFV_ERR_ARG;
+  }
+  const int k = h->st.nstfv;
+  if (k > nmatp) return EXCFV_ERR_ARG;
+  CUDA_TRY(cudaMemcpyAsync(ws.gpc, gpc, sizeof(double) * ngp, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.tpgpc, tpgpc, sizeof(double) * 2 * ngp, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.sfacgp, sfacgp, sizeof(cplx) * (size_t)ngkmax * h->st.natmtot,
+                           cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.igpig, igpig, sizeof(int) * ngp, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.vgpc, vgpc, sizeof(double) * 3 * ngp, cudaMemcpyDeviceToDevice, s));
+  if ((rc = stage_match(h, ngp, ngkmax, nullptr))) return rc;
+  if ((rc = stage_setup(h, nmatp, ngp, false))) return rc;
+  return solve_into(h, nmatp, evalfv, (cplx*)evecfv, nmatmax);
+}
+
+int excfv_seceqn(excfv_handle* h, int32_t ik, int32_t nmatp, int32_t ngp, int32_t ngkmax,
+                 const double* gpc, const double* tpgpc, const double* sfacgp,
+                 const int32_t* igpig, const double* vgpc, int32_t nmatmax, double* evalfv,
+                 double* evecfv) {
+  (void)ik;
+  int rc = check_k(h, nmatp, ngp, ngkmax);
+  if (rc) return rc;
+  if (!gpc || !tpgpc || !sfacgp || !igpig || !vgpc || !evalfv || !evecfv || nmatmax < nmatp)
+    return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  if ((rc = stage_reserve(h, nmatp, ngkmax, std::max(1, h->st.nstfv)))) return rc;
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  if (ngkmax != ws.ngkmax) {
+    free_workspace(ws);
+    if ((rc = stage_reserve(h, nmatp, ngkmax, std::max(1, h->st.nstfv)))) return rc;
+  }
+  const int k = h->st.nstfv;
+  if (k > nmatp) return EXCFV_ERR_ARG;
+  const double t0 = now_s();
+  CUDA_TRY(cudaMemcpyAsync(ws.gpc, gpc, sizeof(double) * ngp, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.tpgpc, tpgpc, sizeof(double) * 2 * ngp, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.sfacgp, sfacgp, sizeof(cplx) * (size_t)ngkmax * h->st.natmtot,
+                           cudaMemcpyHostToDevice, s));
+  if ((rc = stage_gk_host(h, ngp, ngkmax, igpig, vgpc))) return rc;
+  if ((rc = stage_match(h, ngp, ngkmax, nullptr))) return rc;
+  if ((rc = stage_setup(h, nmatp, ngp, false))) return rc;
+  cplx* outv = ws.apwalm;
+  const size_t na = (size_t)ngkmax * h->st.apwordmax * h->st.lmmaxapw * h->st.natmtot;
+  const size_t need = (size_t)nmatp * k;
+  bool own = false;
+  if (need > na) {
+    if ((rc = dalloc(&outv, need))) return rc;
+    own = true;
+  }
+  if ((rc = solve_into(h, nmatp, ws.w, outv, nmatp))) { if (own) cudaFree(outv); return rc; }
+  CUDA_TRY(cudaMemcpy2DAsync(evecfv, sizeof(cplx) * nmatmax, outv, sizeof(cplx) * nmatp,
+                             sizeof(cplx) * nmatp, k, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaMemcpyAsync(evalfv, ws.w, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
+  rc = stage_status(h, nmatp);
+  if (own) cudaFree(outv);
+  h->timings[2] = now_s() - t0;
+  return rc;
+}
+
+int excfv_sync(excfv_handle* h) {
+  if (!h) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  return stage_status(h, 0);
+}
+
+int excfv_get_timings(excfv_handle* h, double* t4) {
+  if (!h || !t4) return EXCFV_ERR_ARG;
+  for (int i = 0; i < 4; ++i) t4[i] = h->timings[i];
+  return EXCFV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,113 @@
+// Internal state of an excfv handle and the stage entry points.
+#pragma once
+
+#include "common.cuh"
+#include "../../include/excfv.h"
+
+// Per-SCF-iteration data resident in HBM.
+struct DevStatic {
+  int natmtot = 0, nspecies = 0;
+  int lmaxapw = 0, lmaxmat = 0, lmmaxapw = 0, apwordmax = 0;
+  int nlomax = 0, lolmmax = 0, nlotot = 0, maxaa = 0, maxnlo = 0;
+  int ngvec = 0, ngrtot = 0, h1on = 0, vrel = 1, npmatch = 0;
+  int intgv[6] = {0, 0, 0, 0, 0, 0};
+  double omega = 0.0;
+  int nstfv = 0;
+  double evaltol = 0.0;
+  bool have_h1aa = false;
+  // device arrays
+  int* idxis = nullptr;     // (natmtot) 0-based species
+  double* rmt = nullptr;    // (nspecies)
+  int* apword = nullptr;    // (lmaxapw+1, nspecies)
+  int* flist = nullptr;     // (maxaa, nspecies) packed (l, m, io) -> lm*apwordmax+io, -1 = unused
+  int* fofl = nullptr;      // (lmmaxapw*apwordmax, nspecies) inverse of flist, -1 unused
+  int* lo_atom = nullptr;   // (nlotot) atom of each LO function
+  int* lo_local = nullptr;  // (nlotot) index inside the atom's LO block
+  int* lo_lm = nullptr;     // (maxnlo, natmtot) lm of LO function j of the atom
+  int* lo_ilo = nullptr;    // (maxnlo, natmtot) ilo of LO function j
+  cplx* aa = nullptr;       // (maxaa, maxaa, natmtot)
+  cplx* loa = nullptr;      // (maxnlo, maxaa, natmtot)
+  cplx* lolo = nullptr;     // (maxnlo, maxnlo, natmtot)
+  double* oalo = nullptr;   // (apwordmax, nlomax, natmtot) (+ h1loa folded in)
+  double* ololo = nullptr;  // (nlomax, nlomax, natmtot) (+ h1lolo folded in)
+  double* h1aa = nullptr;   // (apwordmax, apwordmax, lmaxapw+1, natmtot) or null
+  int* ivg = nullptr;       // (3, ngrtot)
+  int* ivgig = nullptr;     // box
+  cplx* veffig = nullptr;
+  cplx* xig = nullptr;      // meffig (vrel != 0) or cfunig: the kinetic factor of hmlistln
+  cplx* cfunig = nullptr;
+  cplx* m2effig = nullptr;
+  double* zdinv = nullptr;  // (apwordmax, apwordmax, lmaxapw+1, natmtot) inverse of zd
+};
+
+struct Workspace {
+  int nmatmax = 0, ngkmax = 0, kmax = 0;
+  cplx* H = nullptr;        // n x n
+  cplx* O = nullptr;        // n x n
+  cplx* Ui = nullptr;       // n x n, inverse Cholesky factor
+  cplx* T = nullptr;        // n x n, scratch
+  cplx* Apk = nullptr;      // (natmtot*maxaa) x ngkmax packed matching coefficients
+  cplx* Zpk = nullptr;      // (natmtot*maxaa) x ngkmax  aa * A
+  cplx* ylm = nullptr;      // lmmaxapw x ngkmax
+  double* djl = nullptr;    // (ngkmax, lmaxapw+1, apwordmax, nspecies)
+  cplx* apwalm = nullptr;   // reference-layout apwalm (for the host entry points)
+  int* igpig = nullptr;     // (ngkmax)
+  double* vgpc = nullptr;   // (3, ngkmax)
+  double* gpc = nullptr;
+  double* tpgpc = nullptr;
+  cplx* sfacgp = nullptr;   // (ngkmax, natmtot)
+  int* gk_iv = nullptr;     // (3, ngkmax) ivg of each G+k
+  // eigensolver
+  double* d = nullptr;      // (n) tridiagonal diagonal
+  double* e = nullptr;      // (n) off-diagonal
+  cplx* tau = nullptr;      // (n) reflector scalars
+  cplx* Wp = nullptr;       // n x NBT panel W of the tridiagonal reduction
+  double* red = nullptr;    // reduction scratch of the panel kernel
+  double* w = nullptr;      // (n) eigenvalues
+  double* Y = nullptr;      // n x kmax real eigenvectors of T
+  double* stein_ws = nullptr;
+  int* icl = nullptr;       // (kmax) cluster starts
+  cplx* ybuf = nullptr;     // 2 x nmatmax, y = C v of the reduction
+  cplx* Z = nullptr;        // n x kmax complex
+  cplx* Z2 = nullptr;       // n x kmax complex (Cholesky-QR output)
+  cplx* Gk = nullptr;       // kmax x kmax Gram matrix
+  cplx* Gki = nullptr;      // kmax x kmax inverse factor
+  cplx* Tf = nullptr;       // block reflector factors
+  cplx* Xs = nullptr;       // scratch nb x kmax
+  int* status = nullptr;    // ST_NWORDS
+  unsigned int* bar = nullptr;  // grid barrier words
+  // host staging
+  cplx* h_pinned = nullptr;
+  size_t h_pinned_bytes = 0;
+};
+
+struct excfv_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  int prec = EXCFV_PREC_FP64;
+  bool have_static = false;
+  DevStatic st;
+  Workspace ws;
+  double timings[4] = {0, 0, 0, 0};
+  int nsm = 148;
+};
+
+// ---- stages (each enqueues work on h->stream) ------------------------------
+int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax);
+int stage_set_static(excfv_handle* h, const excfv_static* s);
+void free_static(DevStatic& st);
+void free_workspace(Workspace& ws);
+
+// match: G+k data already in ws.{gpc,tpgpc,sfacgp}; writes ws.Apk (packed)
+// and, if apwalm_ref != null, the reference layout.
+int stage_match(excfv_handle* h, int ngp, int ngkmax, cplx* apwalm_ref);
+// reference-layout apwalm (device) -> ws.Apk
+int stage_pack_apwalm(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm);
+// H, O upper triangles (+ mirror of H; mirror of O when mirror_o)
+int stage_setup(excfv_handle* h, int nmatp, int ngp, bool mirror_o);
+// generalized eigensolve on ws.H (full) / ws.O (upper) -> evalfv, evecfv
+int stage_solve(excfv_handle* h, int n, int nstfv, double evaltol, double* d_eval,
+                cplx* d_evec, long long ldevec);
+// device status -> LAPACK-style info (synchronises the stream)
+int stage_status(excfv_handle* h, int n);

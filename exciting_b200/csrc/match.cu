@@ -1,0 +1,429 @@
+// APW matching coefficients on the device (src/match.f90:83-185).
+//
+// The reference solves, per atom and l, ZGESV(zd, zb) with
+//   zd(i,j) = d^{i-1}u_{j,l}/dr^{i-1} at R_MT          (G independent)
+//   zb(i,G,m) = 4 pi i^l / sqrt(Omega) |G+k|^{i-1} j_l^{(i-1)}(|G+k| R)
+//               exp(i (G+k).r_a) conj(Y_lm(G+k)).
+// Because zd is real and independent of G, the solution factorises:
+//   apwalm(G,io,lm,a) = [sum_j zdinv(io,j) djl(l,j,G)] * 4 pi i^l/sqrt(Omega)
+//                       * sfac(G,a) * conj(Y_lm(G+k)).
+// zdinv is formed once per SCF iteration (k_zdinv); per k-point one thread
+// per G+k evaluates Y_lm and the Bessel derivatives (k_ylm_bessel), then a
+// write-bound kernel emits the coefficients directly in the packed layout
+// used by the setup GEMMs (k_apwalm_packed) and, when the caller wants the
+// reference array, in (ngkmax, apwordmax, lmmaxapw, natmtot) order
+// (k_apwalm_ref).
+#include "handle.cuh"
+
+namespace {
+
+constexpr int LMAX_CAP = 20;   // largest lmaxapw supported by the device path
+constexpr int MAXM = 6;        // highest Bessel derivative (sbesseldm limit)
+
+// ---- special functions ------------------------------------------------------
+
+// Y_lm(theta, phi), l <= lmax, packed lm = l(l+1)+m; Masters & Richards-Dinger
+// recursion with the Condon-Shortley phase (src/src_lib/genylm.f90).
+__device__ void d_genylm(int lmax, double theta, double phi, cplx* ylm, int stride) {
+  ylm[0] = cmk(0.28209479177387814347, 0.0);
+  if (lmax == 0) return;
+  const double sn = sin(theta), cs = cos(theta);
+  double x[LMAX_CAP + 1];
+  for (int l = 1; l <= lmax; ++l) {
+    x[l] = (l % 2 == 0) ? 1.0 : -1.0;
+    double dx = 0.0;
+    for (int m = l; m >= 1; --m) {
+      const double t = sqrt((double)((l + m) * (l - m + 1)));
+      x[m - 1] = -(sn * dx + 2.0 * m * cs * x[m]) / t;
+      dx = sn * x[m] * t;
+    }
+    double sc = sn, acc = 0.0;
+    for (int m = 1; m <= l; ++m) {
+      x[m] *= sc;
+      acc += x[m] * x[m];
+      sc *= sn;
+    }
+    acc = 2.0 * acc + x[0] * x[0];
+    const double nrm = sqrt((2 * l + 1) / (4.0 * M_PI * acc));
+    const int c = l * (l + 1);
+    ylm[c * stride] = cmk(nrm * x[0], 0.0);
+    for (int m = 1; m <= l; ++m) {
+      double sp, cp;
+      sincos(m * phi, &sp, &cp);
+      const cplx v = cmk(nrm * x[m] * cp, nrm * x[m] * sp);
+      ylm[(c + m) * stride] = v;
+      const double sg = (m & 1) ? -1.0 : 1.0;
+      ylm[(c - m) * stride] = cmk(sg * v.x, -sg * v.y);
+    }
+  }
+}
+
+// j_l(x), l = 0..lmax (src/src_lib/sbessel.f90): series for x < 1e-8,
+// Miller's downward recurrence with rescaling for x < lmax, upward otherwise.
+__device__ void d_sbessel(int lmax, double x, double* jl) {
+  if (x < 1e-8) {
+    jl[0] = 1.0;
+    double t1 = 1.0, t2 = 1.0;
+    for (int l = 1; l <= lmax; ++l) {
+      t1 /= (2 * l + 1);
+      t2 *= x;
+      jl[l] = t2 * t1;
+    }
+    return;
+  }
+  const double xi = 1.0 / x;
+  if (x < (double)lmax) {
+    const double rsc = 1e150, rsci = 1e-150;
+    double j0 = 0.6370354636449841609 * rsci, j1 = 0.3532702964695481204 * rsci, jt;
+    for (int l = lmax + 25; l > lmax; --l) {
+      jt = j0 * (2 * l + 1) * xi - j1;
+      j1 = j0;
+      j0 = jt;
+      if (fabs(j0) > rsc) { j1 *= rsci; j0 *= rsci; }
+    }
+    for (int l = lmax; l >= 0; --l) {
+      jt = j0 * (2 * l + 1) * xi - j1;
+      j1 = j0;
+      j0 = jt;
+      if (fabs(j0) > rsc) {
+        j1 *= rsci;
+        j0 *= rsci;
+        for (int q = l + 1; q <= lmax; ++q) jl[q] *= rsci;
+      }
+      jl[l] = j1;
+    }
+    double s, c;
+    sincos(x, &s, &c);
+    const double t1 = 1.0 / ((jl[0] - x * jl[1]) * c + x * jl[0] * s);
+    for (int l = 0; l <= lmax; ++l) jl[l] *= t1;
+    return;
+  }
+  double s, c;
+  sincos(x, &s, &c);
+  jl[0] = s * xi;
+  if (lmax == 0) return;
+  jl[1] = (jl[0] - c) * xi;
+  double j0 = jl[0], j1 = jl[1];
+  for (int l = 2; l <= lmax; ++l) {
+    const double jt = (2 * l - 1) * j1 * xi - j0;
+    j0 = j1;
+    j1 = jt;
+    jl[l] = j1;
+  }
+}
+
+// m-th derivative of j_l(x), l = 0..lmax (src/src_lib/sbesseldm.f90).  For
+// x > 1: d^m j_l = sum_i (a_i j_l + b_i j_{l+1}) / x^i with integer a, b from
+// repeated use of j_l' = (l/x) j_l - j_{l+1}, j_{l+1}' = j_l - ((l+2)/x) j_{l+1}.
+// For x <= 1: the power series.
+__device__ void d_sbesseldm(int m, int lmax, double x, double* djl) {
+  double jl[LMAX_CAP + 2];
+  if (m == 0) { d_sbessel(lmax, x, djl); return; }
+  if (x > 1.0) {
+    d_sbessel(lmax + 1, x, jl);
+    for (int l = 0; l <= lmax; ++l) {
+      long long a[MAXM + 2], b[MAXM + 2], na[MAXM + 2], nb[MAXM + 2];
+      for (int i = 0; i < MAXM + 2; ++i) { a[i] = 0; b[i] = 0; }
+      a[0] = 1;
+      for (int it = 0; it < m; ++it) {
+        for (int i = 0; i < MAXM + 2; ++i) { na[i] = 0; nb[i] = 0; }
+        for (int i = 0; i <= m; ++i) {
+          if (a[i]) { na[i + 1] += a[i] * (l - i); nb[i] -= a[i]; }
+          if (b[i]) { na[i] += b[i]; nb[i + 1] -= b[i] * (l + 2 + i); }
+        }
+        for (int i = 0; i < MAXM + 2; ++i) { a[i] = na[i]; b[i] = nb[i]; }
+      }
+      double acc = (double)a[0] * jl[l] + (double)b[0] * jl[l + 1];
+      double t = 1.0;
+      for (int i = 1; i <= m + 1; ++i) {
+        t *= x;
+        acc += ((double)a[i] * jl[l] + (double)b[i] * jl[l + 1]) / t;
+      }
+      djl[l] = acc;
+    }
+    return;
+  }
+  const double x2 = x * x;
+  for (int l = 0; l <= lmax; ++l) {
+    const int i0 = max((m - l + 1) / 2, 0);
+    const int j = 2 * i0 + l - m;
+    double t = (j == 0) ? 1.0 : pow(x, (double)j);
+    double num = 1.0;  // (j+m)!/j!
+    for (int q = j + 1; q <= j + m; ++q) num *= q;
+    double den = 1.0;  // i0! (2 i0 + 2 l + 1)!! (-2)^i0
+    for (int q = 2; q <= i0; ++q) den *= q;
+    for (int q = 2 * i0 + 2 * l + 1; q > 0; q -= 2) den *= q;
+    for (int q = 0; q < i0; ++q) den *= -2.0;
+    t = num * t / den;
+    double acc = t;
+    for (int i = i0 + 1; i <= 20; ++i) {
+      const int jj = 2 * i + l;
+      t = -t * (double)((jj - 1) * jj) * x2 / (double)((jj - l) * (jj - m - 1) * (jj - m) * (jj + l + 1));
+      if (fabs(t) <= 1e-40) break;
+      acc += t;
+    }
+    djl[l] = acc;
+  }
+}
+
+// m-th derivative at x of the polynomial through np points
+// (src/src_lib/polynom.f90; closed forms for np <= 4, Newton form otherwise).
+__device__ double d_polynom(int m, int np, const double* xa, const double* ya, double x) {
+  if (m >= np) return 0.0;
+  if (np == 1) return m == 0 ? ya[0] : 0.0;
+  if (np == 2) {
+    const double c2 = (ya[1] - ya[0]) / (xa[1] - xa[0]);
+    return m == 0 ? c2 * (x - xa[0]) + ya[0] : c2;
+  }
+  if (np == 3) {
+    const double x1 = xa[1] - xa[0], x2 = xa[2] - xa[0];
+    const double y1 = ya[1] - ya[0], y2 = ya[2] - ya[0];
+    double t1 = 1.0 / (x1 * x2 * (x2 - x1));
+    const double t2 = x1 * y2, t3 = x2 * y1;
+    const double c2 = t1 * (x2 * t3 - x1 * t2), c3 = t1 * (t2 - t3);
+    t1 = x - xa[0];
+    if (m == 0) return ya[0] + t1 * (c2 + c3 * t1);
+    if (m == 1) return 2.0 * c3 * t1 + c2;
+    return 2.0 * c3;
+  }
+  if (np == 4) {
+    const double x1 = xa[1] - xa[0], x2 = xa[2] - xa[0], x3 = xa[3] - xa[0];
+    const double y1 = ya[1] - ya[0], y2 = ya[2] - ya[0], y3 = ya[3] - ya[0];
+    double t1 = 1.0 / (x1 * x2 * x3 * (x1 - x2) * (x1 - x3) * (x2 - x3));
+    const double t2 = x1 * x2 * y3, t3 = x2 * x3 * y1, t4 = x3 * x1 * y2;
+    const double t5 = x1 * x1, t6 = x2 * x2, t7 = x3 * x3;
+    const double c2 = t1 * (t3 * (x3 * t6 - x2 * t7) + t4 * (x1 * t7 - x3 * t5) + t2 * (x2 * t5 - x1 * t6));
+    const double c3 = t1 * (t3 * (t7 - t6) + t4 * (t5 - t7) + t2 * (t6 - t5));
+    const double c4 = t1 * (t3 * (x2 - x3) + t4 * (x3 - x1) + t2 * (x1 - x2));
+    t1 = x - xa[0];
+    if (m == 0) return ya[0] + t1 * (c2 + t1 * (c3 + c4 * t1));
+    if (m == 1) return c2 + t1 * (2.0 * c3 + 3.0 * c4 * t1);
+    if (m == 2) return 6.0 * c4 * t1 + 2.0 * c3;
+    return 6.0 * c4;
+  }
+  double c[16];
+  for (int i = 0; i < np; ++i) c[i] = ya[i];
+  for (int i = 1; i < np; ++i)
+    for (int j = np - 1; j >= i; --j) c[j] = (c[j] - c[j - 1]) / (xa[j] - xa[j - i]);
+  if (m == 0) {
+    double acc = c[0], t = 1.0;
+    for (int i = 1; i < np; ++i) { t *= (x - xa[i - 1]); acc += c[i] * t; }
+    return acc;
+  }
+  const double x0 = xa[0];
+  for (int j = 1; j < np; ++j)
+    for (int i = 1; i <= np - j; ++i) {
+      const int k = np - i;
+      c[k - 1] += (x0 - xa[k - j]) * c[k];
+    }
+  for (int j = 1; j <= m; ++j)
+    for (int i = m; i < np; ++i) c[i] *= (double)(i - j + 1);
+  double t1 = c[np - 1];
+  const double t2 = x - x0;
+  for (int i = np - 2; i >= m; --i) t1 = t1 * t2 + c[i];
+  return t1;
+}
+
+// ---- kernels --------------------------------------------------------------
+
+// One thread per (l, atom): zd from the radial window, then its inverse by
+// Gauss-Jordan elimination with partial pivoting.
+__global__ void k_zdinv(int natmtot, int lmaxapw, int apwordmax, int np, const int* idxis,
+                        const int* apword, const double* rmt, const double* sprwin,
+                        const double* apwfrwin, double* zdinv) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= natmtot * (lmaxapw + 1)) return;
+  const int l = t % (lmaxapw + 1), ias = t / (lmaxapw + 1);
+  const int is = idxis[ias];
+  const int nap = apword[l + (lmaxapw + 1) * is];
+  double zd[8][8], inv[8][8];
+  for (int i = 0; i < nap; ++i)
+    for (int j = 0; j < nap; ++j) {
+      const double* ya = apwfrwin + (size_t)np * (j + apwordmax * (l + (lmaxapw + 1) * (size_t)ias));
+      zd[i][j] = d_polynom(i, np, sprwin + (size_t)np * is, ya, rmt[is]);
+      inv[i][j] = (i == j) ? 1.0 : 0.0;
+    }
+  for (int c = 0; c < nap; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < nap; ++r)
+      if (fabs(zd[r][c]) > fabs(zd[piv][c])) piv = r;
+    for (int q = 0; q < nap; ++q) {
+      double tz = zd[c][q]; zd[c][q] = zd[piv][q]; zd[piv][q] = tz;
+      double ti = inv[c][q]; inv[c][q] = inv[piv][q]; inv[piv][q] = ti;
+    }
+    const double p = zd[c][c];
+    const double pi = (p != 0.0) ? 1.0 / p : 0.0;
+    for (int q = 0; q < nap; ++q) { zd[c][q] *= pi; inv[c][q] *= pi; }
+    for (int r = 0; r < nap; ++r) {
+      if (r == c) continue;
+      const double f = zd[r][c];
+      for (int q = 0; q < nap; ++q) { zd[r][q] -= f * zd[c][q]; inv[r][q] -= f * inv[c][q]; }
+    }
+  }
+  double* out = zdinv + (size_t)apwordmax * apwordmax * (l + (lmaxapw + 1) * (size_t)ias);
+  for (int i = 0; i < apwordmax; ++i)
+    for (int j = 0; j < apwordmax; ++j)
+      out[i + apwordmax * j] = (i < nap && j < nap) ? inv[i][j] : 0.0;
+}
+
+// One thread per G+k: Y_lm (ylm[ig*lmmax + lm]) and, per species, the Bessel
+// derivatives |G+k|^j j_l^{(j)}(|G+k| R), djl[((is*ngkmax + ig)*(lmax+1) + l)*apwordmax + j].
+__global__ void k_ylm_bessel(int ngp, int ngkmax, int lmax, int apwordmax, int nspecies,
+                             const int* apword, const double* rmt, const double* gpc,
+                             const double* tpgpc, cplx* ylm, double* djl) {
+  const int ig = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ig >= ngp) return;
+  const int lmmax = (lmax + 1) * (lmax + 1);
+  d_genylm(lmax, tpgpc[2 * ig], tpgpc[2 * ig + 1], ylm + (size_t)ig * lmmax, 1);
+  const double g = gpc[ig];
+  double buf[LMAX_CAP + 1];
+  for (int is = 0; is < nspecies; ++is) {
+    int omax = 0;
+    for (int l = 0; l <= lmax; ++l) omax = max(omax, apword[l + (lmax + 1) * is]);
+    const double x = g * rmt[is];
+    double sc = 1.0;
+    for (int j = 0; j < omax; ++j) {
+      d_sbesseldm(j, lmax, x, buf);
+      for (int l = 0; l <= lmax; ++l)
+        djl[(((size_t)is * ngkmax + ig) * (lmax + 1) + l) * apwordmax + j] = sc * buf[l];
+      sc *= g;
+    }
+  }
+}
+
+__device__ __forceinline__ cplx apw_value(int ig, int io, int l, int lm, int ias, int is, int ngkmax,
+                                          int lmax, int lmmax, int apwordmax, double fpso,
+                                          const cplx* ylm, const double* djl, const double* zdinv,
+                                          const cplx* sfacgp) {
+  const double* zi = zdinv + (size_t)apwordmax * apwordmax * (l + (lmax + 1) * (size_t)ias);
+  const double* dj = djl + (((size_t)is * ngkmax + ig) * (lmax + 1) + l) * apwordmax;
+  double r = 0.0;
+  for (int j = 0; j < apwordmax; ++j) r += zi[io + apwordmax * j] * dj[j];
+  // i^l
+  const int lm4 = l & 3;
+  const double pr = (lm4 == 0) ? 1.0 : (lm4 == 2 ? -1.0 : 0.0);
+  const double pim = (lm4 == 1) ? 1.0 : (lm4 == 3 ? -1.0 : 0.0);
+  const cplx s = sfacgp[ig + (size_t)ngkmax * ias];
+  const cplx y = ylm[(size_t)ig * lmmax + lm];
+  // fpso * i^l * s * conj(y) * r
+  const cplx il = cmk(pr * fpso * r, pim * fpso * r);
+  return cmul(il, cmulc(y, s));
+}
+
+// Packed layout: Apk[(ias*maxaa + f) + natmtot*maxaa*ig], f = (l, m, io).
+__global__ void k_apwalm_packed(int ngp, int ngkmax, int natmtot, int maxaa, int lmax,
+                                int apwordmax, const int* idxis, const int* flist, double fpso,
+                                const cplx* ylm, const double* djl, const double* zdinv,
+                                const cplx* sfacgp, cplx* Apk) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long rows = (long long)natmtot * maxaa;
+  if (t >= rows * ngp) return;
+  const int r = (int)(t % rows);
+  const int ig = (int)(t / rows);
+  const int f = r % maxaa, ias = r / maxaa;
+  const int is = idxis[ias];
+  const int code = flist[f + maxaa * is];
+  cplx v = cmk(0.0, 0.0);
+  if (code >= 0) {
+    const int lm = code / apwordmax, io = code % apwordmax;
+    int l = 0;
+    while ((l + 1) * (l + 1) <= lm) ++l;
+    v = apw_value(ig, io, l, lm, ias, is, ngkmax, lmax, (lmax + 1) * (lmax + 1), apwordmax, fpso,
+                  ylm, djl, zdinv, sfacgp);
+  }
+  Apk[r + rows * ig] = v;
+}
+
+// Reference layout apwalm(ngkmax, apwordmax, lmmaxapw, natmtot).
+__global__ void k_apwalm_ref(int ngp, int ngkmax, int natmtot, int lmax, int apwordmax,
+                             const int* idxis, const int* apword, double fpso, const cplx* ylm,
+                             const double* djl, const double* zdinv, const cplx* sfacgp,
+                             cplx* out) {
+  const int lmmax = (lmax + 1) * (lmax + 1);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long tot = (long long)ngkmax * apwordmax * lmmax * natmtot;
+  if (t >= tot) return;
+  long long q = t;
+  const int ig = (int)(q % ngkmax); q /= ngkmax;
+  const int io = (int)(q % apwordmax); q /= apwordmax;
+  const int lm = (int)(q % lmmax); q /= lmmax;
+  const int ias = (int)q;
+  const int is = idxis[ias];
+  int l = 0;
+  while ((l + 1) * (l + 1) <= lm) ++l;
+  cplx v = cmk(0.0, 0.0);
+  if (ig < ngp && io < apword[l + (lmax + 1) * is])
+    v = apw_value(ig, io, l, lm, ias, is, ngkmax, lmax, lmmax, apwordmax, fpso, ylm, djl, zdinv,
+                  sfacgp);
+  out[t] = v;
+}
+
+// Reference layout (device) -> packed layout (the apwi arrays of
+// hamiltonsetup.f90:62-71 stacked over atoms).
+__global__ void k_pack(int ngp, int ngkmax, int natmtot, int maxaa, int lmmax, int apwordmax,
+                       const int* idxis, const int* flist, const cplx* in, cplx* Apk) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long rows = (long long)natmtot * maxaa;
+  if (t >= rows * ngp) return;
+  const int r = (int)(t % rows);
+  const int ig = (int)(t / rows);
+  const int f = r % maxaa, ias = r / maxaa;
+  const int code = flist[f + maxaa * idxis[ias]];
+  cplx v = cmk(0.0, 0.0);
+  if (code >= 0) {
+    const int lm = code / apwordmax, io = code % apwordmax;
+    v = in[ig + (size_t)ngkmax * (io + (size_t)apwordmax * (lm + (size_t)lmmax * ias))];
+  }
+  Apk[r + rows * ig] = v;
+}
+
+}  // namespace
+
+int match_compute_zdinv(DevStatic& st, const double* d_sprwin, const double* d_apwfrwin,
+                        cudaStream_t s) {
+  if (st.lmaxapw > LMAX_CAP || st.apwordmax > 7 || st.npmatch > 16) return EXCFV_ERR_UNSUPPORTED;
+  const int nt = st.natmtot * (st.lmaxapw + 1);
+  k_zdinv<<<(nt + 127) / 128, 128, 0, s>>>(st.natmtot, st.lmaxapw, st.apwordmax, st.npmatch,
+                                           st.idxis, st.apword, st.rmt, d_sprwin, d_apwfrwin,
+                                           st.zdinv);
+  CUDA_TRY(cudaGetLastError());
+  return EXCFV_OK;
+}
+
+int stage_match(excfv_handle* h, int ngp, int ngkmax, cplx* apwalm_ref) {
+  DevStatic& st = h->st;
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  if (st.lmaxapw > LMAX_CAP) return EXCFV_ERR_UNSUPPORTED;
+  const double fpso = 4.0 * M_PI / sqrt(st.omega);
+  k_ylm_bessel<<<(ngp + 127) / 128, 128, 0, s>>>(ngp, ws.ngkmax, st.lmaxapw, st.apwordmax,
+                                                 st.nspecies, st.apword, st.rmt, ws.gpc,
+                                                 ws.tpgpc, ws.ylm, ws.djl);
+  CUDA_TRY(cudaGetLastError());
+  const long long tot = (long long)st.natmtot * st.maxaa * ngp;
+  k_apwalm_packed<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(
+      ngp, ws.ngkmax, st.natmtot, st.maxaa, st.lmaxapw, st.apwordmax, st.idxis, st.flist, fpso,
+      ws.ylm, ws.djl, st.zdinv, ws.sfacgp, ws.Apk);
+  CUDA_TRY(cudaGetLastError());
+  if (apwalm_ref) {
+    const long long tr = (long long)ngkmax * st.apwordmax * st.lmmaxapw * st.natmtot;
+    // the G+k arrays were staged with leading dimension ws.ngkmax; the
+    // reference layout uses the caller's ngkmax
+    if (ngkmax != ws.ngkmax) return EXCFV_ERR_ARG;
+    k_apwalm_ref<<<(unsigned)((tr + 255) / 256), 256, 0, s>>>(
+        ngp, ngkmax, st.natmtot, st.lmaxapw, st.apwordmax, st.idxis, st.apword, fpso, ws.ylm,
+        ws.djl, st.zdinv, ws.sfacgp, apwalm_ref);
+    CUDA_TRY(cudaGetLastError());
+  }
+  return EXCFV_OK;
+}
+
+int stage_pack_apwalm(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm) {
+  DevStatic& st = h->st;
+  const long long tot = (long long)st.natmtot * st.maxaa * ngp;
+  k_pack<<<(unsigned)((tot + 255) / 256), 256, 0, h->stream>>>(ngp, ngkmax, st.natmtot, st.maxaa,
+                                                               st.lmmaxapw, st.apwordmax, st.idxis,
+                                                               st.flist, apwalm, h->ws.Apk);
+  CUDA_TRY(cudaGetLastError());
+  return EXCFV_OK;
+}

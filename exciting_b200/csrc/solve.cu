@@ -1,0 +1,201 @@
+// Generalized Hermitian eigensolve H x = e O x for the lowest k states
+// (ZHEGVX(1,'V','I','U'), src/src_eigensystem/modfvsystem.f90:691-693).
+//
+//   O = U^H U                      potrf_upper      (ZPOTRF)
+//   Ui = U^-1                      trtri_upper
+//   C = Ui^H (H Ui)                two GEMMs skipping the zero triangles (ZHEGST)
+//   C = Q T Q^H                    tridiag_reduce   (ZHETRD)
+//   T y = e y, lowest k            tridiag_eig      (DSTEBZ + DSTEIN)
+//   Z = orth(y)                    Cholesky-QR on the k vectors
+//   Z <- Q Z                       block reflectors (I - V Tf V^H), GEMMs (ZUNMTR)
+//   X = Ui Z                       one GEMM (ZTRSM)
+#include "handle.cuh"
+
+int potrf_upper(excfv_handle* h, int n, cplx* O, cplx* Ui, long long ld);
+int trtri_upper(excfv_handle* h, int n, const cplx* U, cplx* Ui, long long ld, cplx* scratch);
+int tridiag_reduce(excfv_handle* h, int n, cplx* C, long long ld);
+int tridiag_nb();
+int tridiag_eig(excfv_handle* h, int n, int k, double abstol, const double* d, const double* e,
+                double* w, cplx* Z, long long ldz, double* scratch, int* iscratch);
+int mirror_upper(cudaStream_t s, int n, cplx* M, long long ld);
+
+namespace {
+
+constexpr int NBQ = 32;  // reflectors per block (= panel width of the reduction)
+constexpr int LT = 256;
+
+// Triangular factor of the block reflector H_p ... H_{p+nb-1} = I - V T V^H
+// (forward, columnwise; the ZLARFT recurrence T(0:i,i) = -tau_i T(0:i,0:i) V^H v_i).
+// One CTA per block.  V(r, j) = C(p+1+r, p+j) for r >= j (unit entry stored).
+__global__ void __launch_bounds__(LT) k_larft(int n, const cplx* C, long long ld, const cplx* tau,
+                                              cplx* Tf) {
+  __shared__ cplx VT[32][NBQ + 1];   // row chunk of V, then the triangular factor
+  __shared__ cplx G[NBQ][NBQ + 1];
+  auto& Vs = VT;
+  auto& Ts = VT;
+  const int blk = blockIdx.x;
+  const int p = blk * NBQ;
+  const int nb = min(NBQ, n - 1 - p);
+  if (nb <= 0) return;
+  const int m = n - p - 1;
+  const int tid = threadIdx.x;
+  // each thread owns 4 entries (a, b) of the 32x32 Gram matrix
+  cplx acc[4];
+  int ea[4], eb[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int id = tid + u * LT;
+    ea[u] = id % NBQ;
+    eb[u] = id / NBQ;
+    acc[u] = cmk(0.0, 0.0);
+  }
+  for (int r0 = 0; r0 < m; r0 += 32) {
+    __syncthreads();
+    for (int t = tid; t < 32 * NBQ; t += LT) {
+      const int rr = t % 32, j = t / 32;
+      const int r = r0 + rr;
+      cplx v = cmk(0.0, 0.0);
+      if (r < m && j < nb && r >= j) v = C[(p + 1 + r) + ld * (p + j)];
+      Vs[rr][j] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int a = ea[u], b = eb[u];
+      for (int rr = 0; rr < 32; ++rr) acc[u] = cadd(acc[u], cmulc(Vs[rr][a], Vs[rr][b]));
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) G[ea[u]][eb[u]] = acc[u];
+  __syncthreads();
+  for (int t = tid; t < NBQ * NBQ; t += LT) Ts[t % NBQ][t / NBQ] = cmk(0.0, 0.0);
+  __syncthreads();
+  if (tid == 0) Ts[0][0] = tau[p];
+  __syncthreads();
+  for (int i = 1; i < nb; ++i) {
+    const cplx ti = tau[p + i];
+    cplx val = cmk(0.0, 0.0);
+    if (tid < i) {
+      // sum_{q=tid}^{i-1} T(tid, q) G(q, i)
+      for (int q = tid; q < i; ++q) val = cadd(val, cmul(Ts[tid][q], G[q][i]));
+      val = cmul(cmk(-ti.x, -ti.y), val);
+    }
+    __syncthreads();
+    if (tid < i) Ts[tid][i] = val;
+    if (tid == 0) Ts[i][i] = ti;
+    __syncthreads();
+  }
+  cplx* out = Tf + (size_t)blk * NBQ * NBQ;
+  for (int t = tid; t < NBQ * NBQ; t += LT) out[t] = Ts[t % NBQ][t / NBQ];
+}
+
+__global__ void k_copy_eval(int k, const double* w, double* out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < k) out[j] = w[j];
+}
+
+}  // namespace
+
+// Z (n x k) <- Q Z with Q = H_0 ... H_{n-2} from tridiag_reduce.
+int apply_q(excfv_handle* h, int n, int k, const cplx* C, long long ld, cplx* Z, long long ldz) {
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  if (n < 2) return EXCFV_OK;
+  const int nblk = (n - 1 + NBQ - 1) / NBQ;
+  k_larft<<<nblk, LT, 0, s>>>(n, C, ld, ws.tau, ws.Tf);
+  CUDA_TRY(cudaGetLastError());
+  const cplx one = cmk(1.0, 0.0), mone = cmk(-1.0, 0.0), zero = cmk(0.0, 0.0);
+  cplx* X1 = ws.Xs;
+  cplx* X2 = ws.Xs + (size_t)NBQ * ws.kmax;
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int p = b * NBQ;
+    const int nb = min(NBQ, n - 1 - p);
+    const int m = n - p - 1;
+    const cplx* V = C + (p + 1) + ld * p;
+    cplx* Zs = Z + (p + 1);
+    int rc = zgemm1(s, OP_C, OP_N, nb, k, m, one, V, ld, Zs, ldz, zero, X1, NBQ, TRI_NONE,
+                    TRI_UPPER, TRI_NONE);
+    if (rc) return rc;
+    rc = zgemm1(s, OP_N, OP_N, nb, k, nb, one, ws.Tf + (size_t)b * NBQ * NBQ, NBQ, X1, NBQ, zero,
+                X2, NBQ, TRI_NONE, TRI_UPPER, TRI_NONE);
+    if (rc) return rc;
+    rc = zgemm1(s, OP_N, OP_N, m, k, nb, mone, V, ld, X2, NBQ, one, Zs, ldz, TRI_NONE, TRI_LOWER,
+                TRI_NONE);
+    if (rc) return rc;
+  }
+  return EXCFV_OK;
+}
+
+// Z (n x k) <- Z R^-1 with Z^H Z = R^H R (Cholesky-QR), scratch in ws.Gk/ws.Gki/ws.Z2.
+int cholqr(excfv_handle* h, int n, int k, cplx*& Z, long long ldz) {
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  const cplx one = cmk(1.0, 0.0), zero = cmk(0.0, 0.0);
+  int rc = zgemm1(s, OP_C, OP_N, k, k, n, one, Z, ldz, Z, ldz, zero, ws.Gk, k, TRI_UPPER);
+  if (rc) return rc;
+  if ((rc = potrf_upper(h, k, ws.Gk, ws.Gki, k))) return rc;
+  if ((rc = trtri_upper(h, k, ws.Gk, ws.Gki, k, ws.Z2))) return rc;
+  rc = zgemm1(s, OP_N, OP_N, n, k, k, one, Z, ldz, ws.Gki, k, zero, ws.Z2, ldz, TRI_NONE, TRI_NONE,
+              TRI_UPPER);
+  if (rc) return rc;
+  cplx* t = Z;
+  Z = ws.Z2;
+  ws.Z2 = t;
+  return EXCFV_OK;
+}
+
+int stage_solve(excfv_handle* h, int n, int k, double evaltol, double* d_eval, cplx* d_evec,
+                long long ldevec) {
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  const long long ld = n;
+  const cplx one = cmk(1.0, 0.0), zero = cmk(0.0, 0.0);
+  int rc;
+  if (k < 1 || k > n) return EXCFV_ERR_ARG;
+  if (k > ws.kmax) return EXCFV_ERR_ARG;
+  CUDA_TRY(cudaMemsetAsync(ws.status, 0, ST_NWORDS * sizeof(int), s));
+  // O = U^H U, Ui = U^-1
+  if ((rc = potrf_upper(h, n, ws.O, ws.Ui, ld))) return rc;
+  if ((rc = trtri_upper(h, n, ws.O, ws.Ui, ld, ws.T))) return rc;
+  // C = Ui^H H Ui (upper), then both triangles
+  if ((rc = zgemm1(s, OP_N, OP_N, n, n, n, one, ws.H, ld, ws.Ui, ld, zero, ws.T, ld, TRI_NONE,
+                   TRI_NONE, TRI_UPPER)))
+    return rc;
+  if ((rc = zgemm1(s, OP_C, OP_N, n, n, n, one, ws.Ui, ld, ws.T, ld, zero, ws.H, ld, TRI_UPPER,
+                   TRI_LOWER, TRI_NONE)))
+    return rc;
+  if ((rc = mirror_upper(s, n, ws.H, ld))) return rc;
+  // tridiagonal reduction
+  if ((rc = tridiag_reduce(h, n, ws.H, ld))) return rc;
+  // eigenpairs of T
+  cplx* Z = ws.Z;
+  if ((rc = tridiag_eig(h, n, k, evaltol, ws.d, ws.e, ws.w, Z, ld, ws.stein_ws, ws.icl)))
+    return rc;
+  if ((rc = cholqr(h, n, k, Z, ld))) return rc;
+  // back-transforms
+  if ((rc = apply_q(h, n, k, ws.H, ld, Z, ld))) return rc;
+  if ((rc = zgemm1(s, OP_N, OP_N, n, k, n, one, ws.Ui, ld, Z, ld, zero, d_evec, ldevec, TRI_NONE,
+                   TRI_UPPER, TRI_NONE)))
+    return rc;
+  ws.Z = Z;  // cholqr may have swapped the buffers
+  k_copy_eval<<<(k + 127) / 128, 128, 0, s>>>(k, ws.w, d_eval);
+  CUDA_TRY(cudaGetLastError());
+  return EXCFV_OK;
+}
+
+int stage_status(excfv_handle* h, int n) {
+  int st[ST_NWORDS];
+  CUDA_TRY(cudaMemcpyAsync(st, h->ws.status, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (st[ST_BARRIER]) {
+    excfv_set_error("grid barrier timed out in the tridiagonal reduction");
+    return EXCFV_ERR_TIMEOUT;
+  }
+  if (st[ST_POTRF]) return n + st[ST_POTRF];
+  if (st[ST_STEBZ]) {
+    excfv_set_error("bisection did not converge for %d eigenvalues", st[ST_STEBZ]);
+    return EXCFV_ERR_NOCONV;
+  }
+  if (st[ST_STEIN]) return st[ST_STEIN];
+  return EXCFV_OK;
+}

@@ -1,0 +1,230 @@
+// Complex FP64 GEMM on the FP64 tensor path (DMMA, mma.sync m8n8k4 f64).
+//
+// C = alpha * op(A) * op(B) + beta * C, column-major, op in {N, C, T},
+// strided batch over blockIdx.z, optional triangular structure (see
+// ZgemmArgs).  This is the workhorse of the plain-FP64 form: the muffin-tin
+// contractions A^H (aa A) / A^H A, the Cholesky trailing updates, the
+// triangular inverse, the two-sided reduction U^-H H U^-1, the her2k update
+// of the tridiagonal reduction and the eigenvector back-transforms.
+//
+// tcgen05 has no FP64 kind, so the FP64 tensor instruction on sm_100a is
+// DMMA.  A complex product is four real DMMAs on split re/im planes:
+//   Cre += Are*Bre + Aim*(-Bim),  Cim += Are*Bim + Aim*Bre.
+//
+// Tiling: 64x64 complex outputs per CTA, 4 warps (2x2), 32x32 per warp =
+// 4x4 m8n8 tiles x {re, im}; k-tile 8 complex, two shared-memory stages
+// with register-staged global loads (loads of tile t+1 overlap the DMMAs of
+// tile t).  Shared rows are padded by 4 doubles so that fragment loads
+// (lane%4 -> k row, lane/4 -> column) are bank-conflict free.
+#include "common.cuh"
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 8, PAD = 4, NT = 128;
+constexpr int LDS = BM + PAD;
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <int OPA, int OPB>
+__global__ void __launch_bounds__(NT) zgemm_kernel(ZgemmArgs p) {
+  __shared__ __align__(16) double As[2][2][BK][LDS];
+  __shared__ __align__(16) double Bs[2][2][BK][LDS];
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int i0 = blockIdx.x * BM;
+  const int j0 = blockIdx.y * BN;
+  if (p.uplo_c == TRI_UPPER && i0 > j0 + BN - 1) return;
+  if (p.uplo_c == TRI_LOWER && j0 > i0 + BM - 1) return;
+
+  const long long bz = blockIdx.z;
+  const cplx* __restrict__ A = p.A + bz * p.strideA;
+  const cplx* __restrict__ B = p.B + bz * p.strideB;
+  cplx* __restrict__ C = p.C + bz * p.strideC;
+
+  int kbeg = 0, kend = p.k;
+  if (p.tri_a == TRI_LOWER) kend = min(kend, i0 + BM);
+  if (p.tri_a == TRI_UPPER) kbeg = max(kbeg, i0);
+  if (p.tri_b == TRI_UPPER) kend = min(kend, j0 + BN);
+  if (p.tri_b == TRI_LOWER) kbeg = max(kbeg, j0);
+  kbeg = (kbeg / BK) * BK;
+
+  const int wm = (warp & 1) * 32;
+  const int wn = (warp >> 1) * 32;
+
+  double acc[4][4][2][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) acc[a][b][c][0] = acc[a][b][c][1] = 0.0;
+
+  cplx ra[4], rb[4];
+
+  auto load_tile = [&](int kt) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int idx = tid + r * NT;
+      int ii, kk;
+      if (OPA == OP_N) { ii = idx & 63; kk = idx >> 6; }
+      else { kk = idx & 7; ii = idx >> 3; }
+      const int gi = i0 + ii, gk = kt + kk;
+      bool ok = gi < p.m && gk < kend;
+      if (p.tri_a == TRI_LOWER && gk > gi) ok = false;
+      if (p.tri_a == TRI_UPPER && gk < gi) ok = false;
+      cplx v = cmk(0.0, 0.0);
+      if (ok) {
+        if (OPA == OP_N) v = A[gi + (long long)gk * p.lda];
+        else {
+          v = A[gk + (long long)gi * p.lda];
+          if (OPA == OP_C) v.y = -v.y;
+        }
+      }
+      ra[r] = v;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int idx = tid + r * NT;
+      int jj, kk;
+      if (OPB == OP_N) { kk = idx & 7; jj = idx >> 3; }
+      else { jj = idx & 63; kk = idx >> 6; }
+      const int gj = j0 + jj, gk = kt + kk;
+      bool ok = gj < p.n && gk < kend;
+      if (p.tri_b == TRI_UPPER && gk > gj) ok = false;
+      if (p.tri_b == TRI_LOWER && gk < gj) ok = false;
+      cplx v = cmk(0.0, 0.0);
+      if (ok) {
+        if (OPB == OP_N) v = B[gk + (long long)gj * p.ldb];
+        else {
+          v = B[gj + (long long)gk * p.ldb];
+          if (OPB == OP_C) v.y = -v.y;
+        }
+      }
+      rb[r] = v;
+    }
+  };
+
+  auto store_tile = [&](int st) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int idx = tid + r * NT;
+      int ii, kk;
+      if (OPA == OP_N) { ii = idx & 63; kk = idx >> 6; }
+      else { kk = idx & 7; ii = idx >> 3; }
+      As[st][0][kk][ii] = ra[r].x;
+      As[st][1][kk][ii] = ra[r].y;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int idx = tid + r * NT;
+      int jj, kk;
+      if (OPB == OP_N) { kk = idx & 7; jj = idx >> 3; }
+      else { jj = idx & 63; kk = idx >> 6; }
+      Bs[st][0][kk][jj] = rb[r].x;
+      Bs[st][1][kk][jj] = rb[r].y;
+    }
+  };
+
+  if (kbeg < kend) {
+    load_tile(kbeg);
+    store_tile(0);
+    __syncthreads();
+    int st = 0;
+    for (int kt = kbeg; kt < kend; kt += BK) {
+      const bool more = kt + BK < kend;
+      if (more) load_tile(kt + BK);
+#pragma unroll
+      for (int ks = 0; ks < BK; ks += 4) {
+        const int kr = ks + (lane & 3);
+        const int cc = lane >> 2;
+        double are[4], aim[4], bre[4], bim[4], bimn[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          are[t] = As[st][0][kr][wm + t * 8 + cc];
+          aim[t] = As[st][1][kr][wm + t * 8 + cc];
+          bre[t] = Bs[st][0][kr][wn + t * 8 + cc];
+          bim[t] = Bs[st][1][kr][wn + t * 8 + cc];
+          bimn[t] = -bim[t];
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            dmma(acc[a][b][0][0], acc[a][b][0][1], are[a], bre[b]);
+            dmma(acc[a][b][0][0], acc[a][b][0][1], aim[a], bimn[b]);
+            dmma(acc[a][b][1][0], acc[a][b][1][1], are[a], bim[b]);
+            dmma(acc[a][b][1][0], acc[a][b][1][1], aim[a], bre[b]);
+          }
+      }
+      if (more) store_tile(st ^ 1);
+      __syncthreads();
+      st ^= 1;
+    }
+  }
+
+  const bool use_beta = (p.beta.x != 0.0 || p.beta.y != 0.0);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int row = i0 + wm + a * 8 + (lane >> 2);
+    if (row >= p.m) continue;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int col = j0 + wn + b * 8 + (lane & 3) * 2 + e;
+        if (col >= p.n) continue;
+        if (p.uplo_c == TRI_UPPER && row > col) continue;
+        if (p.uplo_c == TRI_LOWER && row < col) continue;
+        const cplx v = cmk(acc[a][b][0][e], acc[a][b][1][e]);
+        cplx out = cmul(p.alpha, v);
+        cplx* dst = C + row + (long long)col * p.ldc;
+        if (use_beta) out = cadd(out, cmul(p.beta, *dst));
+        *dst = out;
+      }
+    }
+  }
+}
+
+template <int OPA, int OPB>
+int launch(cudaStream_t s, const ZgemmArgs& a) {
+  dim3 grid((a.m + BM - 1) / BM, (a.n + BN - 1) / BN, a.batch);
+  zgemm_kernel<OPA, OPB><<<grid, NT, 0, s>>>(a);
+  return 0;
+}
+
+}  // namespace
+
+int zgemm(cudaStream_t s, int opA, int opB, const ZgemmArgs& a) {
+  if (a.m <= 0 || a.n <= 0 || a.batch <= 0) return 0;
+  if (a.k <= 0 && a.beta.x == 1.0 && a.beta.y == 0.0) return 0;
+  switch (opA * 3 + opB) {
+    case OP_N * 3 + OP_N: return launch<OP_N, OP_N>(s, a);
+    case OP_N * 3 + OP_C: return launch<OP_N, OP_C>(s, a);
+    case OP_N * 3 + OP_T: return launch<OP_N, OP_T>(s, a);
+    case OP_C * 3 + OP_N: return launch<OP_C, OP_N>(s, a);
+    case OP_C * 3 + OP_C: return launch<OP_C, OP_C>(s, a);
+    case OP_C * 3 + OP_T: return launch<OP_C, OP_T>(s, a);
+    case OP_T * 3 + OP_N: return launch<OP_T, OP_N>(s, a);
+    case OP_T * 3 + OP_C: return launch<OP_T, OP_C>(s, a);
+    case OP_T * 3 + OP_T: return launch<OP_T, OP_T>(s, a);
+  }
+  return EXCFV_ERR_ARG;
+}
+
+int zgemm1(cudaStream_t s, int opA, int opB, int m, int n, int k, cplx alpha,
+           const cplx* A, long long lda, const cplx* B, long long ldb, cplx beta,
+           cplx* C, long long ldc, int uplo_c, int tri_a, int tri_b) {
+  ZgemmArgs a;
+  a.m = m; a.n = n; a.k = k; a.alpha = alpha; a.beta = beta;
+  a.A = A; a.lda = lda; a.strideA = 0;
+  a.B = B; a.ldb = ldb; a.strideB = 0;
+  a.C = C; a.ldc = ldc; a.strideC = 0;
+  a.batch = 1; a.uplo_c = uplo_c; a.tri_a = tri_a; a.tri_b = tri_b;
+  return zgemm(s, opA, opB, a);
+}

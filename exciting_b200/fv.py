@@ -1,0 +1,250 @@
+"""Host-side mirror of exciting's first-variational interface on libexcfv.
+
+The methods keep the reference's names, argument meaning and array layouts:
+
+==================================  =============================================
+``FirstVariational.match``          ``match`` (src/match.f90:13)
+``.hamiltonandoverlapsetup``        ``hamiltonandoverlapsetup`` (hamiltonandoverlapsetup.f90:8)
+``.solvewithlapack``                ``solvewithlapack`` (modfvsystem.f90:585)
+``.seceqnfv``                       ``seceqnfv`` (src/seceqnfv.f90:12)
+``.seceqn``                         body of ``seceqn`` for one spin (src/seceqn.f90:57-64)
+==================================  =============================================
+
+Arrays are NumPy arrays in Fortran order.  Errors: a positive LAPACK-style
+``info`` from the eigensolve raises :class:`DiagonalisationFailed` (the
+reference prints the message and stops, modfvsystem.f90:698-711); negative
+codes raise :class:`ExcfvError`.  Every call goes through the CUDA library;
+there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Tuple
+
+import numpy as np
+
+from . import lib as _lib
+from .lib import ExcfvError, ExcfvStatic
+
+
+class DiagonalisationFailed(RuntimeError):
+    def __init__(self, info: int, nmatp: int):
+        self.info = info
+        if info > nmatp:
+            msg = (f"Error(seceqnfv): diagonalisation failed, INFO = {info}: the leading minor of "
+                   f"the overlap matrix of order {info - nmatp} is not positive definite "
+                   f"(order of overlap matrix: {nmatp})")
+        else:
+            msg = f"Error(seceqnfv): diagonalisation failed, INFO = {info}: {info} eigenvectors did not converge"
+        super().__init__(msg)
+
+
+def _ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def _f(a, dtype) -> np.ndarray:
+    return np.asfortranarray(np.asarray(a, dtype=dtype))
+
+
+class FirstVariational:
+    """One libexcfv handle on one GPU."""
+
+    def __init__(self, device: int = 0, precision: int = _lib.EXCFV_PREC_FP64):
+        self._L = _lib.load()
+        h = C.c_void_p()
+        rc = self._L.excfv_create(device, C.byref(h))
+        if rc != 0:
+            raise ExcfvError(rc, "excfv_create")
+        self._h = h
+        self._keep = []
+        self.static = None
+        if precision != _lib.EXCFV_PREC_FP64:
+            self._check(self._L.excfv_set_precision(self._h, precision), "excfv_set_precision")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.excfv_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @staticmethod
+    def _check(rc: int, where: str, nmatp: int = 0):
+        if rc < 0:
+            raise ExcfvError(rc, where)
+        if rc > 0:
+            raise DiagonalisationFailed(rc, nmatp)
+
+    # ------------------------------------------------------------------
+    def set_static(self, st) -> None:
+        """Upload the per-SCF-iteration data (an ``exciting_b200.synthetic.Static``-like object)."""
+        keep = []
+
+        def i32(a):
+            x = _f(a, np.int32)
+            keep.append(x)
+            return x.ctypes.data_as(_lib._i32p)
+
+        def f64(a):
+            if a is None:
+                return None
+            x = _f(a, np.float64)
+            keep.append(x)
+            return x.ctypes.data_as(_lib._f64p)
+
+        def c128(a):
+            if a is None:
+                return None
+            x = _f(a, np.complex128)
+            keep.append(x)
+            return x.ctypes.data_as(_lib._f64p)
+
+        s = ExcfvStatic()
+        s.natmtot = st.natmtot
+        s.nspecies = st.nspecies
+        s.idxis = i32(np.asarray(st.idxis) + 1)
+        s.omega = float(st.omega)
+        s.rmt = f64(st.rmt)
+        s.lmaxapw = st.lmaxapw
+        s.lmaxmat = st.lmaxmat
+        s.apwordmax = st.apwordmax
+        s.apword = i32(st.apword)
+        s.nlomax = st.nlomax
+        s.nlorb = i32(st.nlorb)
+        s.lorbl = i32(st.lorbl)
+        s.lolmax = st.lolmax
+        s.idxlo = i32(st.idxlo)
+        s.nlotot = st.nlotot
+        s.maxaa = st.maxaa
+        s.maxnlo = st.maxnlo
+        s.losize = i32(st.losize)
+        s.aa = c128(st.aa)
+        s.loa = c128(st.loa)
+        s.lolo = c128(st.lolo)
+        s.oalo = f64(st.oalo)
+        s.ololo = f64(st.ololo)
+        s.h1aa = f64(st.h1aa)
+        s.h1loa = f64(st.h1loa)
+        s.h1lolo = f64(st.h1lolo)
+        s.h1on = int(bool(st.h1on))
+        s.valence_relativity = int(st.valence_relativity)
+        s.ngvec = st.ngvec
+        s.ngrtot = st.ngrtot
+        s.ivg = i32(st.ivg)
+        s.ivgig = i32(st.ivgig)
+        iv = np.asarray(st.intgv, dtype=np.int32)
+        for d in range(3):
+            s.intgv[d] = int(iv[d, 0])
+            s.intgv[3 + d] = int(iv[d, 1])
+        s.veffig = c128(st.veffig)
+        s.meffig = c128(st.meffig)
+        s.cfunig = c128(st.cfunig)
+        s.m2effig = c128(st.m2effig)
+        s.npmatch = st.npmatch
+        s.sprwin = f64(st.sprwin)
+        s.apwfrwin = f64(st.apwfrwin)
+        s.nstfv = st.nstfv
+        s.evaltol = float(st.evaltol)
+        self._check(self._L.excfv_set_static(self._h, C.byref(s)), "excfv_set_static")
+        self.static = st
+
+    def reserve(self, nmatmax: int, ngkmax: int) -> None:
+        self._check(self._L.excfv_reserve(self._h, nmatmax, ngkmax), "excfv_reserve")
+
+    # ------------------------------------------------------------------
+    def match(self, kp) -> np.ndarray:
+        st = self.static
+        out = np.zeros((kp.ngkmax, st.apwordmax, st.lmmaxapw, st.natmtot), dtype=np.complex128,
+                       order="F")
+        gpc = _f(kp.gpc, np.float64)
+        tp = _f(kp.tpgpc, np.float64)
+        sf = _f(kp.sfacgp, np.complex128)
+        rc = self._L.excfv_match(self._h, kp.ngp, kp.ngkmax, _ptr(gpc), _ptr(tp), _ptr(sf), _ptr(out))
+        self._check(rc, "excfv_match")
+        return out
+
+    def hamiltonandoverlapsetup(self, kp, apwalm: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+        n = kp.ngp + self.static.nlotot
+        H = np.zeros((n, n), dtype=np.complex128, order="F")
+        O = np.zeros((n, n), dtype=np.complex128, order="F")
+        a = _f(apwalm, np.complex128)
+        ig = _f(kp.igpig, np.int32)
+        vg = _f(kp.vgpc, np.float64)
+        rc = self._L.excfv_hamiltonandoverlapsetup(self._h, n, kp.ngp, kp.ngkmax, _ptr(a), _ptr(ig),
+                                                   _ptr(vg), _ptr(H), _ptr(O))
+        self._check(rc, "excfv_hamiltonandoverlapsetup")
+        return H, O
+
+    def solvewithlapack(self, H: np.ndarray, O: np.ndarray, nstfv: int, evaltol: float = 1e-14,
+                        ldevec: int = 0):
+        n = H.shape[0]
+        ld = max(ldevec, n)
+        Hf = _f(H, np.complex128)
+        Of = _f(O, np.complex128)
+        w = np.zeros(nstfv)
+        X = np.zeros((ld, nstfv), dtype=np.complex128, order="F")
+        rc = self._L.excfv_solvewithlapack(self._h, n, _ptr(Hf), _ptr(Of), nstfv, evaltol, _ptr(w),
+                                           _ptr(X), ld)
+        self._check(rc, "excfv_solvewithlapack", n)
+        return w, X[:n]
+
+    def seceqnfv(self, kp, apwalm: np.ndarray, nmatmax: int = 0, ispn: int = 1, ik: int = 1):
+        st = self.static
+        n = kp.ngp + st.nlotot
+        nmx = max(nmatmax, n)
+        w = np.zeros(st.nstfv)
+        X = np.zeros((nmx, st.nstfv), dtype=np.complex128, order="F")
+        a = _f(apwalm, np.complex128)
+        ig = _f(kp.igpig, np.int32)
+        vg = _f(kp.vgpc, np.float64)
+        rc = self._L.excfv_seceqnfv(self._h, ispn, ik, n, kp.ngp, kp.ngkmax, _ptr(ig), _ptr(vg),
+                                    _ptr(a), nmx, _ptr(w), _ptr(X))
+        self._check(rc, "excfv_seceqnfv", n)
+        return w, X
+
+    def seceqn(self, kp, nmatmax: int = 0, ik: int = 1, out=None):
+        """match + seceqnfv for one k-point; host arrays in and out."""
+        st = self.static
+        n = kp.ngp + st.nlotot
+        nmx = max(nmatmax, n)
+        if out is None:
+            w = np.zeros(st.nstfv)
+            X = np.zeros((nmx, st.nstfv), dtype=np.complex128, order="F")
+        else:
+            w, X = out
+        rc = self._L.excfv_seceqn(self._h, ik, n, kp.ngp, kp.ngkmax, _ptr(kp.gpc), _ptr(kp.tpgpc),
+                                  _ptr(kp.sfacgp), _ptr(kp.igpig), _ptr(kp.vgpc), nmx, _ptr(w),
+                                  _ptr(X))
+        self._check(rc, "excfv_seceqn", n)
+        return w, X
+
+    def seceqn_dev(self, n: int, ngp: int, ngkmax: int, ptrs: dict, nmatmax: int,
+                   eval_ptr: int, evec_ptr: int) -> None:
+        """Device-pointer form (asynchronous on the handle's stream)."""
+        rc = self._L.excfv_seceqn_dev(self._h, n, ngp, ngkmax, C.c_void_p(ptrs["gpc"]),
+                                      C.c_void_p(ptrs["tpgpc"]), C.c_void_p(ptrs["sfacgp"]),
+                                      C.c_void_p(ptrs["igpig"]), C.c_void_p(ptrs["vgpc"]), nmatmax,
+                                      C.c_void_p(eval_ptr), C.c_void_p(evec_ptr))
+        self._check(rc, "excfv_seceqn_dev", n)
+
+    def set_stream(self, stream_ptr: int) -> None:
+        self._check(self._L.excfv_set_stream(self._h, C.c_void_p(stream_ptr)), "excfv_set_stream")
+
+    def sync(self, n: int = 0) -> None:
+        self._check(self._L.excfv_sync(self._h), "excfv_sync", n)
+
+    def timings(self):
+        t = np.zeros(4)
+        self._L.excfv_get_timings(self._h, _ptr(t))
+        return t

@@ -1,0 +1,109 @@
+"""ctypes binding of libexcfv (the C ABI declared in include/excfv.h).
+
+The shared library is built in-tree (``exciting_b200/libexcfv.so``) by
+``exciting_b200.build.build_library``.  There is no fallback: if the library
+is missing, :func:`load` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libexcfv.so")
+
+EXCFV_OK = 0
+EXCFV_ERR_ARG = -1
+EXCFV_ERR_UNSUPPORTED = -2
+EXCFV_ERR_CUDA = -3
+EXCFV_ERR_ALLOC = -4
+EXCFV_ERR_STATE = -5
+EXCFV_ERR_TIMEOUT = -6
+EXCFV_ERR_NOCONV = -7
+
+EXCFV_PREC_FP64 = 0
+EXCFV_PREC_MIXED = 1
+
+_i32p = C.POINTER(C.c_int32)
+_f64p = C.POINTER(C.c_double)
+
+
+class ExcfvStatic(C.Structure):
+    """Mirror of ``struct excfv_static`` (field order and types must match)."""
+    _fields_ = [
+        ("natmtot", C.c_int32), ("nspecies", C.c_int32), ("idxis", _i32p),
+        ("omega", C.c_double), ("rmt", _f64p),
+        ("lmaxapw", C.c_int32), ("lmaxmat", C.c_int32), ("apwordmax", C.c_int32),
+        ("apword", _i32p), ("nlomax", C.c_int32), ("nlorb", _i32p), ("lorbl", _i32p),
+        ("lolmax", C.c_int32), ("idxlo", _i32p), ("nlotot", C.c_int32),
+        ("maxaa", C.c_int32), ("maxnlo", C.c_int32), ("losize", _i32p),
+        ("aa", _f64p), ("loa", _f64p), ("lolo", _f64p), ("oalo", _f64p), ("ololo", _f64p),
+        ("h1aa", _f64p), ("h1loa", _f64p), ("h1lolo", _f64p), ("h1on", C.c_int32),
+        ("valence_relativity", C.c_int32),
+        ("ngvec", C.c_int32), ("ngrtot", C.c_int32), ("ivg", _i32p), ("ivgig", _i32p),
+        ("intgv", C.c_int32 * 6),
+        ("veffig", _f64p), ("meffig", _f64p), ("cfunig", _f64p), ("m2effig", _f64p),
+        ("npmatch", C.c_int32), ("sprwin", _f64p), ("apwfrwin", _f64p),
+        ("nstfv", C.c_int32), ("evaltol", C.c_double),
+    ]
+
+
+#: name -> (restype, argtypes); every symbol declared in include/excfv.h
+SIGNATURES = {
+    "excfv_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "excfv_destroy": (C.c_int, [C.c_void_p]),
+    "excfv_last_error": (C.c_char_p, []),
+    "excfv_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
+    "excfv_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "excfv_reserve": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    "excfv_set_static": (C.c_int, [C.c_void_p, C.POINTER(ExcfvStatic)]),
+    "excfv_match": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                              C.c_void_p, C.c_void_p]),
+    "excfv_hamiltonandoverlapsetup": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_void_p]),
+    "excfv_solvewithlapack": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                        C.c_double, C.c_void_p, C.c_void_p, C.c_int32]),
+    "excfv_seceqnfv": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                 C.c_void_p]),
+    "excfv_seceqn": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                               C.c_void_p, C.c_void_p]),
+    "excfv_seceqn_dev": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                   C.c_void_p, C.c_void_p]),
+    "excfv_sync": (C.c_int, [C.c_void_p]),
+    "excfv_get_timings": (C.c_int, [C.c_void_p, C.c_void_p]),
+}
+
+_lib: Optional[C.CDLL] = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load libexcfv and declare every C-ABI signature.  Raises if missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"libexcfv not found at {path}: build it with exciting_b200.build.build_library() "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().excfv_last_error().decode(errors="replace")
+
+
+class ExcfvError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        super().__init__(f"{where} failed with status {code}: {last_error()}")

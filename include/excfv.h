@@ -1,0 +1,186 @@
+/*
+ * excfv.h -- C ABI of libexcfv: exciting's first-variational LAPW+lo hot path
+ * (APW matching, Hamiltonian/overlap setup, generalized Hermitian eigensolve
+ * for the lowest nstfv states) on one NVIDIA B200 (sm_100a).
+ *
+ * Conventions (identical to the Fortran caller, so arrays cross unchanged):
+ *   - complex arrays are interleaved (re, im) doubles = Fortran complex(8);
+ *   - all arrays are column-major with the reference's index order;
+ *   - index arrays hold the reference's 1-based values (igpig, idxlo, ivgig);
+ *   - "host" entry points take host pointers and copy in/out themselves;
+ *     "_dev" entry points take device pointers and run on the handle's stream.
+ *
+ * Return value of every entry point: 0 on success; > 0 is a LAPACK-style
+ * info from the eigensolve (> nmatp: the leading minor of order info-nmatp
+ * of the overlap matrix is not positive definite; 1..nmatp: that many
+ * eigenvectors failed to converge); < 0 is an EXCFV_ERR_* code.  The
+ * library never stops the process (the reference calls STOP on info /= 0,
+ * src/src_eigensystem/modfvsystem.f90:698-711; the Fortran shim may do so).
+ * excfv_last_error() returns a message for the last failure on the calling
+ * thread.
+ *
+ * Threading: a handle is used by one host thread at a time (the reference
+ * routines are not re-entrant either: save variables in
+ * src/src_eigensystem/hamiltonsetup.f90:27-28).  Separate handles may run
+ * concurrently on separate streams.
+ */
+#ifndef EXCFV_H
+#define EXCFV_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EXCFV_OK 0
+#define EXCFV_ERR_ARG (-1)
+#define EXCFV_ERR_UNSUPPORTED (-2)
+#define EXCFV_ERR_CUDA (-3)
+#define EXCFV_ERR_ALLOC (-4)
+#define EXCFV_ERR_STATE (-5)
+#define EXCFV_ERR_TIMEOUT (-6)
+#define EXCFV_ERR_NOCONV (-7)
+
+/* precision forms */
+#define EXCFV_PREC_FP64 0  /* FP64 end to end */
+#define EXCFV_PREC_MIXED 1 /* split-BF16 tensor-core setup + FP32 reduction + FP64 refinement */
+
+typedef struct excfv_handle excfv_handle;
+
+/*
+ * Per-SCF-iteration data.  In the reference these are module globals read by
+ * match/hamiltonsetup/overlapsetup/hmlistln/olpistln:
+ *   structure      mod_atoms, mod_muffin_tin, mod_lattice
+ *   APW/LO layout  mod_APW_LO (apword, nlorb, lorbl), mod_eigensystem (idxlo,
+ *                  mt_hscf%maxaa, mt_hscf%maxnlo, mt_hscf%losize)
+ *   MT blocks      mt_hscf%main%{aa,loa,lolo} (src/mod_eigensystem.F90:60-80),
+ *                  oalo, ololo, h1aa, h1loa, h1lolo (olprad)
+ *   G vectors      ivg, ivgig, intgv, ngvec (src/gengvec.f90:48-97)
+ *   interstitial   veffig, meffig, cfunig, m2effig
+ *   match window   spr(nrmt-np+1:nrmt,is), apwfr(nrmt-np+1:nrmt,1,io,l,ias), rmt, omega
+ * Every pointer is a host pointer; excfv_set_static copies the data.
+ */
+typedef struct excfv_static {
+  int32_t natmtot;
+  int32_t nspecies;
+  const int32_t* idxis;    /* (natmtot) species of each atom, 1-based (idxis) */
+  double omega;            /* unit-cell volume */
+  const double* rmt;       /* (nspecies) muffin-tin radii */
+  int32_t lmaxapw;         /* input%groundstate%lmaxapw */
+  int32_t lmaxmat;         /* input%groundstate%lmaxmat */
+  int32_t apwordmax;
+  const int32_t* apword;   /* (0:lmaxapw, nspecies) */
+  int32_t nlomax;
+  const int32_t* nlorb;    /* (nspecies) */
+  const int32_t* lorbl;    /* (nlomax, nspecies) */
+  int32_t lolmax;          /* idxlo first extent is (lolmax+1)^2 */
+  const int32_t* idxlo;    /* (lolmmax, nlomax, natmtot), 1-based values */
+  int32_t nlotot;
+  int32_t maxaa;           /* mt_hscf%maxaa */
+  int32_t maxnlo;          /* mt_hscf%maxnlo */
+  const int32_t* losize;   /* (nspecies) mt_hscf%losize */
+  const double* aa;        /* complex (maxaa, maxaa, natmtot) */
+  const double* loa;       /* complex (maxnlo, maxaa, natmtot) */
+  const double* lolo;      /* complex (maxnlo, maxnlo, natmtot) */
+  const double* oalo;      /* (apwordmax, nlomax, natmtot) */
+  const double* ololo;     /* (nlomax, nlomax, natmtot) */
+  const double* h1aa;      /* (apwordmax, apwordmax, 0:lmaxapw, natmtot) or NULL (= 0) */
+  const double* h1loa;     /* (apwordmax, nlomax, natmtot) or NULL */
+  const double* h1lolo;    /* (nlomax, nlomax, natmtot) or NULL */
+  int32_t h1on;            /* ValenceRelativity == 'iora*' (olpistln m2effig term) */
+  int32_t valence_relativity; /* 0 = 'none' (hmlistln uses cfunig), else meffig */
+  int32_t ngvec;
+  int32_t ngrtot;
+  const int32_t* ivg;      /* (3, ngrtot) */
+  const int32_t* ivgig;    /* box intgv(1,1):intgv(1,2) x ... , column-major */
+  int32_t intgv[6];        /* intgv(3,2) column-major: lo1,lo2,lo3,hi1,hi2,hi3 */
+  const double* veffig;    /* complex (ngvec) */
+  const double* meffig;    /* complex (ngvec) */
+  const double* cfunig;    /* complex (ngvec) */
+  const double* m2effig;   /* complex (ngvec) or NULL */
+  int32_t npmatch;         /* np = max(apwordmax+1, 4), src/match.f90:85 */
+  const double* sprwin;    /* (npmatch, nspecies) radial grid window at R_MT */
+  const double* apwfrwin;  /* (npmatch, apwordmax, 0:lmaxapw, natmtot) */
+  int32_t nstfv;           /* states requested */
+  double evaltol;          /* input%groundstate%solver%evaltol (ZHEGVX abstol) */
+} excfv_static;
+
+/* ---- lifetime ---------------------------------------------------------- */
+
+/* Creates a handle on CUDA device `device` with its own stream. */
+int excfv_create(int device, excfv_handle** out);
+/* Frees every device buffer of the handle. */
+int excfv_destroy(excfv_handle* h);
+/* Message for the last failure on the calling thread ("" if none). */
+const char* excfv_last_error(void);
+/* Precision form: EXCFV_PREC_FP64 (default) or EXCFV_PREC_MIXED. */
+int excfv_set_precision(excfv_handle* h, int prec);
+/* Stream used by the _dev entry points (cudaStream_t as void*; NULL = own). */
+int excfv_set_stream(excfv_handle* h, void* stream);
+/* Sizes the device workspace for matrices up to nmatmax and G+k sets up to
+ * ngkmax (the pooled workspace the reference allocates per call in
+ * newsystem, src/seceqnfv.f90:74).  Called implicitly when needed. */
+int excfv_reserve(excfv_handle* h, int32_t nmatmax, int32_t ngkmax);
+
+/* Uploads the per-SCF-iteration data (replaces module globals). */
+int excfv_set_static(excfv_handle* h, const excfv_static* s);
+
+/* ---- the hot path ------------------------------------------------------ */
+
+/* match (src/match.f90:13): APW matching coefficients.
+ * gpc(ngkmax), tpgpc(2,ngkmax), sfacgp complex(ngkmax,natmtot)
+ * -> apwalm complex(ngkmax, apwordmax, lmmaxapw, natmtot). */
+int excfv_match(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc,
+                const double* tpgpc, const double* sfacgp, double* apwalm);
+
+/* hamiltonandoverlapsetup (src/src_eigensystem/hamiltonandoverlapsetup.f90:8),
+ * with the semantics of hamiltonsetup + overlapsetup (hamiltonsetup.f90:8,
+ * overlapsetup.f90:8): H and O complex(nmatp, nmatp), both triangles filled
+ * (after hamiltonoverlapocopy_UL). */
+int excfv_hamiltonandoverlapsetup(excfv_handle* h, int32_t nmatp, int32_t ngp, int32_t ngkmax,
+                                  const double* apwalm, const int32_t* igpig,
+                                  const double* vgpc, double* hmat, double* omat);
+
+/* solvewithlapack (src/src_eigensystem/modfvsystem.f90:585): ZHEGVX(1,'V',
+ * 'I','U') for the lowest nstfv states of H x = e O x, reading the upper
+ * triangles of H and O (nmatp x nmatp, leading dimension nmatp).
+ * evalfv(nstfv), evecfv complex(ldevec, nstfv).  H and O are not modified. */
+int excfv_solvewithlapack(excfv_handle* h, int32_t nmatp, const double* hmat, const double* omat,
+                          int32_t nstfv, double evaltol, double* evalfv, double* evecfv,
+                          int32_t ldevec);
+
+/* seceqnfv (src/seceqnfv.f90:12): setup + solve for one k-point.
+ * igpig(ngkmax), vgpc(3,ngkmax), apwalm complex(ngkmax,apwordmax,lmmaxapw,natmtot)
+ * -> evalfv(nstfv), evecfv complex(nmatmax, nstfv) (rows > nmatp untouched).
+ * ispn and ik are accepted for interface parity; only one first-variational
+ * spin is supported (nspnfv = 1). */
+int excfv_seceqnfv(excfv_handle* h, int32_t ispn, int32_t ik, int32_t nmatp, int32_t ngp,
+                   int32_t ngkmax, const int32_t* igpig, const double* vgpc,
+                   const double* apwalm, int32_t nmatmax, double* evalfv, double* evecfv);
+
+/* seceqn body for one spin (src/seceqn.f90:57-64): match + seceqnfv, so that
+ * apwalm never leaves the device. */
+int excfv_seceqn(excfv_handle* h, int32_t ik, int32_t nmatp, int32_t ngp, int32_t ngkmax,
+                 const double* gpc, const double* tpgpc, const double* sfacgp,
+                 const int32_t* igpig, const double* vgpc, int32_t nmatmax,
+                 double* evalfv, double* evecfv);
+
+/* Device-pointer form of excfv_seceqn, on the handle's stream (asynchronous:
+ * the status is available after excfv_sync). */
+int excfv_seceqn_dev(excfv_handle* h, int32_t nmatp, int32_t ngp, int32_t ngkmax,
+                     const double* gpc, const double* tpgpc, const double* sfacgp,
+                     const int32_t* igpig, const double* vgpc, int32_t nmatmax,
+                     double* evalfv, double* evecfv);
+/* Waits for the handle's stream and returns the status of the last solve. */
+int excfv_sync(excfv_handle* h);
+
+/* Stage timings of the last host-entry call (seconds): [0] match,
+ * [1] setup (timemat), [2] eigensolve (timefv), [3] copies. */
+int excfv_get_timings(excfv_handle* h, double* t4);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EXCFV_H */
