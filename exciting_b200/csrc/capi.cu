@@ -5,6 +5,7 @@
 #include <cstring>
 #include <vector>
 #include <chrono>
+#include <atomic>
 
 #include "handle.cuh"
 
@@ -71,6 +72,41 @@ double now_s() {
 }
 
 }  // namespace
+
+static std::atomic<long long> g_launches{0};
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+void prof_begin(excfv_handle* h, int cls) {
+  Prof& p = h->prof;
+  if (!p.on) return;
+  auto& v = p.ev[cls];
+  while (v.size() < p.used[cls] + 2) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    v.push_back(e);
+  }
+  cudaEventRecord(v[p.used[cls]], h->stream);
+}
+
+void prof_end(excfv_handle* h, int cls) {
+  Prof& p = h->prof;
+  if (!p.on || p.ev[cls].size() < p.used[cls] + 2) return;
+  cudaEventRecord(p.ev[cls][p.used[cls] + 1], h->stream);
+  p.used[cls] += 2;
+}
+
+void prof_collect(excfv_handle* h) {
+  Prof& p = h->prof;
+  cudaStreamSynchronize(h->stream);
+  for (int c = 0; c < PROF_NCLS; ++c) {
+    for (size_t i = 0; i + 1 < p.used[c]; i += 2) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, p.ev[c][i], p.ev[c][i + 1]) == cudaSuccess) p.ms[c] += ms;
+      p.cnt[c] += 1;
+    }
+    p.used[c] = 0;
+  }
+}
 
 void excfv_set_error(const char* fmt, ...) {
   va_list ap;
@@ -349,6 +385,8 @@ int excfv_destroy(excfv_handle* h) {
   if (!h) return EXCFV_OK;
   DeviceGuard g(h->device);
   cudaStreamSynchronize(h->stream);
+  for (int c = 0; c < PROF_NCLS; ++c)
+    for (cudaEvent_t e : h->prof.ev[c]) cudaEventDestroy(e);
   free_workspace(h->ws);
   free_static(h->st);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -621,6 +659,30 @@ int excfv_sync(excfv_handle* h) {
   if (!h) return EXCFV_ERR_ARG;
   DeviceGuard g(h->device);
   return stage_status(h, 0);
+}
+
+long long excfv_launch_count(void) { return g_launches.load(); }
+
+int excfv_profile(excfv_handle* h, int enable) {
+  if (!h) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  prof_collect(h);
+  for (int c = 0; c < PROF_NCLS; ++c) { h->prof.ms[c] = 0.0; h->prof.cnt[c] = 0; }
+  h->prof.on = enable != 0;
+  return EXCFV_OK;
+}
+
+int excfv_profile_read(excfv_handle* h, double* ms, long long* count, int nclasses) {
+  if (!h || !ms || !count || nclasses < 0) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  prof_collect(h);
+  for (int c = 0; c < nclasses && c < PROF_NCLS; ++c) {
+    ms[c] = h->prof.ms[c];
+    count[c] = h->prof.cnt[c];
+    h->prof.ms[c] = 0.0;
+    h->prof.cnt[c] = 0;
+  }
+  return EXCFV_OK;
 }
 
 int excfv_get_timings(excfv_handle* h, double* t4) {

@@ -52,6 +52,8 @@ enum { ST_POTRF = 0, ST_BARRIER = 1, ST_STEIN = 2, ST_STEBZ = 3, ST_NWORDS = 8 }
   } while (0)
 
 void excfv_set_error(const char* fmt, ...);
+// process-wide count of kernel launches made by this library
+void count_launch(int n = 1);
 
 // ---------------------------------------------------------------------------
 // complex FP64 GEMM on the DMMA (mma.sync m8n8k4 f64) tensor path

@@ -1,6 +1,8 @@
 // Internal state of an excfv handle and the stage entry points.
 #pragma once
 
+#include <vector>
+
 #include "common.cuh"
 #include "../../include/excfv.h"
 
@@ -81,6 +83,22 @@ struct Workspace {
   size_t h_pinned_bytes = 0;
 };
 
+// Stage profiler: CUDA events around stages (or single launches) on the
+// handle's stream, enabled by excfv_profile().  Class ids match
+// EXCFV_PROF_* in include/excfv.h.
+enum {
+  PROF_MATCH = 0, PROF_SETUP_GEMM, PROF_SETUP_OTHER, PROF_POTRF, PROF_HEGST, PROF_TRD_PANEL,
+  PROF_TRD_UPDATE, PROF_STEIG, PROF_BACKTR, PROF_NCLS
+};
+
+struct Prof {
+  bool on = false;
+  std::vector<cudaEvent_t> ev[PROF_NCLS];  // begin/end pairs
+  size_t used[PROF_NCLS] = {};
+  double ms[PROF_NCLS] = {};
+  long long cnt[PROF_NCLS] = {};
+};
+
 struct excfv_handle {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -91,7 +109,12 @@ struct excfv_handle {
   Workspace ws;
   double timings[4] = {0, 0, 0, 0};
   int nsm = 148;
+  Prof prof;
 };
+
+void prof_begin(excfv_handle* h, int cls);
+void prof_end(excfv_handle* h, int cls);
+void prof_collect(excfv_handle* h);
 
 // ---- stages (each enqueues work on h->stream) ------------------------------
 int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax);

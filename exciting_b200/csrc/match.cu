@@ -385,7 +385,7 @@ int match_compute_zdinv(DevStatic& st, const double* d_sprwin, const double* d_a
   const int nt = st.natmtot * (st.lmaxapw + 1);
   k_zdinv<<<(nt + 127) / 128, 128, 0, s>>>(st.natmtot, st.lmaxapw, st.apwordmax, st.npmatch,
                                            st.idxis, st.apword, st.rmt, d_sprwin, d_apwfrwin,
-                                           st.zdinv);
+                                           st.zdinv); count_launch();
   CUDA_TRY(cudaGetLastError());
   return EXCFV_OK;
 }
@@ -396,14 +396,15 @@ int stage_match(excfv_handle* h, int ngp, int ngkmax, cplx* apwalm_ref) {
   cudaStream_t s = h->stream;
   if (st.lmaxapw > LMAX_CAP) return EXCFV_ERR_UNSUPPORTED;
   const double fpso = 4.0 * M_PI / sqrt(st.omega);
+  prof_begin(h, PROF_MATCH);
   k_ylm_bessel<<<(ngp + 127) / 128, 128, 0, s>>>(ngp, ws.ngkmax, st.lmaxapw, st.apwordmax,
                                                  st.nspecies, st.apword, st.rmt, ws.gpc,
-                                                 ws.tpgpc, ws.ylm, ws.djl);
+                                                 ws.tpgpc, ws.ylm, ws.djl); count_launch();
   CUDA_TRY(cudaGetLastError());
   const long long tot = (long long)st.natmtot * st.maxaa * ngp;
   k_apwalm_packed<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(
       ngp, ws.ngkmax, st.natmtot, st.maxaa, st.lmaxapw, st.apwordmax, st.idxis, st.flist, fpso,
-      ws.ylm, ws.djl, st.zdinv, ws.sfacgp, ws.Apk);
+      ws.ylm, ws.djl, st.zdinv, ws.sfacgp, ws.Apk); count_launch();
   CUDA_TRY(cudaGetLastError());
   if (apwalm_ref) {
     const long long tr = (long long)ngkmax * st.apwordmax * st.lmmaxapw * st.natmtot;
@@ -412,9 +413,10 @@ int stage_match(excfv_handle* h, int ngp, int ngkmax, cplx* apwalm_ref) {
     if (ngkmax != ws.ngkmax) return EXCFV_ERR_ARG;
     k_apwalm_ref<<<(unsigned)((tr + 255) / 256), 256, 0, s>>>(
         ngp, ngkmax, st.natmtot, st.lmaxapw, st.apwordmax, st.idxis, st.apword, fpso, ws.ylm,
-        ws.djl, st.zdinv, ws.sfacgp, apwalm_ref);
+        ws.djl, st.zdinv, ws.sfacgp, apwalm_ref); count_launch();
     CUDA_TRY(cudaGetLastError());
   }
+  prof_end(h, PROF_MATCH);
   return EXCFV_OK;
 }
 
@@ -423,7 +425,7 @@ int stage_pack_apwalm(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm) 
   const long long tot = (long long)st.natmtot * st.maxaa * ngp;
   k_pack<<<(unsigned)((tot + 255) / 256), 256, 0, h->stream>>>(ngp, ngkmax, st.natmtot, st.maxaa,
                                                                st.lmmaxapw, st.apwordmax, st.idxis,
-                                                               st.flist, apwalm, h->ws.Apk);
+                                                               st.flist, apwalm, h->ws.Apk); count_launch();
   CUDA_TRY(cudaGetLastError());
   return EXCFV_OK;
 }

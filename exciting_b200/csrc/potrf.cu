@@ -93,7 +93,7 @@ int potrf_upper(excfv_handle* h, int n, cplx* O, cplx* Ui, long long ld) {
   const cplx one = cmk(1.0, 0.0), mone = cmk(-1.0, 0.0);
   for (int kb = 0; kb < n; kb += NBP) {
     const int b = min(NBP, n - kb);
-    k_potrf_diag<<<1, PT, smem, s>>>(n, kb, O, ld, Ui, h->ws.status);
+    k_potrf_diag<<<1, PT, smem, s>>>(n, kb, O, ld, Ui, h->ws.status); count_launch();
     CUDA_TRY(cudaGetLastError());
     const int rest = n - kb - b;
     if (rest <= 0) break;

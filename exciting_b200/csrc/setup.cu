@@ -182,7 +182,7 @@ __global__ void k_mirror_upper(int n, cplx* M, long long ld) {
 
 int mirror_upper(cudaStream_t s, int n, cplx* M, long long ld) {
   dim3 grid((n + 31) / 32, (n + 31) / 32);
-  k_mirror_upper<<<grid, dim3(32, 8), 0, s>>>(n, M, ld);
+  k_mirror_upper<<<grid, dim3(32, 8), 0, s>>>(n, M, ld); count_launch();
   CUDA_TRY(cudaGetLastError());
   return EXCFV_OK;
 }
@@ -204,37 +204,44 @@ int stage_setup(excfv_handle* h, int nmatp, int ngp, bool mirror_o) {
   z.B = ws.Apk; z.ldb = AM; z.strideB = st.maxaa;
   z.C = ws.Zpk; z.ldc = AM; z.strideC = st.maxaa;
   z.batch = st.natmtot; z.uplo_c = TRI_NONE; z.tri_a = TRI_NONE; z.tri_b = TRI_NONE;
+  prof_begin(h, PROF_SETUP_OTHER);
   if ((rc = zgemm(s, OP_N, OP_N, z))) return rc;
+  prof_end(h, PROF_SETUP_OTHER);
   CUDA_TRY(cudaGetLastError());
   // H_GG = sum_a A_a^H Z_a (hamiltonsetup.f90:90-103), upper triangle
+  prof_begin(h, PROF_SETUP_GEMM);
   if ((rc = zgemm1(s, OP_C, OP_N, N, N, (int)AM, one, ws.Apk, AM, ws.Zpk, AM, zero, ws.H, ld,
                    TRI_UPPER)))
     return rc;
+  prof_end(h, PROF_SETUP_GEMM);
   // O_GG = sum_a A_a^H (I + H1) A_a (overlapsetup.f90:82-108), upper triangle
   const cplx* rhs = ws.Apk;
   if (st.have_h1aa) {
     const long long tot = AM * N;
     k_apply_h1<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(
         N, st.natmtot, st.maxaa, st.apwordmax, st.lmaxapw, st.idxis, st.flist, st.fofl,
-        st.lmmaxapw, st.h1aa, ws.Apk, ws.Zpk);
+        st.lmmaxapw, st.h1aa, ws.Apk, ws.Zpk); count_launch();
     CUDA_TRY(cudaGetLastError());
     rhs = ws.Zpk;
   }
+  prof_begin(h, PROF_SETUP_GEMM);
   if ((rc = zgemm1(s, OP_C, OP_N, N, N, (int)AM, one, ws.Apk, AM, rhs, AM, zero, ws.O, ld,
                    TRI_UPPER)))
     return rc;
+  prof_end(h, PROF_SETUP_GEMM);
   CUDA_TRY(cudaGetLastError());
+  prof_begin(h, PROF_SETUP_OTHER);
   // local-orbital band (columns N..n-1)
   if (n > N) {
     dim3 grid((n + 127) / 128, n - N);
     k_lo_band<<<grid, 128, 0, s>>>(N, n, st.natmtot, st.maxaa, st.maxnlo, st.nlomax, st.apwordmax,
                                    st.idxis, st.lo_atom, st.lo_local, st.lo_lm, st.lo_ilo,
                                    st.fofl, st.lmmaxapw, ws.Apk, st.loa, st.lolo, st.oalo,
-                                   st.ololo, ws.H, ws.O, ld);
+                                   st.ololo, ws.H, ws.O, ld); count_launch();
     CUDA_TRY(cudaGetLastError());
   }
   // interstitial
-  k_gk_iv<<<(N + 127) / 128, 128, 0, s>>>(N, ws.igpig, st.ivg, ws.gk_iv);
+  k_gk_iv<<<(N + 127) / 128, 128, 0, s>>>(N, ws.igpig, st.ivg, ws.gk_iv); count_launch();
   CUDA_TRY(cudaGetLastError());
   {
     const int e1 = st.intgv[3] - st.intgv[0] + 1;
@@ -244,10 +251,11 @@ int stage_setup(excfv_handle* h, int nmatp, int ngp, bool mirror_o) {
     k_interstitial<<<grid, dim3(32, 8), 0, s>>>(N, ws.gk_iv, ws.vgpc, st.intgv[0], st.intgv[1],
                                                 st.intgv[2], e1, e2, e3, st.ivgig, st.ngvec,
                                                 st.veffig, st.xig, st.cfunig, st.m2effig, st.h1on,
-                                                ws.H, ws.O, ld);
+                                                ws.H, ws.O, ld); count_launch();
     CUDA_TRY(cudaGetLastError());
   }
   if ((rc = mirror_upper(s, n, ws.H, ld))) return rc;
   if (mirror_o && (rc = mirror_upper(s, n, ws.O, ld))) return rc;
+  prof_end(h, PROF_SETUP_OTHER);
   return EXCFV_OK;
 }

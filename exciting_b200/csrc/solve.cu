@@ -102,7 +102,7 @@ int apply_q(excfv_handle* h, int n, int k, const cplx* C, long long ld, cplx* Z,
   cudaStream_t s = h->stream;
   if (n < 2) return EXCFV_OK;
   const int nblk = (n - 1 + NBQ - 1) / NBQ;
-  k_larft<<<nblk, LT, 0, s>>>(n, C, ld, ws.tau, ws.Tf);
+  k_larft<<<nblk, LT, 0, s>>>(n, C, ld, ws.tau, ws.Tf); count_launch();
   CUDA_TRY(cudaGetLastError());
   const cplx one = cmk(1.0, 0.0), mone = cmk(-1.0, 0.0), zero = cmk(0.0, 0.0);
   cplx* X1 = ws.Xs;
@@ -155,8 +155,11 @@ int stage_solve(excfv_handle* h, int n, int k, double evaltol, double* d_eval, c
   if (k > ws.kmax) return EXCFV_ERR_ARG;
   CUDA_TRY(cudaMemsetAsync(ws.status, 0, ST_NWORDS * sizeof(int), s));
   // O = U^H U, Ui = U^-1
+  prof_begin(h, PROF_POTRF);
   if ((rc = potrf_upper(h, n, ws.O, ws.Ui, ld))) return rc;
   if ((rc = trtri_upper(h, n, ws.O, ws.Ui, ld, ws.T))) return rc;
+  prof_end(h, PROF_POTRF);
+  prof_begin(h, PROF_HEGST);
   // C = Ui^H H Ui (upper), then both triangles
   if ((rc = zgemm1(s, OP_N, OP_N, n, n, n, one, ws.H, ld, ws.Ui, ld, zero, ws.T, ld, TRI_NONE,
                    TRI_NONE, TRI_UPPER)))
@@ -165,20 +168,25 @@ int stage_solve(excfv_handle* h, int n, int k, double evaltol, double* d_eval, c
                    TRI_LOWER, TRI_NONE)))
     return rc;
   if ((rc = mirror_upper(s, n, ws.H, ld))) return rc;
+  prof_end(h, PROF_HEGST);
   // tridiagonal reduction
   if ((rc = tridiag_reduce(h, n, ws.H, ld))) return rc;
   // eigenpairs of T
   cplx* Z = ws.Z;
+  prof_begin(h, PROF_STEIG);
   if ((rc = tridiag_eig(h, n, k, evaltol, ws.d, ws.e, ws.w, Z, ld, ws.stein_ws, ws.icl)))
     return rc;
+  prof_end(h, PROF_STEIG);
+  prof_begin(h, PROF_BACKTR);
   if ((rc = cholqr(h, n, k, Z, ld))) return rc;
   // back-transforms
   if ((rc = apply_q(h, n, k, ws.H, ld, Z, ld))) return rc;
   if ((rc = zgemm1(s, OP_N, OP_N, n, k, n, one, ws.Ui, ld, Z, ld, zero, d_evec, ldevec, TRI_NONE,
                    TRI_UPPER, TRI_NONE)))
     return rc;
+  prof_end(h, PROF_BACKTR);
   ws.Z = Z;  // cholqr may have swapped the buffers
-  k_copy_eval<<<(k + 127) / 128, 128, 0, s>>>(k, ws.w, d_eval);
+  k_copy_eval<<<(k + 127) / 128, 128, 0, s>>>(k, ws.w, d_eval); count_launch();
   CUDA_TRY(cudaGetLastError());
   return EXCFV_OK;
 }

@@ -263,16 +263,16 @@ int tridiag_eig(excfv_handle* h, int n, int k, double abstol, const double* d, c
   double* uf = ub + (size_t)n * k;
   double* um = uf + (size_t)n * k;
   double* Yi = um + (size_t)n * k;
-  k_tridiag_prep<<<1, 256, 0, s>>>(n, d, e, e2, scal);
+  k_tridiag_prep<<<1, 256, 0, s>>>(n, d, e, e2, scal); count_launch();
   CUDA_TRY(cudaGetLastError());
-  k_stebz<<<(k * 32 + 127) / 128, 128, 0, s>>>(n, d, e2, scal, k, abstol, w, h->ws.status);
+  k_stebz<<<(k * 32 + 127) / 128, 128, 0, s>>>(n, d, e2, scal, k, abstol, w, h->ws.status); count_launch();
   CUDA_TRY(cudaGetLastError());
-  k_clusters<<<(k + 127) / 128, 128, 0, s>>>(k, w, scal, iscratch);
+  k_clusters<<<(k + 127) / 128, 128, 0, s>>>(k, w, scal, iscratch); count_launch();
   CUDA_TRY(cudaGetLastError());
   k_stein<<<(k + 63) / 64, 64, 0, s>>>(n, d, e, scal, k, w, iscratch, ua, ub, uf, um, Yi,
-                                       h->ws.status);
+                                       h->ws.status); count_launch();
   CUDA_TRY(cudaGetLastError());
-  k_y_to_z<<<dim3((n + 255) / 256, k), 256, 0, s>>>(n, k, Yi, Z, ldz);
+  k_y_to_z<<<dim3((n + 255) / 256, k), 256, 0, s>>>(n, k, Yi, Z, ldz); count_launch();
   CUDA_TRY(cudaGetLastError());
   return EXCFV_OK;
 }

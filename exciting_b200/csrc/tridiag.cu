@@ -397,7 +397,7 @@ int tridiag_reduce(excfv_handle* h, int n, cplx* C, long long ld) {
   Workspace& ws = h->ws;
   cudaStream_t s = h->stream;
   if (n == 1) {
-    k_tail_scalar<<<1, 32, 0, s>>>(n, C, ld, ws.d);
+    k_tail_scalar<<<1, 32, 0, s>>>(n, C, ld, ws.d); count_launch();
     CUDA_TRY(cudaGetLastError());
     return EXCFV_OK;
   }
@@ -420,8 +420,12 @@ int tridiag_reduce(excfv_handle* h, int n, cplx* C, long long ld) {
     ta.red = ws.red; ta.bar = ws.bar; ta.status = ws.status;
     ta.p = p; ta.nbp = nbp; ta.final_panel = final_panel;
     void* args[] = {&ta};
+    prof_begin(h, PROF_TRD_PANEL);
     CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_tridiag_panel, dim3(G), dim3(TT), args, 0, s));
+    count_launch();
+    prof_end(h, PROF_TRD_PANEL);
     if (!final_panel) {
+      prof_begin(h, PROF_TRD_UPDATE);
       const int q = p + nbp;
       const int m2 = n - q;
       cplx* V2 = C + q + ld * p;
@@ -431,6 +435,7 @@ int tridiag_reduce(excfv_handle* h, int n, cplx* C, long long ld) {
       if (rc) return rc;
       rc = zgemm1(s, OP_N, OP_C, m2, m2, nbp, mone, W2, ld, V2, ld, one, C22, ld);
       if (rc) return rc;
+      prof_end(h, PROF_TRD_UPDATE);
     }
   }
   return EXCFV_OK;

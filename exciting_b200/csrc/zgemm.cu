@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(ZgemmArgs p) {
 template <int OPA, int OPB>
 int launch(cudaStream_t s, const ZgemmArgs& a) {
   dim3 grid((a.m + BM - 1) / BM, (a.n + BN - 1) / BN, a.batch);
-  zgemm_kernel<OPA, OPB><<<grid, NT, 0, s>>>(a);
+  zgemm_kernel<OPA, OPB><<<grid, NT, 0, s>>>(a); count_launch();
   return 0;
 }
 

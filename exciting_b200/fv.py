@@ -244,6 +244,19 @@ class FirstVariational:
     def sync(self, n: int = 0) -> None:
         self._check(self._L.excfv_sync(self._h), "excfv_sync", n)
 
+    def profile(self, enable: bool = True) -> None:
+        self._check(self._L.excfv_profile(self._h, int(enable)), "excfv_profile")
+
+    def profile_read(self) -> dict:
+        n = len(_lib.PROF_CLASSES)
+        ms = np.zeros(n)
+        cnt = np.zeros(n, dtype=np.int64)
+        self._check(self._L.excfv_profile_read(self._h, _ptr(ms), _ptr(cnt), n), "excfv_profile_read")
+        return {c: (float(ms[i]), int(cnt[i])) for i, c in enumerate(_lib.PROF_CLASSES)}
+
+    def launch_count(self) -> int:
+        return int(self._L.excfv_launch_count())
+
     def timings(self):
         t = np.zeros(4)
         self._L.excfv_get_timings(self._h, _ptr(t))

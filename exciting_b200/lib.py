@@ -76,7 +76,13 @@ SIGNATURES = {
                                    C.c_void_p, C.c_void_p]),
     "excfv_sync": (C.c_int, [C.c_void_p]),
     "excfv_get_timings": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "excfv_profile": (C.c_int, [C.c_void_p, C.c_int]),
+    "excfv_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "excfv_launch_count": (C.c_longlong, []),
 }
+
+PROF_CLASSES = ["match", "setup_gemm", "setup_other", "potrf", "hegst", "trd_panel",
+                "trd_update", "steig", "backtr"]
 
 _lib: Optional[C.CDLL] = None
 

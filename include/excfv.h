@@ -179,6 +179,27 @@ int excfv_sync(excfv_handle* h);
  * [1] setup (timemat), [2] eigensolve (timefv), [3] copies. */
 int excfv_get_timings(excfv_handle* h, double* t4);
 
+/* Kernel profiling (the device-side counterpart of the reference's timemat /
+ * timefv accumulators, src/mod_timing.F90:13-56).  When enabled, CUDA events
+ * bracket each stage on the handle's stream; excfv_profile_read waits for the
+ * stream and returns, per class, the accumulated milliseconds and the number
+ * of bracketed intervals since the last read (then resets them). */
+#define EXCFV_PROF_MATCH 0       /* Y_lm, Bessel, matching coefficients      */
+#define EXCFV_PROF_SETUP_GEMM 1  /* A^H (aa A), A^H A contractions (launches) */
+#define EXCFV_PROF_SETUP_OTHER 2 /* LO band, interstitial, mirror            */
+#define EXCFV_PROF_POTRF 3       /* Cholesky + inverse factor                */
+#define EXCFV_PROF_HEGST 4       /* U^-H H U^-1                              */
+#define EXCFV_PROF_TRD_PANEL 5   /* tridiagonal panel kernels (launches)     */
+#define EXCFV_PROF_TRD_UPDATE 6  /* trailing rank-2k updates                 */
+#define EXCFV_PROF_STEIG 7       /* bisection + inverse iteration            */
+#define EXCFV_PROF_BACKTR 8      /* orthonormalisation + back-transforms     */
+#define EXCFV_PROF_NCLS 9
+int excfv_profile(excfv_handle* h, int enable);
+int excfv_profile_read(excfv_handle* h, double* ms, long long* count, int nclasses);
+
+/* Number of kernels this library has launched in the process so far. */
+long long excfv_launch_count(void);
+
 #ifdef __cplusplus
 }
 #endif
