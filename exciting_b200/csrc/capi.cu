@@ -129,7 +129,8 @@ void free_workspace(Workspace& ws) {
   dfree(ws.tpgpc); dfree(ws.sfacgp); dfree(ws.gk_iv); dfree(ws.d); dfree(ws.e); dfree(ws.tau);
   dfree(ws.Wp); dfree(ws.red); dfree(ws.w); dfree(ws.stein_ws); dfree(ws.icl); dfree(ws.ybuf);
   dfree(ws.Z); dfree(ws.Z2); dfree(ws.Gk); dfree(ws.Gki); dfree(ws.Tf); dfree(ws.Xs);
-  dfree(ws.status); dfree(ws.bar);
+  dfree(ws.status); dfree(ws.bar); dfree(ws.part);
+  ws.part_cap = 0;
   ws.nmatmax = ws.ngkmax = ws.kmax = 0;
 }
 
@@ -327,16 +328,18 @@ int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax) {
       (rc = dalloc(&ws.sfacgp, (size_t)ngkmax * st.natmtot)) ||
       (rc = dalloc(&ws.gk_iv, (size_t)3 * ngkmax)) || (rc = dalloc(&ws.d, n)) ||
       (rc = dalloc(&ws.e, n)) || (rc = dalloc(&ws.tau, n)) ||
-      (rc = dalloc(&ws.Wp, n * tridiag_nb())) ||
+      (rc = dalloc(&ws.Wp, n * 4 * tridiag_nb())) ||
       (rc = dalloc(&ws.red, (size_t)tridiag_workspace_doubles())) || (rc = dalloc(&ws.w, n)) ||
       (rc = dalloc(&ws.stein_ws, tridiag_eig_scratch_doubles((int)n, (int)K))) ||
       (rc = dalloc(&ws.icl, K)) || (rc = dalloc(&ws.ybuf, 2 * n)) || (rc = dalloc(&ws.Z, n * K)) ||
       (rc = dalloc(&ws.Z2, n * K)) || (rc = dalloc(&ws.Gk, K * K)) || (rc = dalloc(&ws.Gki, K * K)) ||
-      (rc = dalloc(&ws.Tf, ((n + 31) / 32 + 1) * 32 * 32)) || (rc = dalloc(&ws.Xs, 2 * 32 * K)) ||
-      (rc = dalloc(&ws.status, (size_t)ST_NWORDS)) || (rc = dalloc(&ws.bar, (size_t)4))) {
+      (rc = dalloc(&ws.Tf, 2 * ((n + 63) / 64 + 1) * 64 * 64)) || (rc = dalloc(&ws.Xs, 2 * 64 * K)) ||
+      (rc = dalloc(&ws.status, (size_t)ST_NWORDS)) || (rc = dalloc(&ws.bar, (size_t)4)) ||
+      (rc = dalloc(&ws.part, std::max((size_t)(8u << 20), n * 64 * 4)))) {
     free_workspace(ws);
     return rc;
   }
+  ws.part_cap = std::max((size_t)(8u << 20), n * 64 * 4);
   CUDA_TRY(cudaMemset(ws.status, 0, ST_NWORDS * sizeof(int)));
   CUDA_TRY(cudaMemset(ws.bar, 0, 4 * sizeof(unsigned)));
   ws.nmatmax = (int)nmatmax;

@@ -73,7 +73,25 @@ struct ZgemmArgs {
   // in the other triangle are treated as zero (never loaded) and whole
   // k-tiles outside the triangle are skipped.
   int uplo_c, tri_a, tri_b;
+  // split-K: the K range of every tile is cut into splitk pieces whose
+  // partial products go to part (splitk * batch * m * n) and are summed in a
+  // fixed order by a second kernel (deterministic).  Set by zgemm().
+  int splitk;
+  cplx* part;
+  // batch z uses K = k - kdec * z (0 = the same K for every batch entry)
+  int kdec;
 };
+
+// Scratch for split-K partial products, owned by the calling handle and made
+// current for the calling thread by the entry points (a handle is used by one
+// thread at a time).
+struct GemmCtx {
+  cplx* ws = nullptr;
+  size_t cap = 0;  // complex elements
+  int nsm = 148;
+};
+void gemm_ctx_set(const GemmCtx& c);
+const GemmCtx& gemm_ctx();
 
 int zgemm(cudaStream_t s, int opA, int opB, const ZgemmArgs& a);
 

@@ -76,6 +76,8 @@ struct Workspace {
   cplx* Gki = nullptr;      // kmax x kmax inverse factor
   cplx* Tf = nullptr;       // block reflector factors
   cplx* Xs = nullptr;       // scratch nb x kmax
+  cplx* part = nullptr;     // split-K partial products
+  size_t part_cap = 0;      // complex elements
   int* status = nullptr;    // ST_NWORDS
   unsigned int* bar = nullptr;  // grid barrier words
   // host staging
@@ -111,6 +113,15 @@ struct excfv_handle {
   int nsm = 148;
   Prof prof;
 };
+
+// makes the handle's split-K scratch current for this thread's GEMMs
+inline void bind_gemm_ctx(excfv_handle* h) {
+  GemmCtx c;
+  c.ws = h->ws.part;
+  c.cap = h->ws.part_cap;
+  c.nsm = h->nsm;
+  gemm_ctx_set(c);
+}
 
 void prof_begin(excfv_handle* h, int cls);
 void prof_end(excfv_handle* h, int cls);

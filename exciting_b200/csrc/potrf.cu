@@ -15,67 +15,117 @@
 namespace {
 
 constexpr int NBP = 64;
-constexpr int PT = 256;
 
-__global__ void __launch_bounds__(PT) k_potrf_diag(int n, int kb, cplx* O, long long ld, cplx* Ui,
-                                                   int* status) {
-  extern __shared__ cplx sm[];
-  cplx* A = sm;                  // b x b, column-major, ld NBP
-  cplx* X = sm + NBP * NBP;      // inverse
-  __shared__ int fail;
+// One CTA of 32 x 32 threads factors the b x b diagonal block (b <= 64) and
+// inverts the factor, as a 2 x 2 block recursion on 32 x 32 blocks held in
+// shared memory (thread (r, c) owns element (r, c) of a 32-block):
+//   U11 = chol(A11), X11 = U11^-1, U12 = X11^H A12, A22 -= U12^H U12,
+//   U22 = chol(A22), X22 = U22^-1, X12 = -X11 U12 X22.
+// FP64 vector throughput bounds this kernel, so the work is laid out such
+// that whole warps (one row each) drop out of every elimination step.
+// Rows/columns past b are padded with the identity.
+constexpr int LDB = 65;
+
+__device__ __forceinline__ bool chol32(cplx* A, double* rinv, int o, int tr, int tc, int* s_fail, int fail_base) {
+  // A is the 64 x LDB shared block; factor A(o:o+32, o:o+32) in place (upper)
+  if (tr == 0 && tc == 0) {
+    const double a = A[o * LDB + o].x;
+    rinv[o] = (a > 0.0) ? 1.0 / sqrt(a) : 0.0;
+    if (!(a > 0.0)) *s_fail = fail_base + 1;
+  }
+  __syncthreads();
+  for (int j = 0; j < 32; ++j) {
+    if (*s_fail) return false;
+    if (tr == j && tc >= j) A[(o + j) * LDB + o + tc] = cscale(A[(o + j) * LDB + o + tc], rinv[o + j]);
+    __syncthreads();
+    if (tr > j && tc >= tr) {
+      cplx* x = &A[(o + tr) * LDB + o + tc];
+      *x = csub(*x, cmulc(A[(o + j) * LDB + o + tr], A[(o + j) * LDB + o + tc]));
+      if (tr == j + 1 && tc == j + 1) {
+        const double a = x->x;
+        rinv[o + j + 1] = (a > 0.0) ? 1.0 / sqrt(a) : 0.0;
+        if (!(a > 0.0)) *s_fail = fail_base + j + 2;
+      }
+    }
+    __syncthreads();
+  }
+  return true;
+}
+
+// X(o:o+32, o:o+32) = inverse of the upper factor U(o:o+32, o:o+32)
+__device__ __forceinline__ void inv32(const cplx* A, cplx* X, const double* rinv, int o, int tr, int tc) {
+  X[(o + tr) * LDB + o + tc] = cmk(tr == tc ? 1.0 : 0.0, 0.0);
+  __syncthreads();
+  for (int i = 31; i >= 0; --i) {
+    if (tr == i && tc >= i) X[(o + i) * LDB + o + tc] = cscale(X[(o + i) * LDB + o + tc], rinv[o + i]);
+    __syncthreads();
+    if (tr < i && tc >= i)
+      X[(o + tr) * LDB + o + tc] = csub(X[(o + tr) * LDB + o + tc],
+                                        cmul(A[(o + tr) * LDB + o + i], X[(o + i) * LDB + o + tc]));
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_potrf_diag(int n, int kb, cplx* O, long long ld, cplx* Ui,
+                                                     int* status) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  cplx* A = reinterpret_cast<cplx*>(dsm);   // 64 x LDB, row-major [r][c]
+  cplx* X = A + NBP * LDB;
+  __shared__ double rinv[NBP];
+  __shared__ int s_fail;
   if (status[ST_POTRF] != 0) return;
   const int b = min(NBP, n - kb);
-  const int tid = threadIdx.x;
-  for (int t = tid; t < b * b; t += PT) {
-    const int r = t % b, c = t / b;
-    A[r + NBP * c] = (r <= c) ? O[(kb + r) + ld * (kb + c)] : cmk(0.0, 0.0);
-    X[r + NBP * c] = cmk(r == c ? 1.0 : 0.0, 0.0);
+  const int tc = threadIdx.x & 31, tr = threadIdx.x >> 5;
+  for (int t = threadIdx.x; t < NBP * NBP; t += 1024) {
+    const int r = t % NBP, c = t / NBP;  // coalesced along r
+    cplx a = cmk(r == c ? 1.0 : 0.0, 0.0);
+    if (r < b && c < b && r <= c) a = O[(kb + r) + ld * (kb + c)];
+    A[r * LDB + c] = a;
+    X[r * LDB + c] = cmk(0.0, 0.0);
   }
-  if (tid == 0) fail = 0;
+  if (threadIdx.x == 0) s_fail = 0;
   __syncthreads();
-  // right-looking unblocked Cholesky on the upper triangle
-  for (int j = 0; j < b; ++j) {
-    const double ajj = A[j + NBP * j].x;
-    if (!(ajj > 0.0)) {  // also catches NaN
-      if (tid == 0) { fail = j + 1; }
-      __syncthreads();
-      break;
-    }
-    const double ujj = sqrt(ajj);
-    const double inv = 1.0 / ujj;
-    __syncthreads();
-    for (int c = j + 1 + tid; c < b; c += PT) A[j + NBP * c] = cscale(A[j + NBP * c], inv);
-    if (tid == 0) A[j + NBP * j] = cmk(ujj, 0.0);
-    __syncthreads();
-    // trailing: A(r, c) -= conj(U(j, r)) U(j, c), j < r <= c
-    const int m = b - j - 1;
-    for (int t = tid; t < m * m; t += PT) {
-      const int r = j + 1 + t % m, c = j + 1 + t / m;
-      if (r <= c) A[r + NBP * c] = csub(A[r + NBP * c], cmulc(A[j + NBP * r], A[j + NBP * c]));
-    }
-    __syncthreads();
-  }
-  if (fail) {
-    if (tid == 0) atomicCAS(&status[ST_POTRF], 0, kb + fail);
+  if (!chol32(A, rinv, 0, tr, tc, &s_fail, 0)) {
+    if (threadIdx.x == 0 && s_fail <= b) atomicCAS(&status[ST_POTRF], 0, kb + s_fail);
     return;
   }
-  // X = U^-1 by backward elimination on [U | I]: for i = b-1..0:
-  // row i of X /= U(i,i); rows r < i: X(r,:) -= U(r,i) X(i,:)
-  for (int i = b - 1; i >= 0; --i) {
-    const double uii = A[i + NBP * i].x;
-    for (int c = i + tid; c < b; c += PT) X[i + NBP * c] = cscale(X[i + NBP * c], 1.0 / uii);
+  inv32(A, X, rinv, 0, tr, tc);
+  // U12 = X11^H A12 (thread (r, c): column 32 + c)
+  {
+    cplx acc = cmk(0.0, 0.0);
+    for (int k = 0; k <= tr; ++k) acc = cadd(acc, cmulc(X[k * LDB + tr], A[k * LDB + 32 + tc]));
     __syncthreads();
-    for (int t = tid; t < i * (b - i); t += PT) {
-      const int r = t % i, c = i + t / i;
-      X[r + NBP * c] = csub(X[r + NBP * c], cmul(A[r + NBP * i], X[i + NBP * c]));
-    }
+    A[tr * LDB + 32 + tc] = acc;
     __syncthreads();
   }
-  for (int t = tid; t < b * b; t += PT) {
-    const int r = t % b, c = t / b;
-    if (r <= c) {
-      O[(kb + r) + ld * (kb + c)] = A[r + NBP * c];
-      Ui[(kb + r) + ld * (kb + c)] = X[r + NBP * c];
+  // A22 -= U12^H U12 (upper)
+  if (tc >= tr) {
+    cplx acc = cmk(0.0, 0.0);
+    for (int k = 0; k < 32; ++k) acc = cadd(acc, cmulc(A[k * LDB + 32 + tr], A[k * LDB + 32 + tc]));
+    A[(32 + tr) * LDB + 32 + tc] = csub(A[(32 + tr) * LDB + 32 + tc], acc);
+  }
+  __syncthreads();
+  if (!chol32(A, rinv, 32, tr, tc, &s_fail, 32)) {
+    if (threadIdx.x == 0 && s_fail <= b) atomicCAS(&status[ST_POTRF], 0, kb + s_fail);
+    return;
+  }
+  inv32(A, X, rinv, 32, tr, tc);
+  // X12 = -X11 (U12 X22): T = U12 X22 into X's lower-left block, then X12
+  {
+    cplx acc = cmk(0.0, 0.0);
+    for (int k = 0; k <= tc; ++k) acc = cadd(acc, cmul(A[tr * LDB + 32 + k], X[(32 + k) * LDB + 32 + tc]));
+    X[(32 + tr) * LDB + tc] = acc;  // scratch: lower-left block of X
+    __syncthreads();
+    cplx acc2 = cmk(0.0, 0.0);
+    for (int k = tr; k < 32; ++k) acc2 = cadd(acc2, cmul(X[tr * LDB + k], X[(32 + k) * LDB + tc]));
+    X[tr * LDB + 32 + tc] = cmk(-acc2.x, -acc2.y);
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < NBP * NBP; t += 1024) {
+    const int r = t % NBP, c = t / NBP;
+    if (r < b && c < b && r <= c) {
+      O[(kb + r) + ld * (kb + c)] = A[r * LDB + c];
+      Ui[(kb + r) + ld * (kb + c)] = X[r * LDB + c];
     }
   }
 }
@@ -84,16 +134,12 @@ __global__ void __launch_bounds__(PT) k_potrf_diag(int n, int kb, cplx* O, long 
 
 int potrf_upper(excfv_handle* h, int n, cplx* O, cplx* Ui, long long ld) {
   cudaStream_t s = h->stream;
-  const size_t smem = 2 * NBP * NBP * sizeof(cplx);
-  static bool attr = false;
-  if (!attr) {
-    CUDA_TRY(cudaFuncSetAttribute(k_potrf_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
   const cplx one = cmk(1.0, 0.0), mone = cmk(-1.0, 0.0);
+  const int smem = (int)(2 * sizeof(cplx) * NBP * LDB);
+  CUDA_TRY(cudaFuncSetAttribute(k_potrf_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   for (int kb = 0; kb < n; kb += NBP) {
     const int b = min(NBP, n - kb);
-    k_potrf_diag<<<1, PT, smem, s>>>(n, kb, O, ld, Ui, h->ws.status); count_launch();
+    k_potrf_diag<<<1, 1024, smem, s>>>(n, kb, O, ld, Ui, h->ws.status); count_launch();
     CUDA_TRY(cudaGetLastError());
     const int rest = n - kb - b;
     if (rest <= 0) break;

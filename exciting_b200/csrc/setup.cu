@@ -196,6 +196,7 @@ int stage_setup(excfv_handle* h, int nmatp, int ngp, bool mirror_o) {
   const long long AM = (long long)st.natmtot * st.maxaa;
   const cplx one = cmk(1.0, 0.0), zero = cmk(0.0, 0.0);
   int rc;
+  bind_gemm_ctx(h);
 
   // Z_a = aa_a * A_a for every atom (hamiltonsetup.f90:75-88)
   ZgemmArgs z;
@@ -204,6 +205,7 @@ int stage_setup(excfv_handle* h, int nmatp, int ngp, bool mirror_o) {
   z.B = ws.Apk; z.ldb = AM; z.strideB = st.maxaa;
   z.C = ws.Zpk; z.ldc = AM; z.strideC = st.maxaa;
   z.batch = st.natmtot; z.uplo_c = TRI_NONE; z.tri_a = TRI_NONE; z.tri_b = TRI_NONE;
+  z.splitk = 1; z.part = nullptr; z.kdec = 0;
   prof_begin(h, PROF_SETUP_OTHER);
   if ((rc = zgemm(s, OP_N, OP_N, z))) return rc;
   prof_end(h, PROF_SETUP_OTHER);

@@ -21,72 +21,48 @@ int mirror_upper(cudaStream_t s, int n, cplx* M, long long ld);
 
 namespace {
 
-constexpr int NBQ = 32;  // reflectors per block (= panel width of the reduction)
+constexpr int NBQ = 64;  // reflectors per block of the back-transform
 constexpr int LT = 256;
 
 // Triangular factor of the block reflector H_p ... H_{p+nb-1} = I - V T V^H
-// (forward, columnwise; the ZLARFT recurrence T(0:i,i) = -tau_i T(0:i,0:i) V^H v_i).
-// One CTA per block.  V(r, j) = C(p+1+r, p+j) for r >= j (unit entry stored).
-__global__ void __launch_bounds__(LT) k_larft(int n, const cplx* C, long long ld, const cplx* tau,
-                                              cplx* Tf) {
-  __shared__ cplx VT[32][NBQ + 1];   // row chunk of V, then the triangular factor
-  __shared__ cplx G[NBQ][NBQ + 1];
-  auto& Vs = VT;
-  auto& Ts = VT;
+// (forward, columnwise: T(i,i) = tau_i, T(0:i,i) = -tau_i T(0:i,0:i) G(0:i,i)
+// with G = V^H V from a batched GEMM).  One CTA per block; G and T live in
+// shared memory, four threads share each row of the triangular product.
+__global__ void __launch_bounds__(LT) k_larft(int n, const cplx* Gall, const cplx* tau, cplx* Tf) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  cplx (*G)[NBQ + 1] = reinterpret_cast<cplx (*)[NBQ + 1]>(dsm);
+  cplx (*T)[NBQ + 1] = reinterpret_cast<cplx (*)[NBQ + 1]>(dsm + sizeof(cplx) * NBQ * (NBQ + 1));
   const int blk = blockIdx.x;
   const int p = blk * NBQ;
   const int nb = min(NBQ, n - 1 - p);
   if (nb <= 0) return;
-  const int m = n - p - 1;
   const int tid = threadIdx.x;
-  // each thread owns 4 entries (a, b) of the 32x32 Gram matrix
-  cplx acc[4];
-  int ea[4], eb[4];
-#pragma unroll
-  for (int u = 0; u < 4; ++u) {
-    const int id = tid + u * LT;
-    ea[u] = id % NBQ;
-    eb[u] = id / NBQ;
-    acc[u] = cmk(0.0, 0.0);
+  const cplx* Gb = Gall + (size_t)blk * NBQ * NBQ;
+  for (int t = tid; t < NBQ * NBQ; t += LT) {
+    const int r = t % NBQ, c = t / NBQ;
+    G[r][c] = Gb[t];
+    T[r][c] = cmk(0.0, 0.0);
   }
-  for (int r0 = 0; r0 < m; r0 += 32) {
-    __syncthreads();
-    for (int t = tid; t < 32 * NBQ; t += LT) {
-      const int rr = t % 32, j = t / 32;
-      const int r = r0 + rr;
-      cplx v = cmk(0.0, 0.0);
-      if (r < m && j < nb && r >= j) v = C[(p + 1 + r) + ld * (p + j)];
-      Vs[rr][j] = v;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int a = ea[u], b = eb[u];
-      for (int rr = 0; rr < 32; ++rr) acc[u] = cadd(acc[u], cmulc(Vs[rr][a], Vs[rr][b]));
-    }
-  }
-#pragma unroll
-  for (int u = 0; u < 4; ++u) G[ea[u]][eb[u]] = acc[u];
   __syncthreads();
-  for (int t = tid; t < NBQ * NBQ; t += LT) Ts[t % NBQ][t / NBQ] = cmk(0.0, 0.0);
+  if (tid == 0) T[0][0] = tau[p];
   __syncthreads();
-  if (tid == 0) Ts[0][0] = tau[p];
-  __syncthreads();
+  const int row = tid >> 2, sub = tid & 3;
   for (int i = 1; i < nb; ++i) {
     const cplx ti = tau[p + i];
     cplx val = cmk(0.0, 0.0);
-    if (tid < i) {
-      // sum_{q=tid}^{i-1} T(tid, q) G(q, i)
-      for (int q = tid; q < i; ++q) val = cadd(val, cmul(Ts[tid][q], G[q][i]));
-      val = cmul(cmk(-ti.x, -ti.y), val);
-    }
+    if (row < i)
+      for (int q = row + sub; q < i; q += 4) val = cadd(val, cmul(T[row][q], G[q][i]));
+    val.x += __shfl_xor_sync(0xffffffffu, val.x, 1);
+    val.y += __shfl_xor_sync(0xffffffffu, val.y, 1);
+    val.x += __shfl_xor_sync(0xffffffffu, val.x, 2);
+    val.y += __shfl_xor_sync(0xffffffffu, val.y, 2);
     __syncthreads();
-    if (tid < i) Ts[tid][i] = val;
-    if (tid == 0) Ts[i][i] = ti;
+    if (row < i && sub == 0) T[row][i] = cmul(cmk(-ti.x, -ti.y), val);
+    if (tid == 0) T[i][i] = ti;
     __syncthreads();
   }
   cplx* out = Tf + (size_t)blk * NBQ * NBQ;
-  for (int t = tid; t < NBQ * NBQ; t += LT) out[t] = Ts[t % NBQ][t / NBQ];
+  for (int t = tid; t < NBQ * NBQ; t += LT) out[t] = T[t % NBQ][t / NBQ];
 }
 
 __global__ void k_copy_eval(int k, const double* w, double* out) {
@@ -102,9 +78,35 @@ int apply_q(excfv_handle* h, int n, int k, const cplx* C, long long ld, cplx* Z,
   cudaStream_t s = h->stream;
   if (n < 2) return EXCFV_OK;
   const int nblk = (n - 1 + NBQ - 1) / NBQ;
-  k_larft<<<nblk, LT, 0, s>>>(n, C, ld, ws.tau, ws.Tf); count_launch();
-  CUDA_TRY(cudaGetLastError());
   const cplx one = cmk(1.0, 0.0), mone = cmk(-1.0, 0.0), zero = cmk(0.0, 0.0);
+  cplx* Gall = ws.Tf + (size_t)nblk * NBQ * NBQ;
+  // Gram matrices G_b = V_b^H V_b: the full blocks in one batched GEMM
+  // (K shrinks by NBQ from block to block), the last partial block alone.
+  const int nfull = (n - 1) / NBQ;
+  if (nfull > 0) {
+    ZgemmArgs g;
+    g.m = NBQ; g.n = NBQ; g.k = n - 1; g.kdec = NBQ;
+    g.alpha = one; g.beta = zero;
+    g.A = C + 1; g.lda = ld; g.strideA = (long long)NBQ * (ld + 1);
+    g.B = C + 1; g.ldb = ld; g.strideB = (long long)NBQ * (ld + 1);
+    g.C = Gall; g.ldc = NBQ; g.strideC = (long long)NBQ * NBQ;
+    g.batch = nfull; g.uplo_c = TRI_UPPER; g.tri_a = TRI_UPPER; g.tri_b = TRI_LOWER;
+    g.splitk = 1; g.part = nullptr;
+    int rc = zgemm(s, OP_C, OP_N, g);
+    if (rc) return rc;
+  }
+  if (nfull < nblk) {
+    const int p = nfull * NBQ;
+    const int nb = n - 1 - p, m = n - p - 1;
+    const cplx* V = C + (p + 1) + ld * p;
+    int rc = zgemm1(s, OP_C, OP_N, nb, nb, m, one, V, ld, V, ld, zero, Gall + (size_t)nfull * NBQ * NBQ,
+                    NBQ, TRI_UPPER, TRI_UPPER, TRI_LOWER);
+    if (rc) return rc;
+  }
+  const int smem = (int)(2 * sizeof(cplx) * NBQ * (NBQ + 1));
+  CUDA_TRY(cudaFuncSetAttribute(k_larft, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_larft<<<nblk, LT, smem, s>>>(n, Gall, ws.tau, ws.Tf); count_launch();
+  CUDA_TRY(cudaGetLastError());
   cplx* X1 = ws.Xs;
   cplx* X2 = ws.Xs + (size_t)NBQ * ws.kmax;
   for (int b = nblk - 1; b >= 0; --b) {
@@ -152,6 +154,7 @@ int stage_solve(excfv_handle* h, int n, int k, double evaltol, double* d_eval, c
   const cplx one = cmk(1.0, 0.0), zero = cmk(0.0, 0.0);
   int rc;
   if (k < 1 || k > n) return EXCFV_ERR_ARG;
+  bind_gemm_ctx(h);
   if (k > ws.kmax) return EXCFV_ERR_ARG;
   CUDA_TRY(cudaMemsetAsync(ws.status, 0, ST_NWORDS * sizeof(int), s));
   // O = U^H U, Ui = U^-1

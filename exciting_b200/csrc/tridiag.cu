@@ -3,8 +3,8 @@
 //
 // Blocked in panels of NBT columns (the zlatrd/zher2k split of LAPACK's
 // blocked ZHETRD, restated): one persistent cooperative kernel reduces the
-// NBT columns of a panel, then two GEMMs apply the rank-2*NBT update
-// C22 -= V W^H + W V^H to the trailing matrix.  Inside the panel kernel every
+// NBT columns of a panel, then one GEMM applies the rank-2*NBT update
+// C22 -= [V W] [W V]^H to the trailing matrix.  Inside the panel kernel every
 // column costs two grid-wide barriers:
 //
 //   phase 1 (row owners)  finish W(:, i-1); update column c with the panel's
@@ -19,9 +19,11 @@
 //                         from the reduced scalars, so the row of W needed by the
 //                         next column is recomputed locally instead of synced.
 //
-// Rows are owned in chunks of 64 (four threads per row).  All loads of data
-// written by other CTAs inside the kernel use ld.global.cg (L2), since L1 is
-// not coherent across SMs.  Barrier waits are bounded in time; a timeout sets
+// Rows are owned in chunks of 64 (four threads per row); a CTA keeps the
+// panel's V and W rows of the rows it owns in shared memory, so the row
+// phases touch global memory once per row.  All loads of data written by
+// other CTAs inside the kernel use ld.global.cg (L2), since L1 is not
+// coherent across SMs.  Barrier waits are bounded in time; a timeout sets
 // status[ST_BARRIER] and every CTA then leaves the kernel.
 #include "handle.cuh"
 
@@ -30,7 +32,14 @@ namespace {
 constexpr int NBT = 32;
 constexpr int TT = 256;
 constexpr int RCH = 64;
+constexpr int MAXCH = 2;  // row chunks per CTA held in shared memory
 constexpr long long BARRIER_NS = 2000000000LL;  // 2 s
+
+struct PanelSmem {
+  cplx V[MAXCH][NBT][RCH];
+  cplx W[MAXCH][NBT][RCH];
+  cplx X[MAXCH][RCH];
+};
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   unsigned v;
@@ -45,36 +54,30 @@ __device__ __forceinline__ long long gtimer() {
 __device__ __forceinline__ cplx ldc(const cplx* p) { return __ldcg(p); }
 __device__ __forceinline__ double ldd(const double* p) { return __ldcg(p); }
 
-// Returns false when the barrier timed out (here or earlier in any CTA).
-__device__ bool grid_barrier(unsigned* bar, int* status) {
+// Grid barrier on a monotonic arrival counter (zeroed before each launch):
+// barrier number e completes when the counter reaches e * gridDim.x.
+// Returns false when it timed out (here or in another CTA).
+__device__ bool grid_barrier(unsigned* bar, unsigned& epoch, int* status) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    if (atomicAdd(&status[ST_BARRIER], 0) != 0) {
-      ok = 0;
-    } else {
-      const unsigned gen = ld_acquire(&bar[1]);
-      __threadfence();
-      const unsigned arrived = atomicAdd(&bar[0], 1u);
-      if (arrived == gridDim.x - 1) {
-        atomicExch(&bar[0], 0u);
-        __threadfence();
-        atomicAdd(&bar[1], 1u);
-      } else {
-        const long long t0 = gtimer();
-        unsigned it = 0;
-        while (ld_acquire(&bar[1]) == gen) {
-          if ((++it & 63u) == 0) {
-            if (gtimer() - t0 > BARRIER_NS || atomicAdd(&status[ST_BARRIER], 0) != 0) {
-              atomicAdd(&status[ST_BARRIER], 1);
-              ok = 0;
-              break;
-            }
+    epoch += 1;
+    const unsigned target = epoch * gridDim.x;
+    // release this CTA's writes and arrive (no return value needed)
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
+    if (ld_acquire(&bar[0]) < target) {
+      const long long t0 = gtimer();
+      unsigned it = 0;
+      while (ld_acquire(&bar[0]) < target) {
+        if ((++it & 255u) == 0) {
+          if (*(volatile int*)&status[ST_BARRIER] != 0 || gtimer() - t0 > BARRIER_NS) {
+            atomicAdd(&status[ST_BARRIER], 1);
+            ok = 0;
+            break;
           }
         }
       }
-      __threadfence();
     }
     s_ok = ok;
   }
@@ -86,7 +89,8 @@ struct TridArgs {
   int n;
   long long ld;
   cplx* C;
-  cplx* W;       // n x NBT, leading dimension ld
+  cplx* VW;      // n x 2NBT: [V | W] of the panel (leading dimension ld)
+  cplx* WV;      // n x 2NBT: [W | V]
   double* d;
   double* e;
   cplx* tau;
@@ -105,19 +109,37 @@ __device__ __forceinline__ cplx shfl4_sum(cplx v) {
   return v;
 }
 
+// a * conj(b)
+__device__ __forceinline__ cplx cmul_cb(cplx a, cplx b) {
+  return cmk(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+__device__ __forceinline__ cplx warp_sum(cplx v) {
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+  }
+  return v;
+}
+
+constexpr int JB = 8;  // column tiles whose x values are staged per round trip
+
 __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs a) {
-  __shared__ cplx s_vc[NBT], s_wc[NBT];   // row c of V and W
-  __shared__ cplx s_sv[NBT], s_tv[NBT];   // V^H v, W^H v of the previous column
+  extern __shared__ __align__(16) unsigned char dsm[];
+  PanelSmem& S = *reinterpret_cast<PanelSmem*>(dsm);
+  __shared__ cplx s_vc[NBT], s_wc[NBT];   // row c+1 of V and W
+  __shared__ cplx s_sv[NBT], s_tv[NBT];   // V^H v, W^H v of the current column
   __shared__ cplx s_acc_s[NBT], s_acc_t[NBT];
-  __shared__ cplx s_v[64];
+  __shared__ cplx s_x[JB * 64];           // staged x values of the trailing column
+  __shared__ cplx s_xr[64];               // x values of the item's rows
   __shared__ cplx s_part[TT];
   __shared__ double s_dred[TT / 32];
-  __shared__ double s_scal[8];            // tau.re, tau.im, scale.re, scale.im, alpha, beta
+  __shared__ double s_scal[8];            // tau.re, tau.im, scale.re, scale.im, alpha, beta, vav, y(c+1)
+  __shared__ cplx s_y1;
 
   const int n = a.n;
   const long long ld = a.ld;
   cplx* __restrict__ C = a.C;
-  cplx* __restrict__ W = a.W;
   const int tid = threadIdx.x, bid = blockIdx.x, G = gridDim.x;
   const int rsub = tid & 3, rloc = tid >> 2;
   const int lane = tid & 31, warp = tid >> 5;
@@ -125,259 +147,331 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs a) {
   double* red_vav = a.red + NBT;
   double* red_s = a.red + 3 * NBT;
   double* red_t = a.red + 3 * NBT + 2 * NBT * NBT;
+  const int nch = (n + RCH - 1) / RCH;
+  unsigned epoch = 0;
 
-  cplx tau_prev = cmk(0.0, 0.0);
-  double alpha_prev = 0.0;
-
-  for (int i = 0; i <= a.nbp; ++i) {
-    const int c = a.p + i;
-    const bool last = (i == a.nbp);
-    cplx* yprev = a.ybuf + (size_t)((i + 1) & 1) * n;   // y of column i-1
-    cplx* ycur = a.ybuf + (size_t)(i & 1) * n;
-
-    // ---------------- phase 1 ----------------
-    if (tid < i) {
-      const int j = tid;
-      s_vc[j] = (j == i - 1) ? cmk(1.0, 0.0) : ldc(C + c + ld * (a.p + j));
-      if (j < i - 1) s_wc[j] = ldc(W + c + ld * j);
-    }
-    __syncthreads();
-    if (i > 0 && tid == 0) {
-      // W(c, i-1) = tau (y(c) - V(c,:) t - W(c,:) s) + alpha v(c), v(c) = 1
-      cplx acc = cmk(0.0, 0.0);
-      for (int j = 0; j < i - 1; ++j) {
-        acc = cadd(acc, cmul(s_vc[j], s_tv[j]));
-        acc = cadd(acc, cmul(s_wc[j], s_sv[j]));
-      }
-      const cplx y = ldc(yprev + c);
-      cplx w = cmul(tau_prev, csub(y, acc));
-      w.x += alpha_prev;
-      s_wc[i - 1] = w;
-    }
-    __syncthreads();
+  // ---- prologue: column p needs no update; its norm and diagonal
+  {
+    const int c = a.p;
     double nrm_part = 0.0;
-    const bool do_update = (!last) || a.final_panel;
-    for (int q = bid; q * RCH < n; q += G) {
+    for (int ch = 0; ch < MAXCH; ++ch) {
+      const int q = bid + ch * G;
+      if (q >= nch) break;
       const int r = q * RCH + rloc;
-      const bool act = (r >= c) && (r < n);
-      cplx wnew = cmk(0.0, 0.0), vprev = cmk(0.0, 0.0);
-      if (i > 0) {
-        cplx acc = cmk(0.0, 0.0);
-        if (act)
-          for (int j = rsub; j < i - 1; j += 4) {
-            acc = cadd(acc, cmul(ldc(C + r + ld * (a.p + j)), s_tv[j]));
-            acc = cadd(acc, cmul(ldc(W + r + ld * j), s_sv[j]));
-          }
-        acc = shfl4_sum(acc);
-        if (act) {
-          vprev = (r == c) ? cmk(1.0, 0.0) : ldc(C + r + ld * (c - 1));
-          const cplx y = ldc(yprev + r);
-          wnew = cmul(tau_prev, csub(y, acc));
-          wnew = cadd(wnew, cscale(vprev, alpha_prev));
-          if (rsub == 0) W[r + ld * (i - 1)] = wnew;
-        }
-      }
-      if (do_update) {
-        cplx acc = cmk(0.0, 0.0);
-        if (act)
-          for (int j = rsub; j < i; j += 4) {
-            const cplx vr = (j == i - 1) ? vprev : ldc(C + r + ld * (a.p + j));
-            const cplx wr = (j == i - 1) ? wnew : ldc(W + r + ld * j);
-            acc = cadd(acc, cmk(vr.x * s_wc[j].x + vr.y * s_wc[j].y, vr.y * s_wc[j].x - vr.x * s_wc[j].y));
-            acc = cadd(acc, cmk(wr.x * s_vc[j].x + wr.y * s_vc[j].y, wr.y * s_vc[j].x - wr.x * s_vc[j].y));
-          }
-        acc = shfl4_sum(acc);
-        if (act && rsub == 0) {
-          cplx x = csub(ldc(C + r + ld * c), acc);
-          if (r == c) {
-            x.y = 0.0;
-            a.d[c] = x.x;
-          }
+      if (rsub == 0 && r >= c && r < n) {
+        cplx x = ldc(C + r + ld * c);
+        if (r == c) {
+          x.y = 0.0;
+          a.d[c] = x.x;
           C[r + ld * c] = x;
-          if (r >= c + 2) nrm_part += cabs2(x);
         }
+        S.X[ch][rloc] = x;
+        if (r >= c + 2) nrm_part += cabs2(x);
+        a.ybuf[r] = cmk(0.0, 0.0);
       }
-      if (i == 0 && act && rsub == 0) ycur[r] = cmk(0.0, 0.0);
     }
-    if (last) break;
-    // block reduction of the norm
     for (int o = 16; o > 0; o >>= 1) nrm_part += __shfl_xor_sync(0xffffffffu, nrm_part, o);
     if (lane == 0) s_dred[warp] = nrm_part;
     __syncthreads();
     if (tid == 0) {
       double sacc = 0.0;
       for (int w = 0; w < TT / 32; ++w) sacc += s_dred[w];
-      if (sacc != 0.0) atomicAdd(&red_norm[i], sacc);
+      if (sacc != 0.0) atomicAdd(&red_norm[0], sacc);
     }
-    if (!grid_barrier(a.bar, a.status)) return;
+  }
 
-    // ---------------- phase 2 ----------------
-    if (tid == 0) {
-      const cplx alpha = ldc(C + (c + 1) + ld * c);
-      const double xn2 = ldd(red_norm + i);
-      double tr = 0.0, ti = 0.0, scr = 0.0, sci = 0.0, beta;
-      if (xn2 == 0.0 && alpha.y == 0.0) {
-        beta = alpha.x;
-      } else {
-        const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
-        beta = (alpha.x >= 0.0) ? -nrm : nrm;
-        tr = (beta - alpha.x) / beta;
-        ti = -alpha.y / beta;
-        // scale = 1 / (alpha - beta)
-        const double dr = alpha.x - beta, di = alpha.y;
-        const double den = dr * dr + di * di;
-        scr = dr / den;
-        sci = -di / den;
-      }
-      s_scal[0] = tr; s_scal[1] = ti; s_scal[2] = scr; s_scal[3] = sci; s_scal[5] = beta;
-    }
+  for (int i = 0; i < a.nbp; ++i) {
+    const int c = a.p + i;
+    cplx* ycur = a.ybuf + (size_t)(i & 1) * n;
+    cplx* ynext = a.ybuf + (size_t)((i + 1) & 1) * n;
+    if (!grid_barrier(a.bar, epoch, a.status)) return;
+
+    // ================= phase 2: reflector of column c, y = C22 v =================
+    // y = C22 v with v(c+1) = 1, v(j) = scale x(j): accumulate C22 x~ (x~(c+1) = 0)
+    // and the column c+1 separately, so the loads do not wait for the reflector.
+    const int r0g = c + 1;
+    const int m2 = n - r0g;
+    const int nt = (m2 + 63) / 64;
+    int Sg = G / nt;
+    if (Sg < 1) Sg = 1;
+    if (Sg > nt) Sg = nt;
+    const int per = (nt + Sg - 1) / Sg;
+    const int items = nt * Sg;
+    const int rr = tid & 63, cg = tid >> 6;
+    double vav_re = 0.0, vav_im = 0.0;
+    bool have_scal = false;
     if (tid < NBT) { s_acc_s[tid] = cmk(0.0, 0.0); s_acc_t[tid] = cmk(0.0, 0.0); }
-    __syncthreads();
+    for (int it = bid; it < items || !have_scal; it += G) {
+      const bool real_item = it < items;
+      const int I = it / Sg, seg = it % Sg;
+      const int r = r0g + I * 64 + rr;
+      const int Jb = seg * per, Je = real_item ? min(nt, Jb + per) : Jb;
+      cplx acc = cmk(0.0, 0.0), acc1 = cmk(0.0, 0.0);
+      for (int J0 = Jb; J0 < Je || (J0 == Jb && !have_scal); J0 += JB) {
+        const int J1 = min(Je, J0 + JB);
+        // stage x values of tiles J0..J1-1 (and of the item's rows on the first chunk)
+        cplx xv0 = cmk(0.0, 0.0), xv1 = cmk(0.0, 0.0), xrow = cmk(0.0, 0.0);
+        {
+          const int j_a = r0g + J0 * 64 + tid, j_b = j_a + TT;
+          const int lim = r0g + J1 * 64;
+          if (j_a < lim && j_a < n && j_a != c + 1) xv0 = ldc(C + j_a + ld * c);
+          if (j_b < lim && j_b < n && j_b != c + 1) xv1 = ldc(C + j_b + ld * c);
+          if (J0 == Jb && tid < 64 && real_item) {
+            const int rr2 = r0g + I * 64 + tid;
+            if (rr2 < n && rr2 != c + 1) xrow = ldc(C + rr2 + ld * c);
+          }
+        }
+        if (!have_scal && tid == 0) {
+          const cplx alpha = ldc(C + (c + 1) + ld * c);
+          const double xn2 = ldd(red_norm + i);
+          double tr = 0.0, ti = 0.0, scr = 0.0, sci = 0.0, beta;
+          if (xn2 == 0.0 && alpha.y == 0.0) {
+            beta = alpha.x;
+          } else {
+            const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
+            beta = (alpha.x >= 0.0) ? -nrm : nrm;
+            tr = (beta - alpha.x) / beta;
+            ti = -alpha.y / beta;
+            const double dr = alpha.x - beta, di = alpha.y;  // scale = 1 / (alpha - beta)
+            const double den = dr * dr + di * di;
+            scr = dr / den;
+            sci = -di / den;
+          }
+          s_scal[0] = tr; s_scal[1] = ti; s_scal[2] = scr; s_scal[3] = sci; s_scal[5] = beta;
+        }
+        __syncthreads();
+        s_x[tid] = xv0;
+        s_x[tid + TT] = xv1;
+        if (J0 == Jb && tid < 64) s_xr[tid] = xrow;
+        __syncthreads();
+        have_scal = true;
+        if (r < n && real_item) {
+          for (int J = J0; J < J1; ++J) {
+            const int j0 = r0g + J * 64;
+            const int jmax = min(16, n - (j0 + cg * 16));
+            const cplx* col = C + r + ld * (j0 + cg * 16);
+            const cplx* xs = s_x + (J - J0) * 64 + cg * 16;
+            if (jmax == 16) {
+              cplx xl[16];
+#pragma unroll
+              for (int jj = 0; jj < 16; ++jj) xl[jj] = ldc(col + ld * jj);
+#pragma unroll
+              for (int jj = 0; jj < 16; ++jj) {
+                const cplx v = xs[jj];
+                acc.x += xl[jj].x * v.x - xl[jj].y * v.y;
+                acc.y += xl[jj].x * v.y + xl[jj].y * v.x;
+              }
+              if (J == 0 && cg == 0) acc1 = xl[0];
+            } else {
+              for (int jj = 0; jj < jmax; ++jj) {
+                const cplx x = ldc(col + ld * jj);
+                const cplx v = xs[jj];
+                acc.x += x.x * v.x - x.y * v.y;
+                acc.y += x.x * v.y + x.y * v.x;
+                if (J == 0 && cg == 0 && jj == 0) acc1 = x;
+              }
+            }
+          }
+        }
+        if (J1 >= Je) break;
+      }
+      if (!real_item) break;
+      const cplx scale = cmk(s_scal[2], s_scal[3]);
+      __syncthreads();
+      s_part[tid] = cadd(cmul(scale, acc), acc1);
+      __syncthreads();
+      if (tid < 64 && r < n) {
+        cplx sum = cadd(cadd(s_part[tid], s_part[tid + 64]), cadd(s_part[tid + 128], s_part[tid + 192]));
+        atomicAdd(&ycur[r].x, sum.x);
+        atomicAdd(&ycur[r].y, sum.y);
+        const cplx vr = (r == c + 1) ? cmk(1.0, 0.0) : cmul(s_xr[tid], scale);
+        vav_re += vr.x * sum.x + vr.y * sum.y;  // conj(v_r) * sum
+        vav_im += vr.x * sum.y - vr.y * sum.x;
+      }
+    }
     const cplx scale = cmk(s_scal[2], s_scal[3]);
+    for (int o = 16; o > 0; o >>= 1) {
+      vav_re += __shfl_xor_sync(0xffffffffu, vav_re, o);
+      vav_im += __shfl_xor_sync(0xffffffffu, vav_im, o);
+    }
+    __syncthreads();
+    if (lane == 0) { s_part[warp].x = vav_re; s_part[warp].y = vav_im; }
     // own rows: clear y of the next column, V^H v and W^H v partials
     {
       cplx ps[NBT / 4], pt[NBT / 4];
 #pragma unroll
       for (int u = 0; u < NBT / 4; ++u) { ps[u] = cmk(0.0, 0.0); pt[u] = cmk(0.0, 0.0); }
-      for (int q = bid; q * RCH < n; q += G) {
+      for (int ch = 0; ch < MAXCH; ++ch) {
+        const int q = bid + ch * G;
+        if (q >= nch) break;
         const int r = q * RCH + rloc;
         if (r >= c + 1 && r < n) {
-          if (rsub == 0) yprev[r] = cmk(0.0, 0.0);
-          const cplx vr = (r == c + 1) ? cmk(1.0, 0.0) : cmul(ldc(C + r + ld * c), scale);
+          if (rsub == 0) ynext[r] = cmk(0.0, 0.0);
+          if (i > 0) {
+            const cplx vr = (r == c + 1) ? cmk(1.0, 0.0) : cmul(S.X[ch][rloc], scale);
 #pragma unroll
-          for (int u = 0; u < NBT / 4; ++u) {
-            const int j = rsub + 4 * u;
-            if (j < i) {
-              ps[u] = cadd(ps[u], cmulc(ldc(C + r + ld * (a.p + j)), vr));
-              pt[u] = cadd(pt[u], cmulc(ldc(W + r + ld * j), vr));
+            for (int u = 0; u < NBT / 4; ++u) {
+              const int j = rsub + 4 * u;
+              if (j < i) {
+                ps[u] = cadd(ps[u], cmulc(S.V[ch][j][rloc], vr));
+                pt[u] = cadd(pt[u], cmulc(S.W[ch][j][rloc], vr));
+              }
             }
           }
         }
       }
-      // reduce lanes with the same rsub inside the warp, then across warps
-#pragma unroll
-      for (int u = 0; u < NBT / 4; ++u) {
-        for (int o = 4; o < 32; o <<= 1) {
-          ps[u].x += __shfl_xor_sync(0xffffffffu, ps[u].x, o);
-          ps[u].y += __shfl_xor_sync(0xffffffffu, ps[u].y, o);
-          pt[u].x += __shfl_xor_sync(0xffffffffu, pt[u].x, o);
-          pt[u].y += __shfl_xor_sync(0xffffffffu, pt[u].y, o);
-        }
-      }
-      if (lane < 4) {
+      if (i > 0) {
 #pragma unroll
         for (int u = 0; u < NBT / 4; ++u) {
-          const int j = lane + 4 * u;
-          if (j < i) {
-            atomicAdd(&s_acc_s[j].x, ps[u].x);
-            atomicAdd(&s_acc_s[j].y, ps[u].y);
-            atomicAdd(&s_acc_t[j].x, pt[u].x);
-            atomicAdd(&s_acc_t[j].y, pt[u].y);
+          for (int o = 4; o < 32; o <<= 1) {
+            ps[u].x += __shfl_xor_sync(0xffffffffu, ps[u].x, o);
+            ps[u].y += __shfl_xor_sync(0xffffffffu, ps[u].y, o);
+            pt[u].x += __shfl_xor_sync(0xffffffffu, pt[u].x, o);
+            pt[u].y += __shfl_xor_sync(0xffffffffu, pt[u].y, o);
           }
         }
-      }
-      __syncthreads();
-      if (tid < i) {
-        atomicAdd(&red_s[2 * (NBT * i + tid)], s_acc_s[tid].x);
-        atomicAdd(&red_s[2 * (NBT * i + tid) + 1], s_acc_s[tid].y);
-        atomicAdd(&red_t[2 * (NBT * i + tid)], s_acc_t[tid].x);
-        atomicAdd(&red_t[2 * (NBT * i + tid) + 1], s_acc_t[tid].y);
-      }
-    }
-    // y = C22 v on the trailing block [c+1, n)^2
-    {
-      const int r0g = c + 1;
-      const int m2 = n - r0g;
-      const int nt = (m2 + 63) / 64;
-      int S = G / nt;
-      if (S < 1) S = 1;
-      if (S > nt) S = nt;
-      const int per = (nt + S - 1) / S;
-      const int items = nt * S;
-      const int rr = tid & 63, cg = tid >> 6;
-      double vav_re = 0.0, vav_im = 0.0;
-      for (int it = bid; it < items; it += G) {
-        const int I = it / S, seg = it % S;
-        const int r = r0g + I * 64 + rr;
-        cplx acc = cmk(0.0, 0.0);
-        const int Jb = seg * per, Je = min(nt, Jb + per);
-        for (int J = Jb; J < Je; ++J) {
-          const int j0 = r0g + J * 64;
-          __syncthreads();
-          if (tid < 64) {
-            const int j = j0 + tid;
-            cplx v = cmk(0.0, 0.0);
-            if (j < n) v = (j == c + 1) ? cmk(1.0, 0.0) : cmul(ldc(C + j + ld * c), scale);
-            s_v[tid] = v;
-          }
-          __syncthreads();
-          if (r < n) {
-            const int jmax = min(16, n - (j0 + cg * 16));
-            const cplx* col = C + r + ld * (j0 + cg * 16);
-#pragma unroll 4
-            for (int jj = 0; jj < jmax; ++jj) {
-              const cplx x = ldc(col + ld * jj);
-              const cplx v = s_v[cg * 16 + jj];
-              acc.x += x.x * v.x - x.y * v.y;
-              acc.y += x.x * v.y + x.y * v.x;
+        if (lane < 4) {
+#pragma unroll
+          for (int u = 0; u < NBT / 4; ++u) {
+            const int j = lane + 4 * u;
+            if (j < i) {
+              atomicAdd(&s_acc_s[j].x, ps[u].x);
+              atomicAdd(&s_acc_s[j].y, ps[u].y);
+              atomicAdd(&s_acc_t[j].x, pt[u].x);
+              atomicAdd(&s_acc_t[j].y, pt[u].y);
             }
           }
         }
-        __syncthreads();
-        s_part[tid] = acc;
-        __syncthreads();
-        if (tid < 64 && r < n) {
-          cplx sum = cadd(cadd(s_part[tid], s_part[tid + 64]), cadd(s_part[tid + 128], s_part[tid + 192]));
-          atomicAdd(&ycur[r].x, sum.x);
-          atomicAdd(&ycur[r].y, sum.y);
-          const cplx vr = (r == c + 1) ? cmk(1.0, 0.0) : cmul(ldc(C + r + ld * c), scale);
-          // conj(v_r) * sum
-          vav_re += vr.x * sum.x + vr.y * sum.y;
-          vav_im += vr.x * sum.y - vr.y * sum.x;
+      }
+    }
+    __syncthreads();
+    if (tid < i) {
+      atomicAdd(&red_s[2 * (NBT * i + tid)], s_acc_s[tid].x);
+      atomicAdd(&red_s[2 * (NBT * i + tid) + 1], s_acc_s[tid].y);
+      atomicAdd(&red_t[2 * (NBT * i + tid)], s_acc_t[tid].x);
+      atomicAdd(&red_t[2 * (NBT * i + tid) + 1], s_acc_t[tid].y);
+    }
+    if (tid == 32) {
+      double sr = 0.0, si = 0.0;
+      for (int w = 0; w < TT / 32; ++w) { sr += s_part[w].x; si += s_part[w].y; }
+      if (sr != 0.0) atomicAdd(&red_vav[2 * i], sr);
+      if (si != 0.0) atomicAdd(&red_vav[2 * i + 1], si);
+    }
+    if (!grid_barrier(a.bar, epoch, a.status)) return;
+
+    // ========== phase 3 (finish column c) merged with phase 1 (column c+1) ==========
+    const bool upd = (i + 1 < a.nbp) || a.final_panel;  // column c+1 is updated here
+    const int c1 = c + 1;
+    // one round of independent loads
+    if (warp == 0) {
+      if (lane < i) {
+        s_sv[lane] = cmk(ldd(red_s + 2 * (NBT * i + lane)), ldd(red_s + 2 * (NBT * i + lane) + 1));
+        s_tv[lane] = cmk(ldd(red_t + 2 * (NBT * i + lane)), ldd(red_t + 2 * (NBT * i + lane) + 1));
+      }
+      if (lane == 31) s_scal[6] = ldd(red_vav + 2 * i);
+    } else if (warp == 1) {
+      if (lane < i) s_vc[lane] = ldc(a.VW + c1 + ld * lane);
+      if (lane == i) s_vc[i] = cmk(1.0, 0.0);
+    } else if (warp == 2) {
+      if (lane < i) s_wc[lane] = ldc(a.VW + c1 + ld * (NBT + lane));
+      if (lane == 31) s_y1 = ldc(ycur + c1);
+    }
+    cplx yr[MAXCH], cn[MAXCH];
+    for (int ch = 0; ch < MAXCH; ++ch) {
+      yr[ch] = cmk(0.0, 0.0);
+      cn[ch] = cmk(0.0, 0.0);
+      const int q = bid + ch * G;
+      if (q >= nch) break;
+      const int r = q * RCH + rloc;
+      if (r >= c1 && r < n) {
+        yr[ch] = ldc(ycur + r);
+        if (upd && rsub == 0) cn[ch] = ldc(C + r + ld * c1);
+      }
+    }
+    __syncthreads();
+    const cplx tau = cmk(s_scal[0], s_scal[1]);
+    if (warp == 0) {
+      // alpha = -1/2 |tau|^2 (v^H C v - 2 Re(t^H s))
+      double ts = (lane < i) ? s_tv[lane].x * s_sv[lane].x + s_tv[lane].y * s_sv[lane].y : 0.0;
+      for (int o = 16; o > 0; o >>= 1) ts += __shfl_xor_sync(0xffffffffu, ts, o);
+      const double alpha = -0.5 * (tau.x * tau.x + tau.y * tau.y) * (s_scal[6] - 2.0 * ts);
+      // W(c+1, i) = tau (y(c+1) - V(c+1,:) t - W(c+1,:) s) + alpha v(c+1), v(c+1) = 1
+      cplx t = cmk(0.0, 0.0);
+      if (lane < i) t = cadd(cmul(s_vc[lane], s_tv[lane]), cmul(s_wc[lane], s_sv[lane]));
+      t = warp_sum(t);
+      if (lane == 0) {
+        s_scal[4] = alpha;
+        cplx w = cmul(tau, csub(s_y1, t));
+        w.x += alpha;
+        s_wc[i] = w;
+        if (bid == 0) {
+          a.e[c] = s_scal[5];
+          a.tau[c] = tau;
         }
       }
-      for (int o = 16; o > 0; o >>= 1) {
-        vav_re += __shfl_xor_sync(0xffffffffu, vav_re, o);
-        vav_im += __shfl_xor_sync(0xffffffffu, vav_im, o);
+    }
+    __syncthreads();
+    const double alpha = s_scal[4];
+    double nrm_part = 0.0;
+    for (int ch = 0; ch < MAXCH; ++ch) {
+      const int q = bid + ch * G;
+      if (q >= nch) break;
+      const int r = q * RCH + rloc;
+      const bool act = (r >= c1) && (r < n);
+      cplx vr = cmk(0.0, 0.0), wr = cmk(0.0, 0.0);
+      cplx acc = cmk(0.0, 0.0);
+      if (act) {
+        vr = (r == c1) ? cmk(1.0, 0.0) : cmul(S.X[ch][rloc], scale);
+        for (int j = rsub; j < i; j += 4) {
+          acc = cadd(acc, cmul(S.V[ch][j][rloc], s_tv[j]));
+          acc = cadd(acc, cmul(S.W[ch][j][rloc], s_sv[j]));
+        }
       }
-      __syncthreads();
-      if (lane == 0) { s_part[warp].x = vav_re; s_part[warp].y = vav_im; }
+      acc = shfl4_sum(acc);
+      if (act) {
+        wr = cadd(cmul(tau, csub(yr[ch], acc)), cscale(vr, alpha));
+        if (rsub == 0) {
+          C[r + ld * c] = vr;
+          S.V[ch][i][rloc] = vr;
+          S.W[ch][i][rloc] = wr;
+          a.VW[r + ld * i] = vr;
+          a.WV[r + ld * (NBT + i)] = vr;
+          a.VW[r + ld * (NBT + i)] = wr;
+          a.WV[r + ld * i] = wr;
+        }
+      }
+      if (upd) {
+        cplx u = cmk(0.0, 0.0);
+        if (act)
+          for (int j = rsub; j <= i; j += 4) {
+            const cplx vj = (j == i) ? vr : S.V[ch][j][rloc];
+            const cplx wj = (j == i) ? wr : S.W[ch][j][rloc];
+            u = cadd(u, cmul_cb(vj, s_wc[j]));
+            u = cadd(u, cmul_cb(wj, s_vc[j]));
+          }
+        u = shfl4_sum(u);
+        if (act && rsub == 0) {
+          cplx x = csub(cn[ch], u);
+          if (r == c1) {
+            x.y = 0.0;
+            a.d[c1] = x.x;
+          }
+          C[r + ld * c1] = x;
+          S.X[ch][rloc] = x;
+          if (r >= c1 + 2) nrm_part += cabs2(x);
+        }
+      }
+    }
+    if (i + 1 < a.nbp) {
+      for (int o = 16; o > 0; o >>= 1) nrm_part += __shfl_xor_sync(0xffffffffu, nrm_part, o);
+      if (lane == 0) s_dred[warp] = nrm_part;
       __syncthreads();
       if (tid == 0) {
-        double sr = 0.0, si = 0.0;
-        for (int w = 0; w < TT / 32; ++w) { sr += s_part[w].x; si += s_part[w].y; }
-        if (sr != 0.0) atomicAdd(&red_vav[2 * i], sr);
-        if (si != 0.0) atomicAdd(&red_vav[2 * i + 1], si);
+        double sacc = 0.0;
+        for (int w = 0; w < TT / 32; ++w) sacc += s_dred[w];
+        if (sacc != 0.0) atomicAdd(&red_norm[i + 1], sacc);
       }
     }
-    if (!grid_barrier(a.bar, a.status)) return;
-
-    // ---------------- phase 3 ----------------
-    if (tid < i) {
-      s_sv[tid] = cmk(ldd(red_s + 2 * (NBT * i + tid)), ldd(red_s + 2 * (NBT * i + tid) + 1));
-      s_tv[tid] = cmk(ldd(red_t + 2 * (NBT * i + tid)), ldd(red_t + 2 * (NBT * i + tid) + 1));
-    }
-    __syncthreads();
-    if (tid == 0) {
-      const double vav = ldd(red_vav + 2 * i);
-      double ts = 0.0;  // Re(t^H s)
-      for (int j = 0; j < i; ++j) ts += s_tv[j].x * s_sv[j].x + s_tv[j].y * s_sv[j].y;
-      const double t2 = s_scal[0] * s_scal[0] + s_scal[1] * s_scal[1];
-      s_scal[4] = -0.5 * t2 * (vav - 2.0 * ts);
-      if (bid == 0) {
-        a.e[c] = s_scal[5];
-        a.tau[c] = cmk(s_scal[0], s_scal[1]);
-      }
-    }
-    for (int q = bid; q * RCH < n; q += G) {
-      const int r = q * RCH + rloc;
-      if (rsub == 0 && r >= c + 1 && r < n) {
-        C[r + ld * c] = (r == c + 1) ? cmk(1.0, 0.0) : cmul(ldc(C + r + ld * c), scale);
-      }
-    }
-    __syncthreads();
-    tau_prev = cmk(s_scal[0], s_scal[1]);
-    alpha_prev = s_scal[4];
   }
 }
 
@@ -401,39 +495,45 @@ int tridiag_reduce(excfv_handle* h, int n, cplx* C, long long ld) {
     CUDA_TRY(cudaGetLastError());
     return EXCFV_OK;
   }
+  const int G = h->nsm;  // one CTA per SM
+  const int nch = (n + RCH - 1) / RCH;
+  if (nch > MAXCH * G) {
+    excfv_set_error("tridiagonal reduction supports n <= %d on this GPU", MAXCH * G * RCH);
+    return EXCFV_ERR_UNSUPPORTED;
+  }
+  const int smem = (int)sizeof(PanelSmem);
+  CUDA_TRY(cudaFuncSetAttribute(k_tridiag_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int per_sm = 0;
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tridiag_panel, TT, 0));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tridiag_panel, TT, smem));
   if (per_sm < 1) {
     excfv_set_error("tridiag panel kernel cannot be resident");
     return EXCFV_ERR_CUDA;
   }
-  const int G = h->nsm;  // one CTA per SM
   const cplx mone = cmk(-1.0, 0.0), one = cmk(1.0, 0.0);
+  cplx* VW = ws.Wp;
+  cplx* WV = ws.Wp + (size_t)ws.nmatmax * 2 * NBT;
   for (int p = 0; p < n - 1; p += NBT) {
     const int nbp = min(NBT, n - 1 - p);
     const int final_panel = (p + nbp == n - 1) ? 1 : 0;
     CUDA_TRY(cudaMemsetAsync(ws.red, 0, sizeof(double) * tridiag_workspace_doubles(), s));
     CUDA_TRY(cudaMemsetAsync(ws.bar, 0, 2 * sizeof(unsigned), s));
     TridArgs ta;
-    ta.n = n; ta.ld = ld; ta.C = C; ta.W = ws.Wp; ta.d = ws.d; ta.e = ws.e; ta.tau = ws.tau;
-    ta.ybuf = ws.ybuf;
-    ta.red = ws.red; ta.bar = ws.bar; ta.status = ws.status;
+    ta.n = n; ta.ld = ld; ta.C = C; ta.VW = VW; ta.WV = WV; ta.d = ws.d; ta.e = ws.e;
+    ta.tau = ws.tau; ta.ybuf = ws.ybuf; ta.red = ws.red; ta.bar = ws.bar; ta.status = ws.status;
     ta.p = p; ta.nbp = nbp; ta.final_panel = final_panel;
     void* args[] = {&ta};
     prof_begin(h, PROF_TRD_PANEL);
-    CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_tridiag_panel, dim3(G), dim3(TT), args, 0, s));
+    CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_tridiag_panel, dim3(G), dim3(TT), args,
+                                         (size_t)smem, s));
     count_launch();
     prof_end(h, PROF_TRD_PANEL);
     if (!final_panel) {
       prof_begin(h, PROF_TRD_UPDATE);
       const int q = p + nbp;
       const int m2 = n - q;
-      cplx* V2 = C + q + ld * p;
-      cplx* W2 = ws.Wp + q;
-      cplx* C22 = C + q + ld * q;
-      int rc = zgemm1(s, OP_N, OP_C, m2, m2, nbp, mone, V2, ld, W2, ld, one, C22, ld);
-      if (rc) return rc;
-      rc = zgemm1(s, OP_N, OP_C, m2, m2, nbp, mone, W2, ld, V2, ld, one, C22, ld);
+      // C22 -= [V W] [W V]^H (both triangles; the next panel's y = C22 v reads both)
+      int rc = zgemm1(s, OP_N, OP_C, m2, m2, 2 * NBT, mone, VW + q, ld, WV + q, ld, one,
+                      C + q + ld * q, ld);
       if (rc) return rc;
       prof_end(h, PROF_TRD_UPDATE);
     }

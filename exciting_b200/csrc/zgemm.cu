@@ -41,18 +41,26 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(ZgemmArgs p) {
   const int j0 = blockIdx.y * BN;
   if (p.uplo_c == TRI_UPPER && i0 > j0 + BN - 1) return;
   if (p.uplo_c == TRI_LOWER && j0 > i0 + BM - 1) return;
+  const long long bz = (p.splitk > 1) ? blockIdx.z / p.splitk : blockIdx.z;
 
-  const long long bz = blockIdx.z;
   const cplx* __restrict__ A = p.A + bz * p.strideA;
   const cplx* __restrict__ B = p.B + bz * p.strideB;
   cplx* __restrict__ C = p.C + bz * p.strideC;
 
-  int kbeg = 0, kend = p.k;
+  int kbeg = 0, kend = p.k - p.kdec * (int)bz;
   if (p.tri_a == TRI_LOWER) kend = min(kend, i0 + BM);
   if (p.tri_a == TRI_UPPER) kbeg = max(kbeg, i0);
   if (p.tri_b == TRI_UPPER) kend = min(kend, j0 + BN);
   if (p.tri_b == TRI_LOWER) kbeg = max(kbeg, j0);
   kbeg = (kbeg / BK) * BK;
+  const int split = (p.splitk > 1) ? (int)(blockIdx.z % p.splitk) : 0;
+  if (p.splitk > 1 && kend > kbeg) {
+    const int span = kend - kbeg;
+    const int chunk = ((span + p.splitk - 1) / p.splitk + BK - 1) / BK * BK;
+    const int b0 = kbeg + split * chunk;
+    kend = min(kend, b0 + chunk);
+    kbeg = b0;
+  }
 
   const int wm = (warp & 1) * 32;
   const int wn = (warp >> 1) * 32;
@@ -168,6 +176,24 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(ZgemmArgs p) {
     }
   }
 
+  if (p.splitk > 1) {
+    // raw partial sums, leading dimension m, slab (split, batch)
+    cplx* P = p.part + ((long long)split * p.batch + bz) * (long long)p.m * p.n;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int row = i0 + wm + a * 8 + (lane >> 2);
+      if (row >= p.m) continue;
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int col = j0 + wn + b * 8 + (lane & 3) * 2 + e;
+          if (col >= p.n) continue;
+          P[row + (long long)col * p.m] = cmk(acc[a][b][0][e], acc[a][b][1][e]);
+        }
+    }
+    return;
+  }
   const bool use_beta = (p.beta.x != 0.0 || p.beta.y != 0.0);
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
@@ -191,18 +217,65 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(ZgemmArgs p) {
   }
 }
 
+// C = alpha * sum_s P_s + beta * C over the split-K slabs (fixed order).
+__global__ void k_splitk_reduce(ZgemmArgs p) {
+  const long long mn = (long long)p.m * p.n;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= mn * p.batch) return;
+  const long long bz = t / mn, e = t % mn;
+  const int row = (int)(e % p.m), col = (int)(e / p.m);
+  if (p.uplo_c == TRI_UPPER && row > col) return;
+  if (p.uplo_c == TRI_LOWER && row < col) return;
+  cplx acc = cmk(0.0, 0.0);
+  for (int sp = 0; sp < p.splitk; ++sp) acc = cadd(acc, p.part[((long long)sp * p.batch + bz) * mn + e]);
+  cplx* dst = p.C + bz * p.strideC + row + (long long)col * p.ldc;
+  cplx out = cmul(p.alpha, acc);
+  if (p.beta.x != 0.0 || p.beta.y != 0.0) out = cadd(out, cmul(p.beta, *dst));
+  *dst = out;
+}
+
 template <int OPA, int OPB>
 int launch(cudaStream_t s, const ZgemmArgs& a) {
-  dim3 grid((a.m + BM - 1) / BM, (a.n + BN - 1) / BN, a.batch);
+  dim3 grid((a.m + BM - 1) / BM, (a.n + BN - 1) / BN, a.batch * max(1, a.splitk));
   zgemm_kernel<OPA, OPB><<<grid, NT, 0, s>>>(a); count_launch();
+  if (a.splitk > 1) {
+    const long long tot = (long long)a.m * a.n * a.batch;
+    k_splitk_reduce<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(a); count_launch();
+  }
   return 0;
 }
 
+thread_local GemmCtx g_ctx;
+
 }  // namespace
 
-int zgemm(cudaStream_t s, int opA, int opB, const ZgemmArgs& a) {
+void gemm_ctx_set(const GemmCtx& c) { g_ctx = c; }
+const GemmCtx& gemm_ctx() { return g_ctx; }
+
+int zgemm(cudaStream_t s, int opA, int opB, const ZgemmArgs& a_in) {
+  ZgemmArgs a = a_in;
   if (a.m <= 0 || a.n <= 0 || a.batch <= 0) return 0;
   if (a.k <= 0 && a.beta.x == 1.0 && a.beta.y == 0.0) return 0;
+  // split-K when the output has too few tiles to fill the GPU and K is long
+  a.splitk = 1;
+  a.part = nullptr;
+  {
+    const long long tm = (a.m + BM - 1) / BM, tn = (a.n + BN - 1) / BN;
+    long long tiles = tm * tn * a.batch;
+    if (a.uplo_c != TRI_NONE && a.m == a.n) tiles = (tiles + tm * a.batch) / 2;
+    const int nsm = g_ctx.nsm;
+    if (g_ctx.ws && tiles < nsm && a.k >= 256) {
+      int sk = (int)((2 * nsm + tiles - 1) / tiles);
+      sk = min(sk, a.k / 128);
+      sk = min(sk, 32);
+      const long long need = (long long)a.m * a.n * a.batch;
+      while (sk > 1 && (size_t)(need * sk) > g_ctx.cap) --sk;
+      if (sk > 1) {
+        a.splitk = sk;
+        a.part = g_ctx.ws;
+      }
+    }
+  }
   switch (opA * 3 + opB) {
     case OP_N * 3 + OP_N: return launch<OP_N, OP_N>(s, a);
     case OP_N * 3 + OP_C: return launch<OP_N, OP_C>(s, a);
@@ -226,5 +299,6 @@ int zgemm1(cudaStream_t s, int opA, int opB, int m, int n, int k, cplx alpha,
   a.B = B; a.ldb = ldb; a.strideB = 0;
   a.C = C; a.ldc = ldc; a.strideC = 0;
   a.batch = 1; a.uplo_c = uplo_c; a.tri_a = tri_a; a.tri_b = tri_b;
+  a.splitk = 1; a.part = nullptr; a.kdec = 0;
   return zgemm(s, opA, opB, a);
 }
