@@ -156,21 +156,48 @@ int potrf_upper(excfv_handle* h, int n, cplx* O, cplx* Ui, long long ld) {
   return EXCFV_OK;
 }
 
-// Ui = U^-1 (upper); the diagonal blocks were written by k_potrf_diag.
-// scratch: n x NBP, leading dimension ld.
+// Ui = U^-1 (upper).  The diagonal NBP-blocks of Ui were written by
+// k_potrf_diag; pairs of inverted blocks are merged level by level,
+//   inv([[U11, U12], [0, U22]]) = [[X11, -X11 U12 X22], [0, X22]],
+// with all pairs of one level in one batched GEMM (log2(n / NBP) levels).
+// scratch: n x n complex.
 int trtri_upper(excfv_handle* h, int n, const cplx* U, cplx* Ui, long long ld, cplx* scratch) {
   cudaStream_t s = h->stream;
   const cplx one = cmk(1.0, 0.0), mone = cmk(-1.0, 0.0), zero = cmk(0.0, 0.0);
-  for (int jb = NBP; jb < n; jb += NBP) {
-    const int b = min(NBP, n - jb);
-    // W = U(0:jb, jb:jb+b) * inv(U_jj)
-    int rc = zgemm1(s, OP_N, OP_N, jb, b, b, one, U + ld * jb, ld, Ui + jb + ld * jb, ld, zero,
-                    scratch, ld, TRI_NONE, TRI_NONE, TRI_UPPER);
-    if (rc) return rc;
-    // Ui(0:jb, jb:jb+b) = -Ui(0:jb, 0:jb) * W
-    rc = zgemm1(s, OP_N, OP_N, jb, b, jb, mone, Ui, ld, scratch, ld, zero, Ui + ld * jb, ld,
-                TRI_NONE, TRI_UPPER, TRI_NONE);
-    if (rc) return rc;
+  for (int bs = NBP; bs < n; bs *= 2) {
+    const int nfull = n / (2 * bs);             // pairs whose second block is complete
+    const int rem = n - nfull * 2 * bs;          // rows left after the full pairs
+    // full pairs, batched
+    if (nfull > 0) {
+      const long long step = 2LL * bs * (ld + 1);
+      ZgemmArgs g;
+      g.m = bs; g.n = bs; g.k = bs; g.kdec = 0; g.alpha = one; g.beta = zero;
+      g.A = U + ld * bs; g.lda = ld; g.strideA = step;              // U12
+      g.B = Ui + bs * (ld + 1); g.ldb = ld; g.strideB = step;        // X22
+      g.C = scratch; g.ldc = bs; g.strideC = (long long)bs * bs;     // T = U12 X22
+      g.batch = nfull; g.uplo_c = TRI_NONE; g.tri_a = TRI_NONE; g.tri_b = TRI_UPPER;
+      g.splitk = 1; g.part = nullptr;
+      int rc = zgemm(s, OP_N, OP_N, g);
+      if (rc) return rc;
+      g.alpha = mone;
+      g.A = Ui; g.strideA = step;                                    // X11
+      g.B = scratch; g.ldb = bs; g.strideB = (long long)bs * bs;     // T
+      g.C = Ui + ld * bs; g.ldc = ld; g.strideC = step;              // X12
+      g.tri_a = TRI_UPPER; g.tri_b = TRI_NONE;
+      rc = zgemm(s, OP_N, OP_N, g);
+      if (rc) return rc;
+    }
+    // a trailing pair whose second block is shorter than bs
+    if (rem > bs) {
+      const int a0 = nfull * 2 * bs, d0 = a0 + bs, sd = n - d0;
+      cplx* T = scratch + (size_t)nfull * bs * bs;
+      int rc = zgemm1(s, OP_N, OP_N, bs, sd, sd, one, U + a0 + ld * d0, ld, Ui + d0 + ld * d0, ld,
+                      zero, T, bs, TRI_NONE, TRI_NONE, TRI_UPPER);
+      if (rc) return rc;
+      rc = zgemm1(s, OP_N, OP_N, bs, sd, bs, mone, Ui + a0 + ld * a0, ld, T, bs, zero,
+                  Ui + a0 + ld * d0, ld, TRI_NONE, TRI_UPPER, TRI_NONE);
+      if (rc) return rc;
+    }
   }
   return EXCFV_OK;
 }
