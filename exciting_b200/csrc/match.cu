@@ -288,6 +288,11 @@ __global__ void k_ylm_bessel(int ngp, int ngkmax, int lmax, int apwordmax, int n
         djl[(((size_t)is * ngkmax + ig) * (lmax + 1) + l) * apwordmax + j] = sc * buf[l];
       sc *= g;
     }
+    // orders past this species' largest apword are multiplied by zero later;
+    // store zeros so that no uninitialised value (possibly a NaN) takes part
+    for (int j = omax; j < apwordmax; ++j)
+      for (int l = 0; l <= lmax; ++l)
+        djl[(((size_t)is * ngkmax + ig) * (lmax + 1) + l) * apwordmax + j] = 0.0;
   }
 }
 
