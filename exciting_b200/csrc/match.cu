@@ -13,6 +13,8 @@
 // used by the setup GEMMs (k_apwalm_packed) and, when the caller wants the
 // reference array, in (ngkmax, apwordmax, lmmaxapw, natmtot) order
 // (k_apwalm_ref).
+#include <mutex>
+
 #include "handle.cuh"
 
 namespace {
@@ -433,4 +435,101 @@ int stage_pack_apwalm(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm) 
                                                                st.flist, apwalm, h->ws.Apk); count_launch();
   CUDA_TRY(cudaGetLastError());
   return EXCFV_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Matching coefficients without device allocation (excfv_match_noalloc).
+//
+// The Y_lm and Bessel-derivative scratch of the two match kernels lives in a
+// fixed file-scope device array instead of the handle's workspace.  Every
+// GPU that loads this library holds the array until the process exits.  All
+// calls on a device share it: the kernels write every element they read
+// before reading it in the same call, so nothing has to be cleared between
+// calls, but calls that overlap on the GPU (different streams or handles on
+// the same device) race on it.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[EXCFV_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kMaxDevices = 256;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device.  In host code the array's name only stands in for the symbol,
+// so the address has to come from cudaGetSymbolAddress.
+int noalloc_scratch(int device, unsigned char** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (device < 0 || device >= kMaxDevices) {
+    excfv_set_error("excfv_match_noalloc: device ordinal %d out of range", device);
+    return EXCFV_ERR_ARG;
+  }
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      excfv_set_error("excfv_match_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+      return EXCFV_ERR_CUDA;
+    }
+    g_noalloc_ptr[device] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_ptr[device]);
+  return EXCFV_OK;
+}
+
+}  // namespace
+
+extern "C" int excfv_match_noalloc(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc,
+                                   const double* tpgpc, const double* sfacgp, double* apwalm) {
+  if (!h || !gpc || !tpgpc || !sfacgp || !apwalm) return EXCFV_ERR_ARG;
+  if (!h->have_static) {
+    excfv_set_error("excfv_match_noalloc: excfv_set_static must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  if (ngp <= 0 || ngp > ngkmax) {
+    excfv_set_error("excfv_match_noalloc: need 0 < ngp <= ngkmax (ngp=%d ngkmax=%d)", ngp, ngkmax);
+    return EXCFV_ERR_ARG;
+  }
+  const DevStatic& st = h->st;
+  if (st.lmaxapw > LMAX_CAP) {
+    excfv_set_error("excfv_match_noalloc: lmaxapw %d above the supported %d", st.lmaxapw, LMAX_CAP);
+    return EXCFV_ERR_UNSUPPORTED;
+  }
+  const size_t ylm_bytes = sizeof(cplx) * (size_t)st.lmmaxapw * (size_t)ngkmax;
+  const size_t djl_off = (ylm_bytes + 255) / 256 * 256;
+  const size_t djl_bytes = sizeof(double) * (size_t)st.nspecies * (size_t)ngkmax *
+                           (size_t)(st.lmaxapw + 1) * (size_t)st.apwordmax;
+  if (djl_off + djl_bytes > (size_t)EXCFV_NOALLOC_SCRATCH_BYTES) {
+    excfv_set_error("excfv_match_noalloc: this k-point needs %zu bytes of scratch, above the fixed "
+                    "maximum of %zu bytes (reduce ngkmax or use excfv_match)",
+                    djl_off + djl_bytes, (size_t)EXCFV_NOALLOC_SCRATCH_BYTES);
+    return EXCFV_ERR_ARG;
+  }
+  int prev = -1;
+  cudaGetDevice(&prev);
+  if (prev != h->device) cudaSetDevice(h->device);
+  unsigned char* base = nullptr;
+  int rc = noalloc_scratch(h->device, &base);
+  if (rc == EXCFV_OK) {
+    cplx* ylm = reinterpret_cast<cplx*>(base);
+    double* djl = reinterpret_cast<double*>(base + djl_off);
+    const double fpso = 4.0 * M_PI / sqrt(st.omega);
+    cudaStream_t s = h->stream;
+    k_ylm_bessel<<<(ngp + 127) / 128, 128, 0, s>>>(ngp, ngkmax, st.lmaxapw, st.apwordmax, st.nspecies,
+                                                   st.apword, st.rmt, gpc, tpgpc, ylm, djl);
+    count_launch();
+    const long long tr = (long long)ngkmax * st.apwordmax * st.lmmaxapw * st.natmtot;
+    k_apwalm_ref<<<(unsigned)((tr + 255) / 256), 256, 0, s>>>(
+        ngp, ngkmax, st.natmtot, st.lmaxapw, st.apwordmax, st.idxis, st.apword, fpso, ylm, djl,
+        st.zdinv, reinterpret_cast<const cplx*>(sfacgp), reinterpret_cast<cplx*>(apwalm));
+    count_launch();
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      excfv_set_error("excfv_match_noalloc: launch failed: %s", cudaGetErrorString(e));
+      rc = EXCFV_ERR_CUDA;
+    }
+  }
+  if (prev >= 0 && prev != h->device) cudaSetDevice(prev);
+  return rc;
 }

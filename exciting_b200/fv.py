@@ -238,6 +238,14 @@ class FirstVariational:
                                       C.c_void_p(eval_ptr), C.c_void_p(evec_ptr))
         self._check(rc, "excfv_seceqn_dev", n)
 
+    def match_noalloc(self, ngp: int, ngkmax: int, gpc_ptr: int, tpgpc_ptr: int, sfacgp_ptr: int,
+                      apwalm_ptr: int) -> None:
+        """excfv_match_noalloc on device pointers (queued on the handle's stream)."""
+        rc = self._L.excfv_match_noalloc(self._h, ngp, ngkmax, C.c_void_p(gpc_ptr),
+                                         C.c_void_p(tpgpc_ptr), C.c_void_p(sfacgp_ptr),
+                                         C.c_void_p(apwalm_ptr))
+        self._check(rc, "excfv_match_noalloc")
+
     def set_stream(self, stream_ptr: int) -> None:
         self._check(self._L.excfv_set_stream(self._h, C.c_void_p(stream_ptr)), "excfv_set_stream")
 

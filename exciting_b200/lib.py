@@ -79,7 +79,12 @@ SIGNATURES = {
     "excfv_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "excfv_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "excfv_launch_count": (C.c_longlong, []),
+    "excfv_match_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p]),
 }
+
+#: bytes of the fixed scratch array of excfv_match_noalloc (EXCFV_NOALLOC_SCRATCH_BYTES)
+NOALLOC_SCRATCH_BYTES = 32 << 20
 
 PROF_CLASSES = ["match", "setup_gemm", "setup_other", "potrf", "hegst", "trd_panel",
                 "trd_update", "steig", "backtr"]

@@ -200,6 +200,37 @@ int excfv_profile_read(excfv_handle* h, double* ms, long long* count, int nclass
 /* Number of kernels this library has launched in the process so far. */
 long long excfv_launch_count(void);
 
+/* ---- matching coefficients without device allocation ------------------- */
+
+/* Size of the fixed device array that excfv_match_noalloc uses as scratch. */
+#define EXCFV_NOALLOC_SCRATCH_BYTES (32u << 20)
+
+/* excfv_match_noalloc: the matching coefficients of excfv_match, computed
+ * without allocating or freeing any device memory.  It has no counterpart in
+ * the reference; it exists for callers that cannot call cudaMalloc at this
+ * point: an SCF driver whose device memory is already owned by another pool
+ * allocator in the process (cudaMalloc would fail), or a k-loop that must not
+ * pay the device-wide synchronisation cudaMalloc/cudaFree can impose.
+ *
+ * All pointers are device pointers: gpc(ngkmax), tpgpc(2,ngkmax),
+ * sfacgp complex(ngkmax,natmtot) in; apwalm complex(ngkmax, apwordmax,
+ * lmmaxapw, natmtot) out (the reference layout, zero beyond ngp).  The
+ * handle's per-SCF-iteration data must have been uploaded with
+ * excfv_set_static.  The work is queued on the handle's stream; the call
+ * returns without waiting.
+ *
+ * Scratch: 16 * lmmaxapw * ngkmax bytes (rounded up to 256) plus
+ * 8 * nspecies * ngkmax * (lmaxapw+1) * apwordmax bytes, taken from one
+ * file-scope device array of EXCFV_NOALLOC_SCRATCH_BYTES (32 MiB) that every
+ * GPU loading the library holds until the process exits.  Larger requests
+ * are rejected with EXCFV_ERR_ARG and a message.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  All calls on a device share the
+ * array, so calls that overlap on the GPU (other streams or handles on the
+ * same device) race and must be serialised by the caller. */
+int excfv_match_noalloc(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc,
+                        const double* tpgpc, const double* sfacgp, double* apwalm);
+
 #ifdef __cplusplus
 }
 #endif
