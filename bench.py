@@ -167,6 +167,67 @@ def load_traffic():
 
 
 # ---------------------------------------------------------------------------
+# batching form
+# ---------------------------------------------------------------------------
+
+def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn):
+    from exciting_b200.fv import FirstVariational
+    import torch.distributed as dist
+    nk = args.batch_nk
+    # nmat = ngk + 64 (8 atoms x 8 local orbitals) uniform in [1800, 2300]
+    pb = syn.make_problem("cubic8", nk=nk * world, ngk_range=(1800 - 64, 2300 - 64))
+    st = pb.static
+    kpts = pb.kpts[rank * nk:(rank + 1) * nk]
+    fvb = FirstVariational(local_rank)
+    fvb.set_static(st)
+    stream = torch.cuda.Stream(device=dev)
+    fvb.set_stream(stream.cuda_stream)
+
+    def dv(a, dt):
+        return torch.from_numpy(np.asfortranarray(np.asarray(a, dtype=dt)).ravel(order="F")).to(dev)
+
+    ins = [{n: dv(getattr(k, n), dt) for n, dt in (("gpc", np.float64), ("tpgpc", np.float64),
+                                                   ("sfacgp", np.complex128), ("igpig", np.int32),
+                                                   ("vgpc", np.float64))} for k in kpts]
+    ev = [torch.zeros(st.nstfv, dtype=torch.float64, device=dev) for _ in kpts]
+    X = [torch.zeros(pb.nmatmax * st.nstfv, dtype=torch.complex128, device=dev) for _ in kpts]
+    bargs = ([k.nmat for k in kpts], [k.ngp for k in kpts], pb.ngkmax,
+             [d["gpc"].data_ptr() for d in ins], [d["tpgpc"].data_ptr() for d in ins],
+             [d["sfacgp"].data_ptr() for d in ins], [d["igpig"].data_ptr() for d in ins],
+             [d["vgpc"].data_ptr() for d in ins], pb.nmatmax,
+             [e.data_ptr() for e in ev], [x.data_ptr() for x in X])
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        fvb.autotune_lanes(*bargs)          # untimed: picks the lane count
+        flush.zero_()
+        fvb.seceqn_batched_dev(*bargs)      # warm-up with the chosen lanes
+        info = fvb.batch_info(nk)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        tot = 0.0
+        for _ in range(args.batch_steps):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            fvb.seceqn_batched_dev(*bargs)
+            e.record(stream)
+            e.synchronize()
+            tot += s.elapsed_time(e)
+        info = fvb.batch_info(nk)
+    t = torch.tensor([tot], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    tot = float(t.item())
+    lanes = fvb.lanes()
+    fvb.close()
+    nm = [k.nmat for k in kpts]
+    return {"workload": f"{nk} k-points per GPU of the 8-atom cell, nmat {min(nm)}..{max(nm)} "
+                        f"(uniform, seeded), lowest {st.nstfv} states, plain FP64",
+            "value": world * nk * args.batch_steps / (tot / 1e3), "unit": "k-points/s",
+            "ms_per_batch": tot / args.batch_steps, "lanes": lanes,
+            "all_info_zero": bool(np.all(info == 0))}
+
 
 def main():
     ap = argparse.ArgumentParser()
@@ -177,6 +238,9 @@ def main():
     ap.add_argument("--workload", default="cubic8")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0)
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-nk", type=int, default=64)
+    ap.add_argument("--batch-steps", type=int, default=3)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -363,6 +427,11 @@ def main():
                 "peak_source": "cuBLAS ZGEMM 4096^3 measured in this run (FP64 tensor path)"}
     stages = {kk: round(v[0] / args.steps, 4) for kk, v in prof.items()}
 
+    # ---- batching form: 64 k-points of the 8-atom cell, nmat 1800..2300 ------
+    batched = None
+    if not args.no_batched:
+        batched = run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn)
+
     # ---- CPU baseline (rank 0, N = 1) ----------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -387,6 +456,7 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
+        "batched": batched,
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
     }
     if rank == 0:

@@ -390,8 +390,16 @@ int excfv_destroy(excfv_handle* h) {
   cudaStreamSynchronize(h->stream);
   for (int c = 0; c < PROF_NCLS; ++c)
     for (cudaEvent_t e : h->prof.ev[c]) cudaEventDestroy(e);
+  for (excfv_handle* c : h->lanes) {
+    cudaStreamSynchronize(c->stream);
+    free_workspace(c->ws);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+  }
+  h->lanes.clear();
+  if (h->kinfo) cudaFree(h->kinfo);
   free_workspace(h->ws);
-  free_static(h->st);
+  if (h->owns_static) free_static(h->st);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
   return EXCFV_OK;
@@ -665,6 +673,263 @@ int excfv_sync(excfv_handle* h) {
 }
 
 long long excfv_launch_count(void) { return g_launches.load(); }
+
+// ---------------------------------------------------------------------------
+// batched k-points: lanes
+// ---------------------------------------------------------------------------
+
+// Largest lane count whose per-lane CTA budget still holds an n x n panel
+// (the panel kernel keeps 128 rows per CTA in shared memory).
+static int max_lanes_for(const excfv_handle* h, int nmax) {
+  const int need = (nmax + 127) / 128;
+  return std::max(1, h->nsm / std::max(1, need));
+}
+
+static int ensure_lanes(excfv_handle* h, int L, int nmatmax, int ngkmax, int kmax) {
+  while ((int)h->lanes.size() < L) {
+    excfv_handle* c = new excfv_handle();
+    c->device = h->device;
+    c->nsm = h->nsm;
+    c->owns_static = false;
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete c;
+      excfv_set_error("lane stream creation failed");
+      return EXCFV_ERR_CUDA;
+    }
+    c->stream = c->own_stream;
+    h->lanes.push_back(c);
+  }
+  for (int i = 0; i < L; ++i) {
+    excfv_handle* c = h->lanes[i];
+    c->st = h->st;
+    c->have_static = h->have_static;
+    c->prec = h->prec;
+    c->grid_ctas = std::max(1, h->nsm / L);
+    if (c->ws.H && c->ws.ngkmax != ngkmax) free_workspace(c->ws);
+    int rc = stage_reserve(c, nmatmax, ngkmax, kmax);
+    if (rc) return rc;
+  }
+  return EXCFV_OK;
+}
+
+struct BatchArgs {
+  int nk;
+  const int32_t* nmatp;
+  const int32_t* ngp;
+  int ngkmax;
+  const double* const* gpc;
+  const double* const* tpgpc;
+  const double* const* sfacgp;
+  const int32_t* const* igpig;
+  const double* const* vgpc;
+  int nmatmax;
+  double* const* evalfv;
+  double* const* evecfv;
+  bool host;  // pointers are host pointers (copies in/out on the lane streams)
+};
+
+static int check_batch(excfv_handle* h, const BatchArgs& b, int* nmax) {
+  if (!h || b.nk <= 0 || !b.nmatp || !b.ngp || !b.gpc || !b.tpgpc || !b.sfacgp || !b.igpig ||
+      !b.vgpc || !b.evalfv || !b.evecfv)
+    return EXCFV_ERR_ARG;
+  if (!h->have_static) {
+    excfv_set_error("excfv_set_static must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  *nmax = 0;
+  for (int k = 0; k < b.nk; ++k) {
+    if (b.ngp[k] <= 0 || b.ngp[k] > b.ngkmax || b.nmatp[k] != b.ngp[k] + h->st.nlotot ||
+        b.nmatp[k] > b.nmatmax || h->st.nstfv > b.nmatp[k]) {
+      excfv_set_error("batch entry %d: inconsistent sizes", k);
+      return EXCFV_ERR_ARG;
+    }
+    *nmax = std::max(*nmax, (int)b.nmatp[k]);
+  }
+  return EXCFV_OK;
+}
+
+// Enqueues the whole batch on L lanes (round-robin), fork/join on h->stream.
+static int run_batch(excfv_handle* h, const BatchArgs& b, int L) {
+  int nmax = 0;
+  int rc = check_batch(h, b, &nmax);
+  if (rc) return rc;
+  L = std::max(1, std::min(L, std::min(b.nk, max_lanes_for(h, nmax))));
+  if ((rc = ensure_lanes(h, L, b.nmatmax, b.ngkmax, std::max(1, h->st.nstfv)))) return rc;
+  if (h->kinfo_cap < b.nk) {
+    if (h->kinfo) cudaFree(h->kinfo);
+    h->kinfo = nullptr;
+    h->kinfo_cap = 0;
+    if ((rc = dalloc(&h->kinfo, (size_t)b.nk * ST_NWORDS))) return rc;
+    h->kinfo_cap = b.nk;
+  }
+  h->batch_nmat.assign(b.nmatp, b.nmatp + b.nk);
+  h->last_nk = b.nk;
+  cudaEvent_t fork;
+  CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventRecord(fork, h->stream));
+  for (int i = 0; i < L; ++i) CUDA_TRY(cudaStreamWaitEvent(h->lanes[i]->stream, fork, 0));
+  const cudaMemcpyKind in = b.host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  const cudaMemcpyKind out = b.host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  const int k_st = h->st.nstfv;
+  for (int k = 0; k < b.nk && rc == EXCFV_OK; ++k) {
+    excfv_handle* c = h->lanes[k % L];
+    Workspace& ws = c->ws;
+    cudaStream_t s = c->stream;
+    const int ngp = b.ngp[k], n = b.nmatp[k];
+    CUDA_TRY(cudaMemcpyAsync(ws.gpc, b.gpc[k], sizeof(double) * ngp, in, s));
+    CUDA_TRY(cudaMemcpyAsync(ws.tpgpc, b.tpgpc[k], sizeof(double) * 2 * ngp, in, s));
+    CUDA_TRY(cudaMemcpyAsync(ws.sfacgp, b.sfacgp[k], sizeof(cplx) * (size_t)b.ngkmax * h->st.natmtot,
+                             in, s));
+    CUDA_TRY(cudaMemcpyAsync(ws.igpig, b.igpig[k], sizeof(int) * ngp, in, s));
+    CUDA_TRY(cudaMemcpyAsync(ws.vgpc, b.vgpc[k], sizeof(double) * 3 * ngp, in, s));
+    if ((rc = stage_match(c, ngp, b.ngkmax, nullptr))) break;
+    if ((rc = stage_setup(c, n, ngp, false))) break;
+    if (b.host) {
+      // outputs staged in the lane's (now free) reference-layout apwalm buffer
+      cplx* ov = ws.apwalm;
+      const size_t na = (size_t)b.ngkmax * h->st.apwordmax * h->st.lmmaxapw * h->st.natmtot;
+      if ((size_t)n * k_st > na) {
+        excfv_set_error("batched host path: nmatp*nstfv exceeds the lane staging buffer");
+        rc = EXCFV_ERR_UNSUPPORTED;
+        break;
+      }
+      if ((rc = stage_solve(c, n, k_st, h->st.evaltol, ws.w, ov, n))) break;
+      CUDA_TRY(cudaMemcpy2DAsync(b.evecfv[k], sizeof(cplx) * b.nmatmax, ov, sizeof(cplx) * n,
+                                 sizeof(cplx) * n, k_st, out, s));
+      CUDA_TRY(cudaMemcpyAsync(b.evalfv[k], ws.w, sizeof(double) * k_st, out, s));
+    } else {
+      if ((rc = stage_solve(c, n, k_st, h->st.evaltol, b.evalfv[k], (cplx*)b.evecfv[k], b.nmatmax)))
+        break;
+    }
+    CUDA_TRY(cudaMemcpyAsync(h->kinfo + (size_t)k * ST_NWORDS, ws.status, sizeof(int) * ST_NWORDS,
+                             cudaMemcpyDeviceToDevice, s));
+  }
+  for (int i = 0; i < L; ++i) {
+    cudaEvent_t join;
+    CUDA_TRY(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventRecord(join, h->lanes[i]->stream));
+    CUDA_TRY(cudaStreamWaitEvent(h->stream, join, 0));
+    cudaEventDestroy(join);
+  }
+  cudaEventDestroy(fork);
+  return rc;
+}
+
+static int batch_info(excfv_handle* h, int nk, int32_t* info) {
+  if (nk != h->last_nk || !h->kinfo) return EXCFV_ERR_STATE;
+  std::vector<int> st((size_t)nk * ST_NWORDS);
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  CUDA_TRY(cudaMemcpy(st.data(), h->kinfo, sizeof(int) * st.size(), cudaMemcpyDeviceToHost));
+  int worst = EXCFV_OK;
+  for (int k = 0; k < nk; ++k) {
+    const int v = status_to_info(&st[(size_t)k * ST_NWORDS], h->batch_nmat[k]);
+    if (info) info[k] = v;
+    if (worst == EXCFV_OK) worst = v;
+  }
+  return worst;
+}
+
+int excfv_set_lanes(excfv_handle* h, int32_t nlanes) {
+  if (!h || nlanes < 0) return EXCFV_ERR_ARG;
+  h->nlanes_pref = nlanes;
+  return EXCFV_OK;
+}
+
+int excfv_get_lanes(excfv_handle* h) { return h ? h->nlanes_pref : EXCFV_ERR_ARG; }
+
+static BatchArgs make_batch(int32_t nk, const int32_t* nmatp, const int32_t* ngp, int32_t ngkmax,
+                            const double* const* gpc, const double* const* tpgpc,
+                            const double* const* sfacgp, const int32_t* const* igpig,
+                            const double* const* vgpc, int32_t nmatmax, double* const* evalfv,
+                            double* const* evecfv, bool host) {
+  BatchArgs b;
+  b.nk = nk; b.nmatp = nmatp; b.ngp = ngp; b.ngkmax = ngkmax; b.gpc = gpc; b.tpgpc = tpgpc;
+  b.sfacgp = sfacgp; b.igpig = igpig; b.vgpc = vgpc; b.nmatmax = nmatmax; b.evalfv = evalfv;
+  b.evecfv = evecfv; b.host = host;
+  return b;
+}
+
+static int default_lanes(excfv_handle* h, const BatchArgs& b) {
+  if (h->nlanes_pref > 0) return h->nlanes_pref;
+  int nmax = 0;
+  for (int k = 0; k < b.nk; ++k) nmax = std::max(nmax, (int)b.nmatp[k]);
+  return std::min(8, max_lanes_for(h, nmax));
+}
+
+int excfv_seceqn_batched_dev(excfv_handle* h, int32_t nk, const int32_t* nmatp, const int32_t* ngp,
+                             int32_t ngkmax, const double* const* gpc, const double* const* tpgpc,
+                             const double* const* sfacgp, const int32_t* const* igpig,
+                             const double* const* vgpc, int32_t nmatmax, double* const* evalfv,
+                             double* const* evecfv) {
+  if (!h) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  BatchArgs b = make_batch(nk, nmatp, ngp, ngkmax, gpc, tpgpc, sfacgp, igpig, vgpc, nmatmax, evalfv,
+                           evecfv, false);
+  return run_batch(h, b, default_lanes(h, b));
+}
+
+int excfv_seceqn_batched(excfv_handle* h, int32_t nk, const int32_t* nmatp, const int32_t* ngp,
+                         int32_t ngkmax, const double* const* gpc, const double* const* tpgpc,
+                         const double* const* sfacgp, const int32_t* const* igpig,
+                         const double* const* vgpc, int32_t nmatmax, double* const* evalfv,
+                         double* const* evecfv, int32_t* info) {
+  if (!h) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  BatchArgs b = make_batch(nk, nmatp, ngp, ngkmax, gpc, tpgpc, sfacgp, igpig, vgpc, nmatmax, evalfv,
+                           evecfv, true);
+  int rc = run_batch(h, b, default_lanes(h, b));
+  if (rc) return rc;
+  return batch_info(h, nk, info);
+}
+
+int excfv_batch_info(excfv_handle* h, int32_t nk, int32_t* info) {
+  if (!h) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  return batch_info(h, nk, info);
+}
+
+// Times the batch with 1, 2, 4, 8, 16 lanes (those the SM budget allows) and
+// keeps the fastest for later batched calls.  Device pointers; the outputs of
+// the last timed run are valid.  best_ms (optional) receives the winning time.
+int excfv_autotune_lanes(excfv_handle* h, int32_t nk, const int32_t* nmatp, const int32_t* ngp,
+                         int32_t ngkmax, const double* const* gpc, const double* const* tpgpc,
+                         const double* const* sfacgp, const int32_t* const* igpig,
+                         const double* const* vgpc, int32_t nmatmax, double* const* evalfv,
+                         double* const* evecfv, double* best_ms) {
+  if (!h) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  BatchArgs b = make_batch(nk, nmatp, ngp, ngkmax, gpc, tpgpc, sfacgp, igpig, vgpc, nmatmax, evalfv,
+                           evecfv, false);
+  int nmax = 0;
+  int rc = check_batch(h, b, &nmax);
+  if (rc) return rc;
+  const int lmax = std::min(nk, max_lanes_for(h, nmax));
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int bestL = 1;
+  for (int L = 1; L <= lmax; L *= 2) {
+    for (int rep = 0; rep < 2; ++rep) {  // the first run of a lane count sizes its workspaces
+      CUDA_TRY(cudaEventRecord(e0, h->stream));
+      if ((rc = run_batch(h, b, L))) break;
+      CUDA_TRY(cudaEventRecord(e1, h->stream));
+      CUDA_TRY(cudaEventSynchronize(e1));
+    }
+    if (rc) break;
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best) { best = ms; bestL = L; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  h->nlanes_pref = bestL;
+  if (best_ms) *best_ms = best;
+  rc = run_batch(h, b, bestL);
+  if (rc) return rc;
+  return batch_info(h, nk, nullptr);
+}
 
 int excfv_profile(excfv_handle* h, int enable) {
   if (!h) return EXCFV_ERR_ARG;

@@ -103,6 +103,14 @@ struct Prof {
 
 struct excfv_handle {
   int device = 0;
+  int grid_ctas = 0;          // CTAs of the cooperative panel kernel (0 = all SMs)
+  bool owns_static = true;    // lanes share the parent's static data
+  int nlanes_pref = 0;        // lanes of the batched path (0 = autotune)
+  std::vector<excfv_handle*> lanes;
+  int* kinfo = nullptr;       // per-k status words of the last batch (device)
+  int kinfo_cap = 0;
+  int last_nk = 0;
+  std::vector<int> batch_nmat;  // nmatp of the last batch (info offsets)
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
   int prec = EXCFV_PREC_FP64;
@@ -143,5 +151,7 @@ int stage_setup(excfv_handle* h, int nmatp, int ngp, bool mirror_o);
 // generalized eigensolve on ws.H (full) / ws.O (upper) -> evalfv, evecfv
 int stage_solve(excfv_handle* h, int n, int nstfv, double evaltol, double* d_eval,
                 cplx* d_evec, long long ldevec);
+// per-k status -> LAPACK-style info
+int status_to_info(const int* st, int n);
 // device status -> LAPACK-style info (synchronises the stream)
 int stage_status(excfv_handle* h, int n);

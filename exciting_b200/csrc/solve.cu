@@ -198,6 +198,10 @@ int stage_status(excfv_handle* h, int n) {
   int st[ST_NWORDS];
   CUDA_TRY(cudaMemcpyAsync(st, h->ws.status, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return status_to_info(st, n);
+}
+
+int status_to_info(const int* st, int n) {
   if (st[ST_BARRIER]) {
     excfv_set_error("grid barrier timed out in the tridiagonal reduction");
     return EXCFV_ERR_TIMEOUT;

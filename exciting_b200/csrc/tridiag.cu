@@ -495,7 +495,7 @@ int tridiag_reduce(excfv_handle* h, int n, cplx* C, long long ld) {
     CUDA_TRY(cudaGetLastError());
     return EXCFV_OK;
   }
-  const int G = h->nsm;  // one CTA per SM
+  const int G = (h->grid_ctas > 0) ? h->grid_ctas : h->nsm;  // one CTA per SM of the budget
   const int nch = (n + RCH - 1) / RCH;
   if (nch > MAXCH * G) {
     excfv_set_error("tridiagonal reduction supports n <= %d on this GPU", MAXCH * G * RCH);

@@ -246,6 +246,69 @@ class FirstVariational:
                                          C.c_void_p(apwalm_ptr))
         self._check(rc, "excfv_match_noalloc")
 
+    # ---- batching form ------------------------------------------------
+    @staticmethod
+    def _ptr_array(ptrs, ctype=C.c_void_p):
+        arr = (C.c_void_p * len(ptrs))(*[C.c_void_p(int(p)) for p in ptrs])
+        return arr
+
+    def seceqn_batched_dev(self, nmatp, ngp, ngkmax, gpc, tpgpc, sfacgp, igpig, vgpc, nmatmax,
+                           evalfv, evecfv) -> None:
+        """Batch of k-points on device pointers (lists of ints); asynchronous."""
+        nk = len(nmatp)
+        nm = np.ascontiguousarray(nmatp, dtype=np.int32)
+        ng = np.ascontiguousarray(ngp, dtype=np.int32)
+        arrs = [self._ptr_array(x) for x in (gpc, tpgpc, sfacgp, igpig, vgpc, evalfv, evecfv)]
+        self._keep_batch = (nm, ng, arrs)
+        rc = self._L.excfv_seceqn_batched_dev(self._h, nk, _ptr(nm), _ptr(ng), ngkmax, *arrs[:5],
+                                              nmatmax, arrs[5], arrs[6])
+        self._check(rc, "excfv_seceqn_batched_dev")
+
+    def autotune_lanes(self, nmatp, ngp, ngkmax, gpc, tpgpc, sfacgp, igpig, vgpc, nmatmax,
+                       evalfv, evecfv) -> float:
+        nk = len(nmatp)
+        nm = np.ascontiguousarray(nmatp, dtype=np.int32)
+        ng = np.ascontiguousarray(ngp, dtype=np.int32)
+        arrs = [self._ptr_array(x) for x in (gpc, tpgpc, sfacgp, igpig, vgpc, evalfv, evecfv)]
+        best = C.c_double(0.0)
+        rc = self._L.excfv_autotune_lanes(self._h, nk, _ptr(nm), _ptr(ng), ngkmax, *arrs[:5], nmatmax,
+                                          arrs[5], arrs[6], C.byref(best))
+        self._check(rc, "excfv_autotune_lanes")
+        return best.value
+
+    def batch_info(self, nk: int):
+        info = np.zeros(nk, dtype=np.int32)
+        rc = self._L.excfv_batch_info(self._h, nk, _ptr(info))
+        if rc < 0:
+            raise ExcfvError(rc, "excfv_batch_info")
+        return info
+
+    def set_lanes(self, nlanes: int) -> None:
+        self._check(self._L.excfv_set_lanes(self._h, nlanes), "excfv_set_lanes")
+
+    def lanes(self) -> int:
+        return int(self._L.excfv_get_lanes(self._h))
+
+    def seceqn_batched(self, kpts, nmatmax: int, outs=None):
+        """Host-buffer batch: returns [(evalfv, evecfv)] and the per-k info array."""
+        st = self.static
+        nk = len(kpts)
+        ngkmax = kpts[0].ngkmax
+        nm = np.array([k.ngp + st.nlotot for k in kpts], dtype=np.int32)
+        ng = np.array([k.ngp for k in kpts], dtype=np.int32)
+        if outs is None:
+            outs = [(np.zeros(st.nstfv), np.zeros((nmatmax, st.nstfv), dtype=np.complex128, order="F"))
+                    for _ in kpts]
+        cols = [[k.gpc for k in kpts], [k.tpgpc for k in kpts], [k.sfacgp for k in kpts],
+                [k.igpig for k in kpts], [k.vgpc for k in kpts], [o[0] for o in outs], [o[1] for o in outs]]
+        arrs = [self._ptr_array([a.ctypes.data for a in col]) for col in cols]
+        info = np.zeros(nk, dtype=np.int32)
+        rc = self._L.excfv_seceqn_batched(self._h, nk, _ptr(nm), _ptr(ng), ngkmax, *arrs[:5], nmatmax,
+                                          arrs[5], arrs[6], _ptr(info))
+        if rc < 0:
+            raise ExcfvError(rc, "excfv_seceqn_batched")
+        return outs, info
+
     def set_stream(self, stream_ptr: int) -> None:
         self._check(self._L.excfv_set_stream(self._h, C.c_void_p(stream_ptr)), "excfv_set_stream")
 

@@ -79,6 +79,18 @@ SIGNATURES = {
     "excfv_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "excfv_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "excfv_launch_count": (C.c_longlong, []),
+    "excfv_seceqn_batched_dev": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "excfv_seceqn_batched": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "excfv_batch_info": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "excfv_set_lanes": (C.c_int, [C.c_void_p, C.c_int32]),
+    "excfv_get_lanes": (C.c_int, [C.c_void_p]),
+    "excfv_autotune_lanes": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "excfv_match_noalloc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p]),
 }

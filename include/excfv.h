@@ -175,6 +175,44 @@ int excfv_seceqn_dev(excfv_handle* h, int32_t nmatp, int32_t ngp, int32_t ngkmax
 /* Waits for the handle's stream and returns the status of the last solve. */
 int excfv_sync(excfv_handle* h);
 
+/* ---- many k-points at once (the batching form) --------------------------
+ * The k-points are dealt round-robin to "lanes": child contexts with their own
+ * stream and workspace that share the handle's per-SCF-iteration data, each
+ * running its k-points' match + setup + eigensolve with an SM budget of
+ * (number of SMs / lanes) for the cooperative tridiagonal kernel, so several
+ * k-points are in flight at once (the reference's serial k-loop,
+ * src/scf_cycle.f90:256-289, run concurrently on one GPU).  Per-k arrays are
+ * passed as arrays of pointers; sizes may differ per k-point (nmatp, ngp), the
+ * leading dimensions ngkmax / nmatmax are common.  evecfv[k] is
+ * complex(nmatmax, nstfv), rows > nmatp[k] untouched. */
+
+/* Device pointers; asynchronous on the handle's stream.  Returns < 0 for bad
+ * arguments; the per-k eigensolve status comes from excfv_batch_info. */
+int excfv_seceqn_batched_dev(excfv_handle* h, int32_t nk, const int32_t* nmatp, const int32_t* ngp,
+                             int32_t ngkmax, const double* const* gpc, const double* const* tpgpc,
+                             const double* const* sfacgp, const int32_t* const* igpig,
+                             const double* const* vgpc, int32_t nmatmax, double* const* evalfv,
+                             double* const* evecfv);
+/* Host pointers (pinned memory recommended); waits for completion and fills
+ * info[k] (may be NULL) with each k-point's status; returns the first non-zero. */
+int excfv_seceqn_batched(excfv_handle* h, int32_t nk, const int32_t* nmatp, const int32_t* ngp,
+                         int32_t ngkmax, const double* const* gpc, const double* const* tpgpc,
+                         const double* const* sfacgp, const int32_t* const* igpig,
+                         const double* const* vgpc, int32_t nmatmax, double* const* evalfv,
+                         double* const* evecfv, int32_t* info);
+/* Waits for the last batch and returns per-k status (info may be NULL). */
+int excfv_batch_info(excfv_handle* h, int32_t nk, int32_t* info);
+/* Lane count for the batched calls (0 = heuristic default). */
+int excfv_set_lanes(excfv_handle* h, int32_t nlanes);
+int excfv_get_lanes(excfv_handle* h);
+/* The project's autotuner: times the batch with 1, 2, 4, ... lanes and keeps
+ * the fastest (device pointers, same arguments as excfv_seceqn_batched_dev). */
+int excfv_autotune_lanes(excfv_handle* h, int32_t nk, const int32_t* nmatp, const int32_t* ngp,
+                         int32_t ngkmax, const double* const* gpc, const double* const* tpgpc,
+                         const double* const* sfacgp, const int32_t* const* igpig,
+                         const double* const* vgpc, int32_t nmatmax, double* const* evalfv,
+                         double* const* evecfv, double* best_ms);
+
 /* Stage timings of the last host-entry call (seconds): [0] match,
  * [1] setup (timemat), [2] eigensolve (timefv), [3] copies. */
 int excfv_get_timings(excfv_handle* h, double* t4);
