@@ -206,6 +206,7 @@ def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn):
         if world > 1:
             dist.barrier()
         tot = 0.0
+        fvb.profile(True)
         for _ in range(args.batch_steps):
             flush.zero_()
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -215,6 +216,8 @@ def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn):
             e.synchronize()
             tot += s.elapsed_time(e)
         info = fvb.batch_info(nk)
+        bprof = fvb.profile_read()
+        fvb.profile(False)
     t = torch.tensor([tot], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -226,6 +229,7 @@ def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn):
                         f"(uniform, seeded), lowest {st.nstfv} states, plain FP64",
             "value": world * nk * args.batch_steps / (tot / 1e3), "unit": "k-points/s",
             "ms_per_batch": tot / args.batch_steps, "lanes": lanes,
+            "lane_stage_ms_per_k": {kk: round(v[0] / (args.batch_steps * nk), 3) for kk, v in bprof.items()},
             "all_info_zero": bool(np.all(info == 0))}
 
 

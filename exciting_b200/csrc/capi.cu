@@ -705,6 +705,7 @@ static int ensure_lanes(excfv_handle* h, int L, int nmatmax, int ngkmax, int kma
     c->have_static = h->have_static;
     c->prec = h->prec;
     c->grid_ctas = std::max(1, h->nsm / L);
+    c->prof.on = h->prof.on;  // lanes report into the parent's profile
     if (c->ws.H && c->ws.ngkmax != ngkmax) free_workspace(c->ws);
     int rc = stage_reserve(c, nmatmax, ngkmax, kmax);
     if (rc) return rc;
@@ -937,6 +938,11 @@ int excfv_profile(excfv_handle* h, int enable) {
   prof_collect(h);
   for (int c = 0; c < PROF_NCLS; ++c) { h->prof.ms[c] = 0.0; h->prof.cnt[c] = 0; }
   h->prof.on = enable != 0;
+  for (excfv_handle* l : h->lanes) {
+    prof_collect(l);
+    for (int c = 0; c < PROF_NCLS; ++c) { l->prof.ms[c] = 0.0; l->prof.cnt[c] = 0; }
+    l->prof.on = h->prof.on;
+  }
   return EXCFV_OK;
 }
 
@@ -944,11 +950,18 @@ int excfv_profile_read(excfv_handle* h, double* ms, long long* count, int nclass
   if (!h || !ms || !count || nclasses < 0) return EXCFV_ERR_ARG;
   DeviceGuard g(h->device);
   prof_collect(h);
+  for (excfv_handle* l : h->lanes) prof_collect(l);
   for (int c = 0; c < nclasses && c < PROF_NCLS; ++c) {
     ms[c] = h->prof.ms[c];
     count[c] = h->prof.cnt[c];
     h->prof.ms[c] = 0.0;
     h->prof.cnt[c] = 0;
+    for (excfv_handle* l : h->lanes) {  // summed over lanes (their times overlap)
+      ms[c] += l->prof.ms[c];
+      count[c] += l->prof.cnt[c];
+      l->prof.ms[c] = 0.0;
+      l->prof.cnt[c] = 0;
+    }
   }
   return EXCFV_OK;
 }

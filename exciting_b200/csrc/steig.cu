@@ -127,10 +127,15 @@ __device__ __forceinline__ double urand(unsigned long long a, unsigned long long
 
 // One thread per cluster.  Work arrays are interleaved by eigenvalue index
 // (element i of slot j at [i*k + j]) so that neighbouring threads touch
-// neighbouring addresses.  Y (interleaved too) receives the vectors.
-__global__ void k_stein(int n, const double* d, const double* e, const double* scal, int k,
-                        const double* w, const int* cl, double* ua, double* ub, double* uf,
-                        double* um, double* Yi, int* status) {
+// neighbouring addresses.  Y (interleaved too) receives the vectors.  The
+// factorisation stores the pivots' reciprocals, so the solves' dependency
+// chains hold only multiply-adds; the loops are unrolled so that loads run
+// ahead of the recurrences.
+__global__ void k_stein(int n, const double* __restrict__ d, const double* __restrict__ e,
+                        const double* __restrict__ scal, int k, const double* __restrict__ w,
+                        const int* __restrict__ cl, double* __restrict__ ua, double* __restrict__ ub,
+                        double* __restrict__ uf, double* __restrict__ um, double* __restrict__ Yi,
+                        int* status) {
   const int j0 = blockIdx.x * blockDim.x + threadIdx.x;
   if (j0 >= k || !cl[j0]) return;
   int j1 = j0 + 1;
@@ -147,77 +152,85 @@ __global__ void k_stein(int n, const double* d, const double* e, const double* s
       if (lam - xprev < pertol) lam = xprev + pertol;
     }
     xprev = lam;
-    // factor T - lam I (slot j)
+    // factor T - lam I (slot j); ua holds 1/pivot
     double a = d[0] - lam, b = (n > 1) ? e[0] : 0.0;
+    double ulast = 0.0;
+#pragma unroll 4
     for (int i = 0; i < n - 1; ++i) {
       const double c = e[i], dd = d[i + 1] - lam, ee = (i + 1 < n - 1) ? e[i + 1] : 0.0;
       const size_t o = (size_t)i * k + j;
       if (fabs(a) >= fabs(c)) {
         const double aa = (fabs(a) < pert) ? copysign(pert, a) : a;
-        ua[o] = aa; ub[o] = b; uf[o] = 0.0;
-        const double m = c / aa;
+        const double ra = 1.0 / aa;
+        ua[o] = ra; ub[o] = b; uf[o] = 0.0;
+        const double m = c * ra;
         um[o] = m;
         a = dd - m * b;
         b = ee;
       } else {
-        ua[o] = c; ub[o] = dd; uf[o] = ee;
-        const double m = a / c;
-        um[o] = -m - 2.0;  // encodes a swap (value < -1 never arises without a swap since |m|<=1)
+        const double rc = 1.0 / c;
+        ua[o] = rc; ub[o] = dd; uf[o] = ee;
+        const double m = a * rc;
+        um[o] = -m - 2.0;  // encodes a swap (a multiplier |m| <= 1 never reaches below -1)
         a = b - m * dd;
         b = -m * ee;
       }
     }
     {
       const size_t o = (size_t)(n - 1) * k + j;
-      ua[o] = (fabs(a) < pert) ? copysign(pert, a) : a;
+      const double aa = (fabs(a) < pert) ? copysign(pert, a) : a;
+      ua[o] = 1.0 / aa;
       ub[o] = 0.0; uf[o] = 0.0; um[o] = 0.0;
+      ulast = fabs(aa);
     }
-    const double ulast = fabs(ua[(size_t)(n - 1) * k + j]);
-    // start vector
     for (int i = 0; i < n; ++i) Yi[(size_t)i * k + j] = urand(j + 1, i + 1);
     int nrmchk = 0;
     bool conv = false;
     for (int its = 0; its < 5; ++its) {
       // scale the right-hand side: ||x||_1 = n ||T|| max(eps, |u_last|)
       double s1 = 0.0;
+#pragma unroll 8
       for (int i = 0; i < n; ++i) s1 += fabs(Yi[(size_t)i * k + j]);
       const double scl = (s1 > 0.0) ? n * tnorm * fmax(eps, ulast) / s1 : 1.0;
       // forward elimination on the right-hand side
       double cur = Yi[j] * scl;
+#pragma unroll 4
       for (int i = 0; i < n - 1; ++i) {
         const size_t o = (size_t)i * k + j;
-        const double nx = Yi[(size_t)(i + 1) * k + j] * scl;
+        const double nx = Yi[o + k] * scl;
         const double m = um[o];
         if (m < -1.0) {  // swapped
-          const double mm = -(m + 2.0);
           Yi[o] = nx;
-          cur = cur - mm * nx;
+          cur = cur + (m + 2.0) * nx;
         } else {
           Yi[o] = cur;
           cur = nx - m * cur;
         }
       }
-      Yi[(size_t)(n - 1) * k + j] = cur;
-      // back substitution
-      double x2 = 0.0, x1 = Yi[(size_t)(n - 1) * k + j] / ua[(size_t)(n - 1) * k + j];
+      // back substitution with the stored reciprocals
+      double x2 = 0.0, x1 = cur * ua[(size_t)(n - 1) * k + j];
       Yi[(size_t)(n - 1) * k + j] = x1;
+      double nrm = fabs(x1);
+#pragma unroll 4
       for (int i = n - 2; i >= 0; --i) {
         const size_t o = (size_t)i * k + j;
-        const double x = (Yi[o] - ub[o] * x1 - uf[o] * x2) / ua[o];
+        const double x = (Yi[o] - ub[o] * x1 - uf[o] * x2) * ua[o];
         Yi[o] = x;
+        nrm = fmax(nrm, fabs(x));
         x2 = x1;
         x1 = x;
       }
       // orthogonalise against the earlier members of the cluster
-      for (int q = j0; q < j; ++q) {
-        double dot = 0.0;
-        for (int i = 0; i < n; ++i) dot += Yi[(size_t)i * k + q] * Yi[(size_t)i * k + j];
-        for (int i = 0; i < n; ++i) Yi[(size_t)i * k + j] -= dot * Yi[(size_t)i * k + q];
+      if (j > j0) {
+        for (int q = j0; q < j; ++q) {
+          double dot = 0.0;
+          for (int i = 0; i < n; ++i) dot += Yi[(size_t)i * k + q] * Yi[(size_t)i * k + j];
+          for (int i = 0; i < n; ++i) Yi[(size_t)i * k + j] -= dot * Yi[(size_t)i * k + q];
+        }
+        nrm = 0.0;
+        for (int i = 0; i < n; ++i) nrm = fmax(nrm, fabs(Yi[(size_t)i * k + j]));
       }
-      double nrm = 0.0;
-      for (int i = 0; i < n; ++i) nrm = fmax(nrm, fabs(Yi[(size_t)i * k + j]));
       if (!(nrm >= dtpcrt)) {
-        // rescale to avoid overflow in the next solve
         if (nrm > 0.0 && nrm < 1e-200) {
           for (int i = 0; i < n; ++i) Yi[(size_t)i * k + j] *= 1e200;
         }
@@ -238,6 +251,142 @@ __global__ void k_stein(int n, const double* d, const double* e, const double* s
     double sc = (s2 > 0.0) ? 1.0 / sqrt(s2) : 0.0;
     if (Yi[(size_t)ib * k + j] < 0.0) sc = -sc;
     for (int i = 0; i < n; ++i) Yi[(size_t)i * k + j] *= sc;
+  }
+}
+
+// The same inverse iteration with the factor and the working vector of one
+// eigenvector in shared memory (40 n bytes): one warp per cluster, lane 0
+// runs the recurrences (factorisation, forward elimination, back
+// substitution) at shared-memory latency, the warp shares the element-wise
+// passes.  The finished vectors go to Yi (interleaved as in k_stein) because
+// later members of a cluster are orthogonalised against them.
+__global__ void __launch_bounds__(32) k_stein_smem(int n, const double* __restrict__ d,
+                                                   const double* __restrict__ e,
+                                                   const double* __restrict__ scal, int k,
+                                                   const double* __restrict__ w,
+                                                   const int* __restrict__ cl, double* Yi,
+                                                   int* status) {
+  extern __shared__ double sm[];
+  double* ra = sm;          // 1 / pivot
+  double* rb = ra + n;      // first superdiagonal of U
+  double* rf = rb + n;      // second superdiagonal (fill-in from swaps)
+  double* rm = rf + n;      // multiplier (swap encoded as -m-2)
+  double* y = rm + n;       // working vector
+  const int j0 = blockIdx.x;
+  const int lane = threadIdx.x;
+  if (!cl[j0]) return;
+  int j1 = j0 + 1;
+  while (j1 < k && !cl[j1]) ++j1;
+  const double eps = 1.1102230246251565e-16;
+  const double tnorm = scal[3];
+  const double dtpcrt = sqrt(0.1 / n);
+  const double pert = fmax(eps * tnorm, 1e-300);
+  double xprev = 0.0;
+  for (int j = j0; j < j1; ++j) {
+    double lam = w[j];
+    if (j > j0) {
+      const double pertol = 10.0 * fabs(eps * lam);
+      if (lam - xprev < pertol) lam = xprev + pertol;
+    }
+    xprev = lam;
+    __shared__ double s_ulast;
+    if (lane == 0) {
+      double a = d[0] - lam, b = (n > 1) ? e[0] : 0.0;
+      for (int i = 0; i < n - 1; ++i) {
+        const double c = e[i], dd = d[i + 1] - lam, ee = (i + 1 < n - 1) ? e[i + 1] : 0.0;
+        if (fabs(a) >= fabs(c)) {
+          const double aa = (fabs(a) < pert) ? copysign(pert, a) : a;
+          const double r = 1.0 / aa;
+          ra[i] = r; rb[i] = b; rf[i] = 0.0;
+          const double m = c * r;
+          rm[i] = m;
+          a = dd - m * b;
+          b = ee;
+        } else {
+          const double r = 1.0 / c;
+          ra[i] = r; rb[i] = dd; rf[i] = ee;
+          const double m = a * r;
+          rm[i] = -m - 2.0;
+          a = b - m * dd;
+          b = -m * ee;
+        }
+      }
+      const double aa = (fabs(a) < pert) ? copysign(pert, a) : a;
+      ra[n - 1] = 1.0 / aa;
+      rb[n - 1] = 0.0; rf[n - 1] = 0.0; rm[n - 1] = 0.0;
+      s_ulast = fabs(aa);
+    }
+    for (int i = lane; i < n; i += 32) y[i] = urand(j + 1, i + 1);
+    __syncwarp();
+    const double ulast = s_ulast;
+    int nrmchk = 0;
+    bool conv = false;
+    for (int its = 0; its < 5; ++its) {
+      double s1 = 0.0;
+      for (int i = lane; i < n; i += 32) s1 += fabs(y[i]);
+      for (int o = 16; o > 0; o >>= 1) s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      const double scl = (s1 > 0.0) ? n * tnorm * fmax(eps, ulast) / s1 : 1.0;
+      if (lane == 0) {
+        double cur = y[0] * scl;
+        for (int i = 0; i < n - 1; ++i) {
+          const double nx = y[i + 1] * scl;
+          const double m = rm[i];
+          if (m < -1.0) {
+            y[i] = nx;
+            cur = cur + (m + 2.0) * nx;
+          } else {
+            y[i] = cur;
+            cur = nx - m * cur;
+          }
+        }
+        double x2 = 0.0, x1 = cur * ra[n - 1];
+        y[n - 1] = x1;
+        for (int i = n - 2; i >= 0; --i) {
+          const double x = (y[i] - rb[i] * x1 - rf[i] * x2) * ra[i];
+          y[i] = x;
+          x2 = x1;
+          x1 = x;
+        }
+      }
+      __syncwarp();
+      for (int q = j0; q < j; ++q) {
+        double dot = 0.0;
+        for (int i = lane; i < n; i += 32) dot += Yi[(size_t)i * k + q] * y[i];
+        for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+        for (int i = lane; i < n; i += 32) y[i] -= dot * Yi[(size_t)i * k + q];
+        __syncwarp();
+      }
+      double nrm = 0.0;
+      for (int i = lane; i < n; i += 32) nrm = fmax(nrm, fabs(y[i]));
+      for (int o = 16; o > 0; o >>= 1) nrm = fmax(nrm, __shfl_xor_sync(0xffffffffu, nrm, o));
+      if (!(nrm >= dtpcrt)) {
+        if (nrm > 0.0 && nrm < 1e-200)
+          for (int i = lane; i < n; i += 32) y[i] *= 1e200;
+        __syncwarp();
+        continue;
+      }
+      ++nrmchk;
+      if (nrmchk >= 3) { conv = true; break; }
+    }
+    if (!conv && lane == 0) atomicAdd(&status[ST_STEIN], 1);
+    // normalise: unit 2-norm, largest component positive (lowest index on ties)
+    double s2 = 0.0, big = -1.0;
+    int ib = 0;
+    for (int i = lane; i < n; i += 32) {
+      const double v = y[i];
+      s2 += v * v;
+      if (fabs(v) > big) { big = fabs(v); ib = i; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      const double ob = __shfl_xor_sync(0xffffffffu, big, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, ib, o);
+      if (ob > big || (ob == big && oi < ib)) { big = ob; ib = oi; }
+    }
+    double sc = (s2 > 0.0) ? 1.0 / sqrt(s2) : 0.0;
+    if (y[ib] < 0.0) sc = -sc;
+    for (int i = lane; i < n; i += 32) Yi[(size_t)i * k + j] = y[i] * sc;
+    __syncwarp();
   }
 }
 
@@ -269,8 +418,14 @@ int tridiag_eig(excfv_handle* h, int n, int k, double abstol, const double* d, c
   CUDA_TRY(cudaGetLastError());
   k_clusters<<<(k + 127) / 128, 128, 0, s>>>(k, w, scal, iscratch); count_launch();
   CUDA_TRY(cudaGetLastError());
-  k_stein<<<(k + 63) / 64, 64, 0, s>>>(n, d, e, scal, k, w, iscratch, ua, ub, uf, um, Yi,
-                                       h->ws.status); count_launch();
+  const size_t sbytes = 40 * (size_t)n;
+  if (sbytes <= 200 * 1024) {
+    CUDA_TRY(cudaFuncSetAttribute(k_stein_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sbytes));
+    k_stein_smem<<<k, 32, sbytes, s>>>(n, d, e, scal, k, w, iscratch, Yi, h->ws.status); count_launch();
+  } else {
+    k_stein<<<(k + 31) / 32, 32, 0, s>>>(n, d, e, scal, k, w, iscratch, ua, ub, uf, um, Yi,
+                                         h->ws.status); count_launch();
+  }
   CUDA_TRY(cudaGetLastError());
   k_y_to_z<<<dim3((n + 255) / 256, k), 256, 0, s>>>(n, k, Yi, Z, ldz); count_launch();
   CUDA_TRY(cudaGetLastError());
