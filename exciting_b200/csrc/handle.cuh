@@ -111,6 +111,7 @@ struct excfv_handle {
   int kinfo_cap = 0;
   int last_nk = 0;
   std::vector<int> batch_nmat;  // nmatp of the last batch (info offsets)
+  excfv_handle* sub = nullptr;  // nested context of the precision form's Rayleigh-Ritz solve
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
   int prec = EXCFV_PREC_FP64;
@@ -152,6 +153,8 @@ int stage_setup(excfv_handle* h, int nmatp, int ngp, bool mirror_o);
 int stage_solve(excfv_handle* h, int n, int nstfv, double evaltol, double* d_eval,
                 cplx* d_evec, long long ldevec);
 // per-k status -> LAPACK-style info
+// states carried by the precision form (k plus a Rayleigh-Ritz buffer)
+int mixed_states(int n, int k);
 int status_to_info(const int* st, int n);
 // device status -> LAPACK-style info (synchronises the stream)
 int stage_status(excfv_handle* h, int n);

@@ -9,6 +9,8 @@
 //   Z = orth(y)                    Cholesky-QR on the k vectors
 //   Z <- Q Z                       block reflectors (I - V Tf V^H), GEMMs (ZUNMTR)
 //   X = Ui Z                       one GEMM (ZTRSM)
+#include <algorithm>
+
 #include "handle.cuh"
 
 int potrf_upper(excfv_handle* h, int n, cplx* O, cplx* Ui, long long ld);
@@ -18,6 +20,8 @@ int tridiag_nb();
 int tridiag_eig(excfv_handle* h, int n, int k, double abstol, const double* d, const double* e,
                 double* w, cplx* Z, long long ldz, double* scratch, int* iscratch);
 int mirror_upper(cudaStream_t s, int n, cplx* M, long long ld);
+int tridiag_reduce_f32(excfv_handle* h, int n, float2* C, long long ld);
+int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax);
 
 namespace {
 
@@ -63,6 +67,28 @@ __global__ void __launch_bounds__(LT) k_larft(int n, const cplx* Gall, const cpl
   }
   cplx* out = Tf + (size_t)blk * NBQ * NBQ;
   for (int t = tid; t < NBQ * NBQ; t += LT) out[t] = T[t % NBQ][t / NBQ];
+}
+
+__global__ void k_to_f32(long long cnt, const cplx* __restrict__ in, float2* __restrict__ out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < cnt) out[t] = make_float2((float)in[t].x, (float)in[t].y);
+}
+
+// reflectors (below the diagonal) of an n x n complex64 matrix -> FP64
+__global__ void k_lower_to_f64(int n, const float2* __restrict__ in, long long ld,
+                               cplx* __restrict__ out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (r >= n || r <= c) return;
+  const float2 v = in[r + ld * c];
+  out[r + ld * c] = cmk((double)v.x, (double)v.y);
+}
+
+// status words of the nested Rayleigh-Ritz solve added into the caller's
+// (its Cholesky-QR word is not an overlap failure of the caller's problem)
+__global__ void k_or_status(const int* from, int* to) {
+  const int i = threadIdx.x;
+  if (i < ST_NWORDS && i != ST_POTRF && from[i]) to[i] += from[i];
 }
 
 __global__ void k_copy_eval(int k, const double* w, double* out) {
@@ -146,8 +172,17 @@ int cholqr(excfv_handle* h, int n, int k, cplx*& Z, long long ldz) {
   return EXCFV_OK;
 }
 
+// States carried through the complex64 reduction so that the Rayleigh-Ritz
+// step has a buffer between the kept and the discarded part of the spectrum.
+int mixed_states(int n, int k) { return std::min(n, k + std::max(16, k / 8)); }
+
+static int stage_solve_mixed(excfv_handle* h, int n, int k, double evaltol, double* d_eval,
+                             cplx* d_evec, long long ldevec);
+
 int stage_solve(excfv_handle* h, int n, int k, double evaltol, double* d_eval, cplx* d_evec,
                 long long ldevec) {
+  if (h->prec == EXCFV_PREC_MIXED && n > 64)
+    return stage_solve_mixed(h, n, k, evaltol, d_eval, d_evec, ldevec);
   Workspace& ws = h->ws;
   cudaStream_t s = h->stream;
   const long long ld = n;
@@ -191,6 +226,111 @@ int stage_solve(excfv_handle* h, int n, int k, double evaltol, double* d_eval, c
   ws.Z = Z;  // cholqr may have swapped the buffers
   k_copy_eval<<<(k + 127) / 128, 128, 0, s>>>(k, ws.w, d_eval); count_launch();
   CUDA_TRY(cudaGetLastError());
+  return EXCFV_OK;
+}
+
+// Standard Hermitian eigenproblem on ws.H (n x n, both triangles, destroyed):
+// lowest k eigenpairs -> ws.w and Z (n x k, ld n; returned pointer, one of
+// ws.Z / ws.Z2).  The k' x k' Rayleigh-Ritz problem of the precision form.
+static int solve_standard(excfv_handle* h, int n, int k, double evaltol, cplx** Zout) {
+  Workspace& ws = h->ws;
+  int rc;
+  if ((rc = tridiag_reduce(h, n, ws.H, n))) return rc;
+  cplx* Z = ws.Z;
+  if ((rc = tridiag_eig(h, n, k, evaltol, ws.d, ws.e, ws.w, Z, n, ws.stein_ws, ws.icl))) return rc;
+  if ((rc = cholqr(h, n, k, Z, n))) return rc;
+  if ((rc = apply_q(h, n, k, ws.H, n, Z, n))) return rc;
+  ws.Z = Z;
+  *Zout = Z;
+  return EXCFV_OK;
+}
+
+// The precision form: FP64 Cholesky and reduction to C = U^-H H U^-1; the
+// Householder tridiagonal reduction of a complex64 copy of C; eigenpairs of T
+// for k' = k + extra states and their back-transform; then Rayleigh-Ritz in
+// FP64: X0 = orth(Q Z_T), Hk = X0^H C X0 (k' x k') solved in FP64, X = X0 Y.
+// The Ritz values' errors are second order in the FP32 perturbation of X0
+// (relative to the gap between state k and the discarded states beyond k').
+static int stage_solve_mixed(excfv_handle* h, int n, int k, double evaltol, double* d_eval,
+                             cplx* d_evec, long long ldevec) {
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  const long long ld = n;
+  const cplx one = cmk(1.0, 0.0), zero = cmk(0.0, 0.0);
+  int rc;
+  const int kx = mixed_states(n, k);
+  if (k < 1 || k > n) return EXCFV_ERR_ARG;
+  if (kx > ws.kmax) {
+    excfv_set_error("mixed solve: workspace holds %d states, needs %d", ws.kmax, kx);
+    return EXCFV_ERR_ARG;
+  }
+  bind_gemm_ctx(h);
+  CUDA_TRY(cudaMemsetAsync(ws.status, 0, ST_NWORDS * sizeof(int), s));
+  prof_begin(h, PROF_POTRF);
+  if ((rc = potrf_upper(h, n, ws.O, ws.Ui, ld))) return rc;
+  if ((rc = trtri_upper(h, n, ws.O, ws.Ui, ld, ws.T))) return rc;
+  prof_end(h, PROF_POTRF);
+  prof_begin(h, PROF_HEGST);
+  if ((rc = zgemm1(s, OP_N, OP_N, n, n, n, one, ws.H, ld, ws.Ui, ld, zero, ws.T, ld, TRI_NONE,
+                   TRI_NONE, TRI_UPPER)))
+    return rc;
+  if ((rc = zgemm1(s, OP_C, OP_N, n, n, n, one, ws.Ui, ld, ws.T, ld, zero, ws.H, ld, TRI_UPPER,
+                   TRI_LOWER, TRI_NONE)))
+    return rc;
+  if ((rc = mirror_upper(s, n, ws.H, ld))) return rc;
+  // complex64 copy of C for the reduction (ws.T is free now)
+  float2* Cf = reinterpret_cast<float2*>(ws.T);
+  const long long nn = (long long)n * n;
+  k_to_f32<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(nn, ws.H, Cf); count_launch();
+  CUDA_TRY(cudaGetLastError());
+  prof_end(h, PROF_HEGST);
+  if ((rc = tridiag_reduce_f32(h, n, Cf, ld))) return rc;
+  // reflectors back to FP64 into ws.O (the Cholesky factor is no longer needed)
+  k_lower_to_f64<<<dim3((n + 255) / 256, n), 256, 0, s>>>(n, Cf, ld, ws.O); count_launch();
+  CUDA_TRY(cudaGetLastError());
+  cplx* Z = ws.Z;
+  prof_begin(h, PROF_STEIG);
+  if ((rc = tridiag_eig(h, n, kx, evaltol, ws.d, ws.e, ws.w, Z, ld, ws.stein_ws, ws.icl))) return rc;
+  prof_end(h, PROF_STEIG);
+  prof_begin(h, PROF_BACKTR);
+  if ((rc = apply_q(h, n, kx, ws.O, ld, Z, ld))) return rc;
+  if ((rc = cholqr(h, n, kx, Z, ld))) return rc;
+  // R = C X0 (FP64, full C)
+  cplx* R = ws.Z2;
+  if ((rc = zgemm1(s, OP_N, OP_N, n, kx, n, one, ws.H, ld, Z, ld, zero, R, ld))) return rc;
+  // the k' x k' problem runs on a nested context with its own workspace
+  if (!h->sub) {
+    h->sub = new excfv_handle();
+    h->sub->owns_static = false;
+  }
+  excfv_handle* sub = h->sub;
+  sub->device = h->device;
+  sub->nsm = h->nsm;
+  sub->grid_ctas = h->grid_ctas;
+  sub->stream = s;
+  sub->st = h->st;
+  sub->have_static = h->have_static;
+  sub->prec = EXCFV_PREC_FP64;
+  sub->prof.on = false;
+  if ((rc = stage_reserve(sub, kx, 1, k))) return rc;
+  if ((rc = zgemm1(s, OP_C, OP_N, kx, kx, n, one, Z, ld, R, ld, zero, sub->ws.H, kx, TRI_UPPER)))
+    return rc;
+  if ((rc = mirror_upper(s, kx, sub->ws.H, kx))) return rc;
+  CUDA_TRY(cudaMemsetAsync(sub->ws.status, 0, ST_NWORDS * sizeof(int), s));
+  cplx* Y = nullptr;
+  if ((rc = solve_standard(sub, kx, k, evaltol, &Y))) return rc;
+  bind_gemm_ctx(h);
+  // X = X0 Y (n x k) into R's buffer, then the back-transform with U^-1
+  if ((rc = zgemm1(s, OP_N, OP_N, n, k, kx, one, Z, ld, Y, kx, zero, R, ld))) return rc;
+  if ((rc = zgemm1(s, OP_N, OP_N, n, k, n, one, ws.Ui, ld, R, ld, zero, d_evec, ldevec, TRI_NONE,
+                   TRI_UPPER, TRI_NONE)))
+    return rc;
+  ws.Z = Z;
+  k_copy_eval<<<(k + 127) / 128, 128, 0, s>>>(k, sub->ws.w, d_eval); count_launch();
+  CUDA_TRY(cudaGetLastError());
+  k_or_status<<<1, ST_NWORDS, 0, s>>>(sub->ws.status, ws.status); count_launch();
+  CUDA_TRY(cudaGetLastError());
+  prof_end(h, PROF_BACKTR);
   return EXCFV_OK;
 }
 

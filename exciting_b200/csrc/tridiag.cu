@@ -35,9 +35,27 @@ constexpr int RCH = 64;
 constexpr int MAXCH = 2;  // row chunks per CTA held in shared memory
 constexpr long long BARRIER_NS = 2000000000LL;  // 2 s
 
+// Storage type T2 of C, V and W: double2 (FP64 form) or float2 (the precision
+// form's complex64 copy).  Arithmetic is FP64 in both.
+__device__ __forceinline__ cplx ldT(const double2* p) { return __ldcg(p); }
+__device__ __forceinline__ cplx ldT(const float2* p) {
+  const float2 v = __ldcg(p);
+  return cmk((double)v.x, (double)v.y);
+}
+__device__ __forceinline__ void stT(double2* p, cplx v) { *p = v; }
+__device__ __forceinline__ void stT(float2* p, cplx v) { *p = make_float2((float)v.x, (float)v.y); }
+__device__ __forceinline__ cplx toD(double2 v) { return v; }
+__device__ __forceinline__ cplx toD(float2 v) { return cmk((double)v.x, (double)v.y); }
+template <typename T2> __device__ __forceinline__ T2 fromD(cplx v);
+template <> __device__ __forceinline__ double2 fromD<double2>(cplx v) { return v; }
+template <> __device__ __forceinline__ float2 fromD<float2>(cplx v) {
+  return make_float2((float)v.x, (float)v.y);
+}
+
+template <typename T2>
 struct PanelSmem {
-  cplx V[MAXCH][NBT][RCH];
-  cplx W[MAXCH][NBT][RCH];
+  T2 V[MAXCH][NBT][RCH];
+  T2 W[MAXCH][NBT][RCH];
   cplx X[MAXCH][RCH];
 };
 
@@ -85,12 +103,13 @@ __device__ bool grid_barrier(unsigned* bar, unsigned& epoch, int* status) {
   return s_ok != 0;
 }
 
+template <typename T2>
 struct TridArgs {
   int n;
   long long ld;
-  cplx* C;
-  cplx* VW;      // n x 2NBT: [V | W] of the panel (leading dimension ld)
-  cplx* WV;      // n x 2NBT: [W | V]
+  T2* C;
+  T2* VW;        // n x 2NBT: [V | W] of the panel (leading dimension ld)
+  T2* WV;        // n x 2NBT: [W | V]
   double* d;
   double* e;
   cplx* tau;
@@ -124,9 +143,10 @@ __device__ __forceinline__ cplx warp_sum(cplx v) {
 
 constexpr int JB = 8;  // column tiles whose x values are staged per round trip
 
-__global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs a) {
+template <typename T2>
+__global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs<T2> a) {
   extern __shared__ __align__(16) unsigned char dsm[];
-  PanelSmem& S = *reinterpret_cast<PanelSmem*>(dsm);
+  PanelSmem<T2>& S = *reinterpret_cast<PanelSmem<T2>*>(dsm);
   __shared__ cplx s_vc[NBT], s_wc[NBT];   // row c+1 of V and W
   __shared__ cplx s_sv[NBT], s_tv[NBT];   // V^H v, W^H v of the current column
   __shared__ cplx s_acc_s[NBT], s_acc_t[NBT];
@@ -139,7 +159,7 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs a) {
 
   const int n = a.n;
   const long long ld = a.ld;
-  cplx* __restrict__ C = a.C;
+  T2* __restrict__ C = a.C;
   const int tid = threadIdx.x, bid = blockIdx.x, G = gridDim.x;
   const int rsub = tid & 3, rloc = tid >> 2;
   const int lane = tid & 31, warp = tid >> 5;
@@ -159,11 +179,11 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs a) {
       if (q >= nch) break;
       const int r = q * RCH + rloc;
       if (rsub == 0 && r >= c && r < n) {
-        cplx x = ldc(C + r + ld * c);
+        cplx x = ldT(C + r + ld * c);
         if (r == c) {
           x.y = 0.0;
           a.d[c] = x.x;
-          C[r + ld * c] = x;
+          stT(C + r + ld * c, x);
         }
         S.X[ch][rloc] = x;
         if (r >= c + 2) nrm_part += cabs2(x);
@@ -214,15 +234,15 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs a) {
         {
           const int j_a = r0g + J0 * 64 + tid, j_b = j_a + TT;
           const int lim = r0g + J1 * 64;
-          if (j_a < lim && j_a < n && j_a != c + 1) xv0 = ldc(C + j_a + ld * c);
-          if (j_b < lim && j_b < n && j_b != c + 1) xv1 = ldc(C + j_b + ld * c);
+          if (j_a < lim && j_a < n && j_a != c + 1) xv0 = ldT(C + j_a + ld * c);
+          if (j_b < lim && j_b < n && j_b != c + 1) xv1 = ldT(C + j_b + ld * c);
           if (J0 == Jb && tid < 64 && real_item) {
             const int rr2 = r0g + I * 64 + tid;
-            if (rr2 < n && rr2 != c + 1) xrow = ldc(C + rr2 + ld * c);
+            if (rr2 < n && rr2 != c + 1) xrow = ldT(C + rr2 + ld * c);
           }
         }
         if (!have_scal && tid == 0) {
-          const cplx alpha = ldc(C + (c + 1) + ld * c);
+          const cplx alpha = ldT(C + (c + 1) + ld * c);
           const double xn2 = ldd(red_norm + i);
           double tr = 0.0, ti = 0.0, scr = 0.0, sci = 0.0, beta;
           if (xn2 == 0.0 && alpha.y == 0.0) {
@@ -249,12 +269,12 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs a) {
           for (int J = J0; J < J1; ++J) {
             const int j0 = r0g + J * 64;
             const int jmax = min(16, n - (j0 + cg * 16));
-            const cplx* col = C + r + ld * (j0 + cg * 16);
+            const T2* col = C + r + ld * (j0 + cg * 16);
             const cplx* xs = s_x + (J - J0) * 64 + cg * 16;
             if (jmax == 16) {
               cplx xl[16];
 #pragma unroll
-              for (int jj = 0; jj < 16; ++jj) xl[jj] = ldc(col + ld * jj);
+              for (int jj = 0; jj < 16; ++jj) xl[jj] = ldT(col + ld * jj);
 #pragma unroll
               for (int jj = 0; jj < 16; ++jj) {
                 const cplx v = xs[jj];
@@ -264,7 +284,7 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs a) {
               if (J == 0 && cg == 0) acc1 = xl[0];
             } else {
               for (int jj = 0; jj < jmax; ++jj) {
-                const cplx x = ldc(col + ld * jj);
+                const cplx x = ldT(col + ld * jj);
                 const cplx v = xs[jj];
                 acc.x += x.x * v.x - x.y * v.y;
                 acc.y += x.x * v.y + x.y * v.x;
@@ -313,8 +333,8 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs a) {
             for (int u = 0; u < NBT / 4; ++u) {
               const int j = rsub + 4 * u;
               if (j < i) {
-                ps[u] = cadd(ps[u], cmulc(S.V[ch][j][rloc], vr));
-                pt[u] = cadd(pt[u], cmulc(S.W[ch][j][rloc], vr));
+                ps[u] = cadd(ps[u], cmulc(toD(S.V[ch][j][rloc]), vr));
+                pt[u] = cadd(pt[u], cmulc(toD(S.W[ch][j][rloc]), vr));
               }
             }
           }
@@ -370,10 +390,10 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs a) {
       }
       if (lane == 31) s_scal[6] = ldd(red_vav + 2 * i);
     } else if (warp == 1) {
-      if (lane < i) s_vc[lane] = ldc(a.VW + c1 + ld * lane);
+      if (lane < i) s_vc[lane] = ldT(a.VW + c1 + ld * lane);
       if (lane == i) s_vc[i] = cmk(1.0, 0.0);
     } else if (warp == 2) {
-      if (lane < i) s_wc[lane] = ldc(a.VW + c1 + ld * (NBT + lane));
+      if (lane < i) s_wc[lane] = ldT(a.VW + c1 + ld * (NBT + lane));
       if (lane == 31) s_y1 = ldc(ycur + c1);
     }
     cplx yr[MAXCH], cn[MAXCH];
@@ -385,7 +405,7 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs a) {
       const int r = q * RCH + rloc;
       if (r >= c1 && r < n) {
         yr[ch] = ldc(ycur + r);
-        if (upd && rsub == 0) cn[ch] = ldc(C + r + ld * c1);
+        if (upd && rsub == 0) cn[ch] = ldT(C + r + ld * c1);
       }
     }
     __syncthreads();
@@ -423,29 +443,29 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs a) {
       if (act) {
         vr = (r == c1) ? cmk(1.0, 0.0) : cmul(S.X[ch][rloc], scale);
         for (int j = rsub; j < i; j += 4) {
-          acc = cadd(acc, cmul(S.V[ch][j][rloc], s_tv[j]));
-          acc = cadd(acc, cmul(S.W[ch][j][rloc], s_sv[j]));
+          acc = cadd(acc, cmul(toD(S.V[ch][j][rloc]), s_tv[j]));
+          acc = cadd(acc, cmul(toD(S.W[ch][j][rloc]), s_sv[j]));
         }
       }
       acc = shfl4_sum(acc);
       if (act) {
         wr = cadd(cmul(tau, csub(yr[ch], acc)), cscale(vr, alpha));
         if (rsub == 0) {
-          C[r + ld * c] = vr;
-          S.V[ch][i][rloc] = vr;
-          S.W[ch][i][rloc] = wr;
-          a.VW[r + ld * i] = vr;
-          a.WV[r + ld * (NBT + i)] = vr;
-          a.VW[r + ld * (NBT + i)] = wr;
-          a.WV[r + ld * i] = wr;
+          stT(C + r + ld * c, vr);
+          S.V[ch][i][rloc] = fromD<T2>(vr);
+          S.W[ch][i][rloc] = fromD<T2>(wr);
+          stT(a.VW + r + ld * i, vr);
+          stT(a.WV + r + ld * (NBT + i), vr);
+          stT(a.VW + r + ld * (NBT + i), wr);
+          stT(a.WV + r + ld * i, wr);
         }
       }
       if (upd) {
         cplx u = cmk(0.0, 0.0);
         if (act)
           for (int j = rsub; j <= i; j += 4) {
-            const cplx vj = (j == i) ? vr : S.V[ch][j][rloc];
-            const cplx wj = (j == i) ? wr : S.W[ch][j][rloc];
+            const cplx vj = (j == i) ? vr : toD(S.V[ch][j][rloc]);
+            const cplx wj = (j == i) ? wr : toD(S.W[ch][j][rloc]);
             u = cadd(u, cmul_cb(vj, s_wc[j]));
             u = cadd(u, cmul_cb(wj, s_vc[j]));
           }
@@ -456,7 +476,7 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs a) {
             x.y = 0.0;
             a.d[c1] = x.x;
           }
-          C[r + ld * c1] = x;
+          stT(C + r + ld * c1, x);
           S.X[ch][rloc] = x;
           if (r >= c1 + 2) nrm_part += cabs2(x);
         }
@@ -475,9 +495,80 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs a) {
   }
 }
 
-__global__ void k_tail_scalar(int n, cplx* C, long long ld, double* d) {
+template <typename T2>
+__global__ void k_tail_scalar(const T2* C, double* d) {
   // n == 1: nothing to reduce
-  if (threadIdx.x == 0 && blockIdx.x == 0) d[0] = C[0].x;
+  if (threadIdx.x == 0 && blockIdx.x == 0) d[0] = toD(C[0]).x;
+}
+
+// C (m x m, complex64) -= A B^H with A, B m x 2NBT (leading dimension ld):
+// the trailing update of the complex64 reduction, FP32 products.  64 x 64
+// tiles of C per CTA, 16 x 16 threads with 4 x 4 outputs each (rows on the
+// fast thread index for coalesced stores), K staged in two chunks of NBT.
+__global__ void __launch_bounds__(256) k_her2k_f32(int m, const float2* __restrict__ A,
+                                                   const float2* __restrict__ B, long long ld,
+                                                   float2* __restrict__ C) {
+  __shared__ float2 sA[NBT][64 + 1];
+  __shared__ float2 sB[NBT][64 + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
+  float accr[4][4], acci[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) { accr[u][v] = 0.f; acci[u][v] = 0.f; }
+  for (int kc = 0; kc < 2 * NBT; kc += NBT) {
+    for (int e = threadIdx.x; e < 64 * NBT; e += 256) {
+      const int rr = e & 63, kk = e >> 6;
+      const int ra = r0 + rr, cb = c0 + rr;
+      sA[kk][rr] = (ra < m) ? A[ra + ld * (kc + kk)] : make_float2(0.f, 0.f);
+      sB[kk][rr] = (cb < m) ? B[cb + ld * (kc + kk)] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < NBT; ++kk) {
+      float2 av[4], bv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) { av[u] = sA[kk][tx + 16 * u]; bv[u] = sB[kk][ty + 16 * u]; }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {  // a * conj(b)
+          accr[u][v] = fmaf(av[u].x, bv[v].x, fmaf(av[u].y, bv[v].y, accr[u][v]));
+          acci[u][v] = fmaf(av[u].y, bv[v].x, fmaf(-av[u].x, bv[v].y, acci[u][v]));
+        }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    const int cc = c0 + ty + 16 * v;
+    if (cc >= m) continue;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int rr = r0 + tx + 16 * u;
+      if (rr < m) {
+        float2 x = C[rr + ld * cc];
+        x.x -= accr[u][v];
+        x.y -= acci[u][v];
+        C[rr + ld * cc] = x;
+      }
+    }
+  }
+}
+
+// C22 -= [V W] [W V]^H: one K = 2 NBT GEMM in the storage precision
+int her2k_update(excfv_handle* h, int m2, const double2* VW, const double2* WV, long long ld,
+                 double2* C22) {
+  const cplx mone = cmk(-1.0, 0.0), one = cmk(1.0, 0.0);
+  return zgemm1(h->stream, OP_N, OP_C, m2, m2, 2 * NBT, mone, VW, ld, WV, ld, one, C22, ld);
+}
+int her2k_update(excfv_handle* h, int m2, const float2* VW, const float2* WV, long long ld,
+                 float2* C22) {
+  const dim3 grid((m2 + 63) / 64, (m2 + 63) / 64);
+  k_her2k_f32<<<grid, 256, 0, h->stream>>>(m2, VW, WV, ld, C22); count_launch();
+  CUDA_TRY(cudaGetLastError());
+  return EXCFV_OK;
 }
 
 }  // namespace
@@ -485,13 +576,12 @@ __global__ void k_tail_scalar(int n, cplx* C, long long ld, double* d) {
 int tridiag_workspace_doubles() { return NBT + 2 * NBT + 4 * NBT * NBT; }
 int tridiag_nb() { return NBT; }
 
-// Reduces C (n x n, both triangles) to tridiagonal d, e with reflectors
-// stored below the subdiagonal of C (unit entry stored explicitly).
-int tridiag_reduce(excfv_handle* h, int n, cplx* C, long long ld) {
+template <typename T2>
+static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
   Workspace& ws = h->ws;
   cudaStream_t s = h->stream;
   if (n == 1) {
-    k_tail_scalar<<<1, 32, 0, s>>>(n, C, ld, ws.d); count_launch();
+    k_tail_scalar<T2><<<1, 32, 0, s>>>(C, ws.d); count_launch();
     CUDA_TRY(cudaGetLastError());
     return EXCFV_OK;
   }
@@ -501,42 +591,51 @@ int tridiag_reduce(excfv_handle* h, int n, cplx* C, long long ld) {
     excfv_set_error("tridiagonal reduction supports n <= %d on this GPU", MAXCH * G * RCH);
     return EXCFV_ERR_UNSUPPORTED;
   }
-  const int smem = (int)sizeof(PanelSmem);
-  CUDA_TRY(cudaFuncSetAttribute(k_tridiag_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  const int smem = (int)sizeof(PanelSmem<T2>);
+  CUDA_TRY(cudaFuncSetAttribute(k_tridiag_panel<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int per_sm = 0;
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tridiag_panel, TT, smem));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tridiag_panel<T2>, TT, smem));
   if (per_sm < 1) {
     excfv_set_error("tridiag panel kernel cannot be resident");
     return EXCFV_ERR_CUDA;
   }
-  const cplx mone = cmk(-1.0, 0.0), one = cmk(1.0, 0.0);
-  cplx* VW = ws.Wp;
-  cplx* WV = ws.Wp + (size_t)ws.nmatmax * 2 * NBT;
+  // [V W] and [W V] of the panel in the storage type, inside ws.Wp
+  T2* VW = reinterpret_cast<T2*>(ws.Wp);
+  T2* WV = VW + (size_t)ws.nmatmax * 2 * NBT;
   for (int p = 0; p < n - 1; p += NBT) {
     const int nbp = min(NBT, n - 1 - p);
     const int final_panel = (p + nbp == n - 1) ? 1 : 0;
     CUDA_TRY(cudaMemsetAsync(ws.red, 0, sizeof(double) * tridiag_workspace_doubles(), s));
     CUDA_TRY(cudaMemsetAsync(ws.bar, 0, 2 * sizeof(unsigned), s));
-    TridArgs ta;
+    TridArgs<T2> ta;
     ta.n = n; ta.ld = ld; ta.C = C; ta.VW = VW; ta.WV = WV; ta.d = ws.d; ta.e = ws.e;
     ta.tau = ws.tau; ta.ybuf = ws.ybuf; ta.red = ws.red; ta.bar = ws.bar; ta.status = ws.status;
     ta.p = p; ta.nbp = nbp; ta.final_panel = final_panel;
     void* args[] = {&ta};
     prof_begin(h, PROF_TRD_PANEL);
-    CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_tridiag_panel, dim3(G), dim3(TT), args,
+    CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_tridiag_panel<T2>, dim3(G), dim3(TT), args,
                                          (size_t)smem, s));
     count_launch();
     prof_end(h, PROF_TRD_PANEL);
     if (!final_panel) {
       prof_begin(h, PROF_TRD_UPDATE);
       const int q = p + nbp;
-      const int m2 = n - q;
       // C22 -= [V W] [W V]^H (both triangles; the next panel's y = C22 v reads both)
-      int rc = zgemm1(s, OP_N, OP_C, m2, m2, 2 * NBT, mone, VW + q, ld, WV + q, ld, one,
-                      C + q + ld * q, ld);
+      int rc = her2k_update(h, n - q, VW + q, WV + q, ld, C + q + ld * q);
       if (rc) return rc;
       prof_end(h, PROF_TRD_UPDATE);
     }
   }
   return EXCFV_OK;
+}
+
+// Reduces C (n x n, both triangles) to tridiagonal d, e with reflectors
+// stored below the diagonal of C (unit entry stored explicitly).
+int tridiag_reduce(excfv_handle* h, int n, cplx* C, long long ld) {
+  return tridiag_reduce_t<double2>(h, n, C, ld);
+}
+
+// The same on a complex64 matrix (d, e and tau stay FP64).
+int tridiag_reduce_f32(excfv_handle* h, int n, float2* C, long long ld) {
+  return tridiag_reduce_t<float2>(h, n, C, ld);
 }

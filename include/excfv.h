@@ -44,7 +44,12 @@ extern "C" {
 
 /* precision forms */
 #define EXCFV_PREC_FP64 0  /* FP64 end to end */
-#define EXCFV_PREC_MIXED 1 /* split-BF16 tensor-core setup + FP32 reduction + FP64 refinement */
+/* FP64 setup, Cholesky and reduction to standard form; Householder tridiagonal
+   reduction in complex64 storage for k' = k + max(16, k/8) states; FP64
+   Rayleigh-Ritz on those k' vectors.  Matrices of order <= 64 use the FP64
+   solver.  Eigenvalues agree with ZHEGVX to ~1e-12 Ha; residuals of the
+   eigenvectors are ~1e-8 relative (first order in the complex64 rounding). */
+#define EXCFV_PREC_MIXED 1
 
 typedef struct excfv_handle excfv_handle;
 

@@ -1,0 +1,95 @@
+"""GPU parity of the precision form (EXCFV_PREC_MIXED) against the oracle.
+
+The precision form reduces C = U^-H H U^-1 to tridiagonal form in complex64
+storage, carries k' = k + max(16, k/8) states through the eigensolver and
+restores FP64 accuracy with a Rayleigh-Ritz step in FP64.  Its bar is the
+metric's: eigenvalues within 1e-8 Ha of ZHEGVX.  Eigenvectors are O-orthonormal
+to FP64 rounding (both the Ritz basis and the Ritz vectors are orthonormalised
+in FP64); their residuals are those of Ritz vectors from a complex64 basis,
+first order in the FP32 perturbation (2e-8 relative to ||H||_F measured on the
+diamond cell), and are bounded here at RES_TOL = 1e-7.  The Ritz values are
+second order: measured within 2e-12 Ha of ZHEGVX.
+"""
+import numpy as np
+import pytest
+
+from exciting_b200 import synthetic as syn
+from exciting_b200.lib import EXCFV_PREC_MIXED
+from oracle import fvref
+
+pytestmark = pytest.mark.gpu
+
+EIG_TOL = 1e-8
+RES_TOL = 1e-7
+ORTH_TOL = 1e-11
+
+
+@pytest.fixture(scope="module")
+def mixed_fv():
+    from exciting_b200.fv import FirstVariational
+    fv = FirstVariational(0, precision=EXCFV_PREC_MIXED)
+    yield fv
+    fv.close()
+
+
+def _ref(st, kp):
+    A = fvref.match(st, kp)
+    H, O = fvref.hamiltonandoverlapsetup(st, kp, A)
+    w, X, info = fvref.solvewithlapack(H, O, st.nstfv, st.evaltol)
+    assert info == 0
+    return H, O, w, X
+
+
+def _check(H, O, w, X, w_ref):
+    n = H.shape[0]
+    assert np.abs(w - w_ref).max() < EIG_TOL
+    assert fvref.residuals(H, O, w, X[:n]).max() < RES_TOL
+    assert fvref.o_orthonormality(O, X[:n]) < ORTH_TOL
+
+
+def test_mixed_cubic8_full_size(mixed_fv):
+    """n = 1964, lowest 200 states, through excfv_seceqn."""
+    p = syn.make_problem("cubic8")
+    st, kp = p.static, p.kpts[0]
+    H, O, w_ref, _ = _ref(st, kp)
+    mixed_fv.set_static(st)
+    w, X = mixed_fv.seceqn(kp, nmatmax=kp.nmat + 5)
+    assert np.all(X[kp.nmat:] == 0)
+    _check(H, O, w, X, w_ref)
+
+
+@pytest.mark.parametrize("nstfv", [1, 20, 300])
+def test_mixed_diamond2_state_counts(mixed_fv, nstfv):
+    """A single state, the default count, and k' clipped at n (300 of n = 316)."""
+    p = syn.make_problem("diamond2", nstfv=nstfv)
+    st, kp = p.static, p.kpts[0]
+    H, O, w_ref, _ = _ref(st, kp)
+    mixed_fv.set_static(st)
+    w, X = mixed_fv.seceqn(kp)
+    _check(H, O, w, X, w_ref)
+
+
+def test_mixed_small_matrix_uses_fp64(mixed_fv):
+    """n <= 64 takes the FP64 solver even in the precision form."""
+    p = syn.make_problem("diamond2", ngk=40, nstfv=12)
+    st, kp = p.static, p.kpts[0]
+    assert kp.nmat <= 64
+    H, O, w_ref, _ = _ref(st, kp)
+    mixed_fv.set_static(st)
+    w, X = mixed_fv.seceqn(kp)
+    assert np.abs(w - w_ref).max() < 1e-10
+    assert fvref.residuals(H, O, w, X[:kp.nmat]).max() < 1e-13
+
+
+def test_mixed_batched(mixed_fv):
+    """Uneven k-points on two lanes, each lane with its own Rayleigh-Ritz context."""
+    p = syn.make_problem("cubic8", nk=4, ngk_range=(260, 420), nstfv=24)
+    refs = [_ref(p.static, kp) for kp in p.kpts]
+    mixed_fv.set_static(p.static)
+    mixed_fv.set_lanes(2)
+    outs, info = mixed_fv.seceqn_batched(p.kpts, p.nmatmax)
+    mixed_fv.set_lanes(0)
+    assert np.all(info == 0)
+    for (H, O, w_ref, _), kp, (w, X) in zip(refs, p.kpts, outs):
+        _check(H, O, w, X, w_ref)
+        assert np.all(X[kp.nmat:] == 0)
