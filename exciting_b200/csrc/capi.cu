@@ -342,8 +342,9 @@ int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax) {
     return rc;
   }
   ws.part_cap = std::max((size_t)(8u << 20), n * 64 * 4);
-  CUDA_TRY(cudaMemset(ws.status, 0, ST_NWORDS * sizeof(int)));
-  CUDA_TRY(cudaMemset(ws.bar, 0, 4 * sizeof(unsigned)));
+  // zeroed in the handle's stream order (lane streams do not wait for the legacy stream)
+  CUDA_TRY(cudaMemsetAsync(ws.status, 0, ST_NWORDS * sizeof(int), h->stream));
+  CUDA_TRY(cudaMemsetAsync(ws.bar, 0, 4 * sizeof(unsigned), h->stream));
   ws.nmatmax = (int)nmatmax;
   ws.ngkmax = (int)ngkmax;
   ws.kmax = (int)kmax;
@@ -681,6 +682,10 @@ int excfv_seceqn(excfv_handle* h, int32_t ik, int32_t nmatp, int32_t ngp, int32_
 int excfv_sync(excfv_handle* h) {
   if (!h) return EXCFV_ERR_ARG;
   DeviceGuard g(h->device);
+  if (!h->ws.status) {  // only batched calls so far: their status is read by excfv_batch_info
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return EXCFV_OK;
+  }
   return stage_status(h, 0);
 }
 

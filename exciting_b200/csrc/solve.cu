@@ -69,19 +69,24 @@ __global__ void __launch_bounds__(LT) k_larft(int n, const cplx* Gall, const cpl
   for (int t = tid; t < NBQ * NBQ; t += LT) out[t] = T[t % NBQ][t / NBQ];
 }
 
-__global__ void k_to_f32(long long cnt, const cplx* __restrict__ in, float2* __restrict__ out) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < cnt) out[t] = make_float2((float)in[t].x, (float)in[t].y);
+// n x n FP64 (leading dimension ldi) -> complex64 (leading dimension ldo)
+__global__ void k_to_f32(int n, const cplx* __restrict__ in, long long ldi, float2* __restrict__ out,
+                         long long ldo) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (r >= n) return;
+  const cplx v = in[r + ldi * c];
+  out[r + ldo * c] = make_float2((float)v.x, (float)v.y);
 }
 
 // reflectors (below the diagonal) of an n x n complex64 matrix -> FP64
-__global__ void k_lower_to_f64(int n, const float2* __restrict__ in, long long ld,
-                               cplx* __restrict__ out) {
+__global__ void k_lower_to_f64(int n, const float2* __restrict__ in, long long ldi,
+                               cplx* __restrict__ out, long long ldo) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   const int c = blockIdx.y;
   if (r >= n || r <= c) return;
-  const float2 v = in[r + ld * c];
-  out[r + ld * c] = cmk((double)v.x, (double)v.y);
+  const float2 v = in[r + ldi * c];
+  out[r + ldo * c] = cmk((double)v.x, (double)v.y);
 }
 
 // status words of the nested Rayleigh-Ritz solve added into the caller's
@@ -278,15 +283,16 @@ static int stage_solve_mixed(excfv_handle* h, int n, int k, double evaltol, doub
                    TRI_LOWER, TRI_NONE)))
     return rc;
   if ((rc = mirror_upper(s, n, ws.H, ld))) return rc;
-  // complex64 copy of C for the reduction (ws.T is free now)
+  // complex64 copy of C for the reduction (ws.T is free now); an even leading
+  // dimension keeps its columns 16-byte aligned for the tile loads
   float2* Cf = reinterpret_cast<float2*>(ws.T);
-  const long long nn = (long long)n * n;
-  k_to_f32<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(nn, ws.H, Cf); count_launch();
+  const long long ldf = (n + 1) & ~1;
+  k_to_f32<<<dim3((n + 255) / 256, n), 256, 0, s>>>(n, ws.H, ld, Cf, ldf); count_launch();
   CUDA_TRY(cudaGetLastError());
   prof_end(h, PROF_HEGST);
-  if ((rc = tridiag_reduce_f32(h, n, Cf, ld))) return rc;
+  if ((rc = tridiag_reduce_f32(h, n, Cf, ldf))) return rc;
   // reflectors back to FP64 into ws.O (the Cholesky factor is no longer needed)
-  k_lower_to_f64<<<dim3((n + 255) / 256, n), 256, 0, s>>>(n, Cf, ld, ws.O); count_launch();
+  k_lower_to_f64<<<dim3((n + 255) / 256, n), 256, 0, s>>>(n, Cf, ldf, ws.O, ld); count_launch();
   CUDA_TRY(cudaGetLastError());
   cplx* Z = ws.Z;
   prof_begin(h, PROF_STEIG);

@@ -25,6 +25,9 @@
 // other CTAs inside the kernel use ld.global.cg (L2), since L1 is not
 // coherent across SMs.  Barrier waits are bounded in time; a timeout sets
 // status[ST_BARRIER] and every CTA then leaves the kernel.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "handle.cuh"
 
 namespace {
@@ -71,6 +74,70 @@ __device__ __forceinline__ long long gtimer() {
 }
 __device__ __forceinline__ cplx ldc(const cplx* p) { return __ldcg(p); }
 __device__ __forceinline__ double ldd(const double* p) { return __ldcg(p); }
+
+// Tiles of the trailing matrix for y = C22 v: 64 rows x BC columns (16 KB),
+// streamed through a ring of STAGES shared-memory slots by TMA.
+template <typename T2>
+struct Ring {
+  static constexpr int BC = (sizeof(T2) == 16) ? 16 : 32;
+  static constexpr int STAGES = (sizeof(T2) == 16) ? 4 : 8;
+  static constexpr int TILE = RCH * BC;  // elements
+  static constexpr unsigned BYTES = TILE * sizeof(T2);
+};
+constexpr int MAX_STAGES = 8;
+
+template <typename T2>
+constexpr size_t panel_smem_bytes() {
+  return sizeof(PanelSmem<T2>) + 128 + (size_t)Ring<T2>::STAGES * Ring<T2>::BYTES;
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for a TMA tile; gives up (status[ST_BARRIER] set) after 2 s or
+// as soon as another wait of the launch has given up.
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, int* status) {
+  if (mbar_try_wait(bar, parity)) return;
+  const long long t0 = gtimer();
+  unsigned it = 0;
+  while (!mbar_try_wait(bar, parity)) {
+    if ((++it & 63u) == 0) {
+      if (*(volatile int*)&status[ST_BARRIER] != 0) return;
+      if (gtimer() - t0 > BARRIER_NS) {
+        atomicAdd(&status[ST_BARRIER], 1);
+        return;
+      }
+    }
+  }
+}
+// 2-D tiled TMA load (no multicast) of one 64 x BC tile; x counts scalars
+// (re and im separately) along the rows, y counts columns.
+__device__ __forceinline__ void tma_tile(void* dst, const CUtensorMap* tm, int x, int y,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
 
 // Grid barrier on a monotonic arrival counter (zeroed before each launch):
 // barrier number e completes when the counter reaches e * gridDim.x.
@@ -144,13 +211,22 @@ __device__ __forceinline__ cplx warp_sum(cplx v) {
 constexpr int JB = 8;  // column tiles whose x values are staged per round trip
 
 template <typename T2>
-__global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs<T2> a) {
-  extern __shared__ __align__(16) unsigned char dsm[];
+__global__ void __launch_bounds__(TT, 1)
+    k_tridiag_panel(TridArgs<T2> a, const __grid_constant__ CUtensorMap tmap) {
+  using R = Ring<T2>;
+  extern __shared__ __align__(128) unsigned char dsm[];
   PanelSmem<T2>& S = *reinterpret_cast<PanelSmem<T2>*>(dsm);
+  T2* ring;
+  {
+    const unsigned b0 = smem_u32(dsm);
+    const unsigned r0 = (b0 + (unsigned)sizeof(PanelSmem<T2>) + 127u) & ~127u;
+    ring = reinterpret_cast<T2*>(dsm + (r0 - b0));
+  }
+  __shared__ __align__(8) uint64_t s_full[MAX_STAGES];
   __shared__ cplx s_vc[NBT], s_wc[NBT];   // row c+1 of V and W
   __shared__ cplx s_sv[NBT], s_tv[NBT];   // V^H v, W^H v of the current column
   __shared__ cplx s_acc_s[NBT], s_acc_t[NBT];
-  __shared__ cplx s_x[JB * 64];           // staged x values of the trailing column
+  __shared__ T2 s_x[JB * 64];             // staged x values of the trailing column
   __shared__ cplx s_xr[64];               // x values of the item's rows
   __shared__ cplx s_part[TT];
   __shared__ double s_dred[TT / 32];
@@ -169,6 +245,12 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs<T2> a) {
   double* red_t = a.red + 3 * NBT + 2 * NBT * NBT;
   const int nch = (n + RCH - 1) / RCH;
   unsigned epoch = 0;
+  unsigned gtile = 0;  // tiles consumed by this CTA (ring slot and mbarrier phase)
+  if (tid == 0) {
+    for (int q = 0; q < R::STAGES; ++q) mbar_init(&s_full[q], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
 
   // ---- prologue: column p needs no update; its norm and diagonal
   {
@@ -208,10 +290,13 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs<T2> a) {
 
     // ================= phase 2: reflector of column c, y = C22 v =================
     // y = C22 v with v(c+1) = 1, v(j) = scale x(j): accumulate C22 x~ (x~(c+1) = 0)
-    // and the column c+1 separately, so the loads do not wait for the reflector.
+    // and the column c+1 separately, so that the tile loads do not wait for the
+    // reflector.  The tile grid starts at row and column rb (even for complex64:
+    // the TMA row coordinate needs 16-byte alignment); rows and columns below
+    // c+1 carry zero weight.  Every CTA computes the reflector scalars.
     const int r0g = c + 1;
-    const int m2 = n - r0g;
-    const int nt = (m2 + 63) / 64;
+    const int rb = (sizeof(T2) == 8) ? (r0g & ~1) : r0g;
+    const int nt = (n - rb + 63) / 64;
     int Sg = G / nt;
     if (Sg < 1) Sg = 1;
     if (Sg > nt) Sg = nt;
@@ -219,88 +304,110 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs<T2> a) {
     const int items = nt * Sg;
     const int rr = tid & 63, cg = tid >> 6;
     double vav_re = 0.0, vav_im = 0.0;
-    bool have_scal = false;
     if (tid < NBT) { s_acc_s[tid] = cmk(0.0, 0.0); s_acc_t[tid] = cmk(0.0, 0.0); }
-    for (int it = bid; it < items || !have_scal; it += G) {
-      const bool real_item = it < items;
-      const int I = it / Sg, seg = it % Sg;
-      const int r = r0g + I * 64 + rr;
-      const int Jb = seg * per, Je = real_item ? min(nt, Jb + per) : Jb;
-      cplx acc = cmk(0.0, 0.0), acc1 = cmk(0.0, 0.0);
-      for (int J0 = Jb; J0 < Je || (J0 == Jb && !have_scal); J0 += JB) {
-        const int J1 = min(Je, J0 + JB);
-        // stage x values of tiles J0..J1-1 (and of the item's rows on the first chunk)
-        cplx xv0 = cmk(0.0, 0.0), xv1 = cmk(0.0, 0.0), xrow = cmk(0.0, 0.0);
-        {
-          const int j_a = r0g + J0 * 64 + tid, j_b = j_a + TT;
-          const int lim = r0g + J1 * 64;
-          if (j_a < lim && j_a < n && j_a != c + 1) xv0 = ldT(C + j_a + ld * c);
-          if (j_b < lim && j_b < n && j_b != c + 1) xv1 = ldT(C + j_b + ld * c);
-          if (J0 == Jb && tid < 64 && real_item) {
-            const int rr2 = r0g + I * 64 + tid;
-            if (rr2 < n && rr2 != c + 1) xrow = ldT(C + rr2 + ld * c);
-          }
-        }
-        if (!have_scal && tid == 0) {
-          const cplx alpha = ldT(C + (c + 1) + ld * c);
-          const double xn2 = ldd(red_norm + i);
-          double tr = 0.0, ti = 0.0, scr = 0.0, sci = 0.0, beta;
-          if (xn2 == 0.0 && alpha.y == 0.0) {
-            beta = alpha.x;
-          } else {
-            const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
-            beta = (alpha.x >= 0.0) ? -nrm : nrm;
-            tr = (beta - alpha.x) / beta;
-            ti = -alpha.y / beta;
-            const double dr = alpha.x - beta, di = alpha.y;  // scale = 1 / (alpha - beta)
-            const double den = dr * dr + di * di;
-            scr = dr / den;
-            sci = -di / den;
-          }
-          s_scal[0] = tr; s_scal[1] = ti; s_scal[2] = scr; s_scal[3] = sci; s_scal[5] = beta;
-        }
-        __syncthreads();
-        s_x[tid] = xv0;
-        s_x[tid + TT] = xv1;
-        if (J0 == Jb && tid < 64) s_xr[tid] = xrow;
-        __syncthreads();
-        have_scal = true;
-        if (r < n && real_item) {
-          for (int J = J0; J < J1; ++J) {
-            const int j0 = r0g + J * 64;
-            const int jmax = min(16, n - (j0 + cg * 16));
-            const T2* col = C + r + ld * (j0 + cg * 16);
-            const cplx* xs = s_x + (J - J0) * 64 + cg * 16;
-            if (jmax == 16) {
-              cplx xl[16];
-#pragma unroll
-              for (int jj = 0; jj < 16; ++jj) xl[jj] = ldT(col + ld * jj);
-#pragma unroll
-              for (int jj = 0; jj < 16; ++jj) {
-                const cplx v = xs[jj];
-                acc.x += xl[jj].x * v.x - xl[jj].y * v.y;
-                acc.y += xl[jj].x * v.y + xl[jj].y * v.x;
-              }
-              if (J == 0 && cg == 0) acc1 = xl[0];
-            } else {
-              for (int jj = 0; jj < jmax; ++jj) {
-                const cplx x = ldT(col + ld * jj);
-                const cplx v = xs[jj];
-                acc.x += x.x * v.x - x.y * v.y;
-                acc.y += x.x * v.y + x.y * v.x;
-                if (J == 0 && cg == 0 && jj == 0) acc1 = x;
-              }
-            }
-          }
-        }
-        if (J1 >= Je) break;
+    // issue the leading tiles of item `it` (thread 0)
+    auto issue_lead = [&](int it, unsigned g0) {
+      const int I = it / Sg, Jb = (it % Sg) * per, Je = min(nt, Jb + per);
+      if (Jb >= Je) return;
+      const int colb = rb + Jb * 64;
+      const int ntile = (min(n, rb + Je * 64) - colb + R::BC - 1) / R::BC;
+      for (int b = 0; b < min(R::STAGES, ntile); ++b) {
+        const unsigned q = (g0 + b) % R::STAGES;
+        mbar_expect_tx(&s_full[q], R::BYTES);
+        tma_tile(ring + (size_t)q * R::TILE, &tmap, 2 * (rb + I * 64), colb + b * R::BC, &s_full[q]);
       }
-      if (!real_item) break;
+    };
+    if (tid == 0 && bid < items) issue_lead(bid, gtile);
+    if (tid == 0) {
+      const cplx alpha = ldT(C + (c + 1) + ld * c);
+      const double xn2 = ldd(red_norm + i);
+      double tr = 0.0, ti = 0.0, scr = 0.0, sci = 0.0, beta;
+      if (xn2 == 0.0 && alpha.y == 0.0) {
+        beta = alpha.x;
+      } else {
+        const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
+        beta = (alpha.x >= 0.0) ? -nrm : nrm;
+        tr = (beta - alpha.x) / beta;
+        ti = -alpha.y / beta;
+        const double dr = alpha.x - beta, di = alpha.y;  // scale = 1 / (alpha - beta)
+        const double den = dr * dr + di * di;
+        scr = dr / den;
+        sci = -di / den;
+      }
+      s_scal[0] = tr; s_scal[1] = ti; s_scal[2] = scr; s_scal[3] = sci; s_scal[5] = beta;
+    }
+    for (int it = bid; it < items; it += G) {
+      const int I = it / Sg, Jb = (it % Sg) * per, Je = min(nt, Jb + per);
+      if (Jb >= Je) continue;
+      const int row0 = rb + I * 64;
+      const int colb = rb + Jb * 64;
+      const int ntile = (min(n, rb + Je * 64) - colb + R::BC - 1) / R::BC;
+      if (tid == 0 && it != bid) issue_lead(it, gtile);
+      const int r = row0 + rr;
+      cplx acc = cmk(0.0, 0.0), acc1 = cmk(0.0, 0.0);
+      int b = 0;
+      for (int g0 = Jb; g0 < Je; g0 += JB) {
+        const int g1 = min(Je, g0 + JB);
+        __syncthreads();  // the previous group's x values are consumed
+        {
+          const int j_a = rb + g0 * 64 + tid, j_b = j_a + TT;
+          const int lim = min(n, rb + g1 * 64);
+          s_x[tid] = fromD<T2>((j_a < lim && j_a > c + 1) ? ldT(C + j_a + ld * c) : cmk(0.0, 0.0));
+          s_x[tid + TT] = fromD<T2>((j_b < lim && j_b > c + 1) ? ldT(C + j_b + ld * c) : cmk(0.0, 0.0));
+          if (g0 == Jb && tid < 64) {
+            const int r2 = row0 + tid;
+            s_xr[tid] = (r2 < n && r2 > c + 1) ? ldT(C + r2 + ld * c) : cmk(0.0, 0.0);
+          }
+        }
+        __syncthreads();
+        const int bend = min(ntile, (g1 - Jb) * (64 / R::BC));
+        for (; b < bend; ++b) {
+          const unsigned q = gtile + b;
+          const unsigned slot = q % R::STAGES;
+          mbar_wait(&s_full[slot], (q / R::STAGES) & 1u, a.status);
+          const T2* tile = ring + (size_t)slot * R::TILE;
+          constexpr int CPT = R::BC / 4;         // columns per thread
+          const int cl = cg * CPT;                // first column of this thread in the tile
+          const int xo = b * R::BC - (g0 - Jb) * 64 + cl;
+          const int j0 = colb + b * R::BC + cl;
+          if constexpr (sizeof(T2) == 16) {
+#pragma unroll
+            for (int u = 0; u < CPT; ++u) {
+              const cplx av = toD(tile[(cl + u) * RCH + rr]);
+              const cplx xv = toD(s_x[xo + u]);
+              acc.x += av.x * xv.x - av.y * xv.y;
+              acc.y += av.x * xv.y + av.y * xv.x;
+              if (j0 + u == c + 1) acc1 = av;
+            }
+          } else {
+            float pr = 0.f, pi = 0.f;
+#pragma unroll
+            for (int u = 0; u < CPT; ++u) {
+              const T2 av = tile[(cl + u) * RCH + rr];
+              const T2 xv = s_x[xo + u];
+              pr = fmaf(av.x, xv.x, fmaf(-av.y, xv.y, pr));
+              pi = fmaf(av.x, xv.y, fmaf(av.y, xv.x, pi));
+              if (j0 + u == c + 1) acc1 = toD(av);
+            }
+            acc.x += (double)pr;
+            acc.y += (double)pi;
+          }
+          // The slot is refilled by the async proxy (TMA): order this thread's
+          // generic reads of it before that write, then release it to thread 0.
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncthreads();
+          if (tid == 0 && b + R::STAGES < ntile) {
+            mbar_expect_tx(&s_full[slot], R::BYTES);
+            tma_tile(ring + (size_t)slot * R::TILE, &tmap, 2 * row0,
+                     colb + (b + R::STAGES) * R::BC, &s_full[slot]);
+          }
+        }
+      }
+      gtile += ntile;
       const cplx scale = cmk(s_scal[2], s_scal[3]);
-      __syncthreads();
       s_part[tid] = cadd(cmul(scale, acc), acc1);
       __syncthreads();
-      if (tid < 64 && r < n) {
+      if (tid < 64 && r < n && r >= r0g) {
         cplx sum = cadd(cadd(s_part[tid], s_part[tid + 64]), cadd(s_part[tid + 128], s_part[tid + 192]));
         atomicAdd(&ycur[r].x, sum.x);
         atomicAdd(&ycur[r].y, sum.y);
@@ -309,6 +416,7 @@ __global__ void __launch_bounds__(TT, 1) k_tridiag_panel(TridArgs<T2> a) {
         vav_im += vr.x * sum.y - vr.y * sum.x;
       }
     }
+    __syncthreads();  // the scalars of thread 0 are visible
     const cplx scale = cmk(s_scal[2], s_scal[3]);
     for (int o = 16; o > 0; o >>= 1) {
       vav_re += __shfl_xor_sync(0xffffffffu, vav_re, o);
@@ -576,6 +684,48 @@ int her2k_update(excfv_handle* h, int m2, const float2* VW, const float2* WV, lo
 int tridiag_workspace_doubles() { return NBT + 2 * NBT + 4 * NBT * NBT; }
 int tridiag_nb() { return NBT; }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point
+static PFN_cuTensorMapEncodeTiled_v12000 encode_tiled_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// Tensor map of the n x n matrix C (leading dimension ld) as real scalars:
+// 2n rows of re/im pairs, n columns; tiles of 64 complex rows x BC columns.
+template <typename T2>
+static int make_tile_map(CUtensorMap* tm, const T2* C, int n, long long ld) {
+  auto fn = encode_tiled_fn();
+  if (!fn) {
+    excfv_set_error("cuTensorMapEncodeTiled is not available from the driver");
+    return EXCFV_ERR_CUDA;
+  }
+  if ((reinterpret_cast<uintptr_t>(C) & 15) || ((ld * sizeof(T2)) & 15)) {
+    excfv_set_error("tridiagonal reduction: matrix base or column stride not 16-byte aligned");
+    return EXCFV_ERR_ARG;
+  }
+  const cuuint64_t dims[2] = {2ull * (cuuint64_t)n, (cuuint64_t)n};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(T2)};
+  const cuuint32_t box[2] = {2u * RCH, (cuuint32_t)Ring<T2>::BC};
+  const cuuint32_t estr[2] = {1u, 1u};
+  const CUtensorMapDataType dt =
+      (sizeof(T2) == 16) ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const CUresult r = fn(tm, dt, 2, const_cast<T2*>(C), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    excfv_set_error("cuTensorMapEncodeTiled failed (%d) for n=%d ld=%lld", (int)r, n, ld);
+    return EXCFV_ERR_CUDA;
+  }
+  return EXCFV_OK;
+}
+
 template <typename T2>
 static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
   Workspace& ws = h->ws;
@@ -591,7 +741,9 @@ static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
     excfv_set_error("tridiagonal reduction supports n <= %d on this GPU", MAXCH * G * RCH);
     return EXCFV_ERR_UNSUPPORTED;
   }
-  const int smem = (int)sizeof(PanelSmem<T2>);
+  const int smem = (int)panel_smem_bytes<T2>();
+  CUtensorMap tmap;
+  if (int rc = make_tile_map(&tmap, C, n, ld)) return rc;
   CUDA_TRY(cudaFuncSetAttribute(k_tridiag_panel<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int per_sm = 0;
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tridiag_panel<T2>, TT, smem));
@@ -599,9 +751,15 @@ static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
     excfv_set_error("tridiag panel kernel cannot be resident");
     return EXCFV_ERR_CUDA;
   }
-  // [V W] and [W V] of the panel in the storage type, inside ws.Wp
+  // [V W] and [W V] of the panel in the storage type, both with leading
+  // dimension ld, inside ws.Wp (n_max x 4 NBT FP64 complex: room for ld <= n_max
+  // in FP64 storage and ld <= 2 n_max in complex64)
+  if ((size_t)ld * 2 * NBT * 2 * sizeof(T2) > (size_t)ws.nmatmax * 4 * NBT * sizeof(cplx)) {
+    excfv_set_error("tridiagonal reduction: leading dimension %lld exceeds the panel workspace", ld);
+    return EXCFV_ERR_ARG;
+  }
   T2* VW = reinterpret_cast<T2*>(ws.Wp);
-  T2* WV = VW + (size_t)ws.nmatmax * 2 * NBT;
+  T2* WV = VW + (size_t)ld * 2 * NBT;
   for (int p = 0; p < n - 1; p += NBT) {
     const int nbp = min(NBT, n - 1 - p);
     const int final_panel = (p + nbp == n - 1) ? 1 : 0;
@@ -611,7 +769,7 @@ static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
     ta.n = n; ta.ld = ld; ta.C = C; ta.VW = VW; ta.WV = WV; ta.d = ws.d; ta.e = ws.e;
     ta.tau = ws.tau; ta.ybuf = ws.ybuf; ta.red = ws.red; ta.bar = ws.bar; ta.status = ws.status;
     ta.p = p; ta.nbp = nbp; ta.final_panel = final_panel;
-    void* args[] = {&ta};
+    void* args[] = {&ta, &tmap};
     prof_begin(h, PROF_TRD_PANEL);
     CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_tridiag_panel<T2>, dim3(G), dim3(TT), args,
                                          (size_t)smem, s));

@@ -93,3 +93,47 @@ def test_mixed_batched(mixed_fv):
     for (H, O, w_ref, _), kp, (w, X) in zip(refs, p.kpts, outs):
         _check(H, O, w, X, w_ref)
         assert np.all(X[kp.nmat:] == 0)
+
+
+def test_mixed_concurrent_lanes_device_pointers():
+    """Large k-points on four concurrent lanes through the device-pointer entry point.
+
+    Every lane keeps several complex64 panel reductions in flight next to the
+    other lanes' kernels, and each lane runs more than one k-point, so a tile
+    of the shared-memory ring is refilled while other work competes for the
+    memory system.  Eigenvalues must match the FP64 form's (itself held to the
+    oracle) within the precision form's bar.
+    """
+    import torch
+    from exciting_b200.fv import FirstVariational
+    from exciting_b200.lib import EXCFV_PREC_FP64
+    p = syn.make_problem("cubic8", nk=12, ngk_range=(1800 - 64, 2300 - 64))
+    st = p.static
+
+    def dv(a, dt):
+        return torch.from_numpy(np.asfortranarray(np.asarray(a, dtype=dt)).ravel(order="F")).to("cuda:0")
+
+    ins = [{n: dv(getattr(k, n), dt) for n, dt in (("gpc", np.float64), ("tpgpc", np.float64),
+                                                   ("sfacgp", np.complex128), ("igpig", np.int32),
+                                                   ("vgpc", np.float64))} for k in p.kpts]
+    res = {}
+    for prec in (EXCFV_PREC_FP64, EXCFV_PREC_MIXED):
+        ev = [torch.zeros(st.nstfv, dtype=torch.float64, device="cuda:0") for _ in p.kpts]
+        X = [torch.zeros(p.nmatmax * st.nstfv, dtype=torch.complex128, device="cuda:0") for _ in p.kpts]
+        with FirstVariational(0, precision=prec) as fv:
+            fv.set_static(st)
+            fv.set_lanes(4)
+            for _ in range(2):
+                fv.seceqn_batched_dev([k.nmat for k in p.kpts], [k.ngp for k in p.kpts], p.ngkmax,
+                                      [d["gpc"].data_ptr() for d in ins], [d["tpgpc"].data_ptr() for d in ins],
+                                      [d["sfacgp"].data_ptr() for d in ins], [d["igpig"].data_ptr() for d in ins],
+                                      [d["vgpc"].data_ptr() for d in ins], p.nmatmax,
+                                      [e.data_ptr() for e in ev], [x.data_ptr() for x in X])
+                fv.sync()
+                torch.cuda.synchronize()
+                assert np.all(fv.batch_info(len(p.kpts)) == 0)
+                res.setdefault(prec, []).append(np.array([e.cpu().numpy() for e in ev]))
+    ref = res[EXCFV_PREC_FP64][0]
+    assert np.abs(res[EXCFV_PREC_FP64][1] - ref).max() < 1e-12
+    for w in res[EXCFV_PREC_MIXED]:
+        assert np.abs(w - ref).max() < EIG_TOL
