@@ -51,12 +51,15 @@ def cores_used():
 # CPU: the reference algorithm (oracle port) timed on the host cores
 # ---------------------------------------------------------------------------
 
-def time_cpu_reference(p, steps: int, warmup: int, min_seconds: float = 0.0):
+def time_cpu_reference(p, steps: int, warmup: int, min_seconds: float = 0.0, keep_first=False):
     from oracle import fvref
     st = p.static
     times = []
+    first = None
     for i in range(warmup):
-        fvref.seceqn(st, p.kpts[i % len(p.kpts)])
+        w, X, info = fvref.seceqn(st, p.kpts[i % len(p.kpts)])
+        if i == 0:
+            first = w
     t_all = time.perf_counter()
     i = 0
     while i < steps or (time.perf_counter() - t_all) < min_seconds:
@@ -64,10 +67,12 @@ def time_cpu_reference(p, steps: int, warmup: int, min_seconds: float = 0.0):
         t0 = time.perf_counter()
         w, X, info = fvref.seceqn(st, kp)
         times.append(time.perf_counter() - t0)
+        if first is None:
+            first = w
         i += 1
         if i >= 10 * max(steps, 1):
             break
-    return times
+    return (times, first) if keep_first else times
 
 
 # ---------------------------------------------------------------------------
@@ -170,15 +175,16 @@ def load_traffic():
 # batching form
 # ---------------------------------------------------------------------------
 
-def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn):
+def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn, prec):
     from exciting_b200.fv import FirstVariational
+    from exciting_b200.lib import EXCFV_PREC_MIXED
     import torch.distributed as dist
     nk = args.batch_nk
     # nmat = ngk + 64 (8 atoms x 8 local orbitals) uniform in [1800, 2300]
     pb = syn.make_problem("cubic8", nk=nk * world, ngk_range=(1800 - 64, 2300 - 64))
     st = pb.static
     kpts = pb.kpts[rank * nk:(rank + 1) * nk]
-    fvb = FirstVariational(local_rank)
+    fvb = FirstVariational(local_rank, precision=prec)
     fvb.set_static(st)
     stream = torch.cuda.Stream(device=dev)
     fvb.set_stream(stream.cuda_stream)
@@ -224,13 +230,16 @@ def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn):
     tot = float(t.item())
     lanes = fvb.lanes()
     fvb.close()
+    evals = np.array([e.cpu().numpy() for e in ev])
     nm = [k.nmat for k in kpts]
+    form = "mixed (complex64 tridiagonal reduction + FP64 Rayleigh-Ritz)" if prec == EXCFV_PREC_MIXED \
+        else "plain FP64"
     return {"workload": f"{nk} k-points per GPU of the 8-atom cell, nmat {min(nm)}..{max(nm)} "
-                        f"(uniform, seeded), lowest {st.nstfv} states, plain FP64",
+                        f"(uniform, seeded), lowest {st.nstfv} states, {form}",
             "value": world * nk * args.batch_steps / (tot / 1e3), "unit": "k-points/s",
             "ms_per_batch": tot / args.batch_steps, "lanes": lanes,
             "lane_stage_ms_per_k": {kk: round(v[0] / (args.batch_steps * nk), 3) for kk, v in bprof.items()},
-            "all_info_zero": bool(np.all(info == 0))}
+            "all_info_zero": bool(np.all(info == 0))}, evals
 
 
 def main():
@@ -283,6 +292,7 @@ def main():
     from datetime import timedelta
 
     from exciting_b200.fv import FirstVariational
+    from exciting_b200.lib import EXCFV_PREC_FP64, EXCFV_PREC_MIXED
 
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
@@ -431,18 +441,61 @@ def main():
                 "peak_source": "cuBLAS ZGEMM 4096^3 measured in this run (FP64 tensor path)"}
     stages = {kk: round(v[0] / args.steps, 4) for kk, v in prof.items()}
 
+    # ---- precision form, same k-point: device-resident timing ----------------
+    fvm = FirstVariational(local_rank, precision=EXCFV_PREC_MIXED)
+    fvm.set_static(st)
+    fvm.reserve(nmatmax, p.ngkmax)
+    fvm.set_stream(stream.cuda_stream)
+    dm_eval = torch.zeros(k, dtype=torch.float64, device=dev)
+    dm_evec = torch.zeros(k * nmatmax, dtype=torch.complex128, device=dev)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.zero_()
+            fvm.seceqn_dev(n, kp.ngp, kp.ngkmax, ptrs, nmatmax, dm_eval.data_ptr(), dm_evec.data_ptr())
+        fvm.sync(n)
+        torch.cuda.synchronize()
+        mevs = []
+        for _ in range(args.steps):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            fvm.seceqn_dev(n, kp.ngp, kp.ngkmax, ptrs, nmatmax, dm_eval.data_ptr(), dm_evec.data_ptr())
+            e.record(stream)
+            mevs.append((s, e))
+        fvm.sync(n)
+        torch.cuda.synchronize()
+    m_ms = sum(s.elapsed_time(e) for s, e in mevs)
+    tm = torch.tensor([m_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+    m_ms = float(tm.item())
+    wm_host = dm_eval.cpu().numpy()
+    fvm.close()
+    mixed_single = {"value": world * args.steps / (m_ms / 1e3), "unit": UNIT,
+                    "ms_per_step": m_ms / args.steps,
+                    "eig_err_vs_fp64_gpu": float(np.abs(wm_host - ev_host).max())}
+
     # ---- batching form: 64 k-points of the 8-atom cell, nmat 1800..2300 ------
     batched = None
     if not args.no_batched:
-        batched = run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn)
+        b64, w64 = run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn, EXCFV_PREC_FP64)
+        bmx, wmx = run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn, EXCFV_PREC_MIXED)
+        bmx["eig_err_vs_fp64_gpu"] = float(np.abs(wmx - w64).max())
+        batched = {"fp64": b64, "mixed": bmx,
+                   "mixed_batched_over_fp64_single": bmx["value"] / value,
+                   "mixed_batched_over_fp64_batched": bmx["value"] / b64["value"]}
 
-    # ---- CPU baseline (rank 0, N = 1) ----------------------------------------
+    # ---- CPU baseline (rank 0, N = 1); its first k-point is the timed one ----
     cpu = None
+    oracle_err = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         pc = syn.make_problem(args.workload, nk=1)
-        times = time_cpu_reference(pc, 2, 1, min_seconds=10.0)
+        times, w_or = time_cpu_reference(pc, 2, 1, min_seconds=10.0, keep_first=True)
         cpu = {"value": len(times) / sum(times), "unit": UNIT, "cores": cores_used(), "kind": "port",
                "sample": f"{len(times)} k-points of {args.workload} (NumPy + OpenBLAS ZHEGVX lwork=2n)"}
+        oracle_err = {"fp64": float(np.abs(ev_host - w_or).max()),
+                      "mixed": float(np.abs(wm_host - w_or).max()),
+                      "note": "max |eigenvalue - oracle ZHEGVX| over the lowest nstfv states, Ha"}
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -450,6 +503,7 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator of the named shape)",
         "config": {"workload": workload_desc(args.workload, p), "form": "plain FP64",
+                   "mixed_single_k": mixed_single, "eig_err_vs_oracle": oracle_err,
                    "l2": "flushed between steps (512 MB write, outside the timed events)",
                    "parallelism": f"k-points over {world} GPU(s), no data-path collective",
                    "stage_ms_per_step": stages, "fp64_tensor_peak_tflops": zpeak,
