@@ -128,6 +128,28 @@ __device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, int* s
     }
   }
 }
+// Bounded wait that reports whether the phase completed.
+__device__ __forceinline__ bool mbar_wait_ok(uint64_t* bar, unsigned parity, int* status) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = gtimer();
+  unsigned it = 0;
+  while (!mbar_try_wait(bar, parity)) {
+    if ((++it & 63u) == 0) {
+      if (*(volatile int*)&status[ST_BARRIER] != 0) return false;
+      if (gtimer() - t0 > BARRIER_NS) {
+        atomicAdd(&status[ST_BARRIER], 1);
+        return false;
+      }
+    }
+  }
+  return true;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// Barrier of the TT consumer threads (named barrier 1; the producer warp does not take part).
+__device__ __forceinline__ void csync() { asm volatile("bar.sync 1, %0;" ::"n"(TT) : "memory"); }
+
 // 2-D tiled TMA load (no multicast) of one 64 x BC tile; x counts scalars
 // (re and im separately) along the rows, y counts columns.
 __device__ __forceinline__ void tma_tile(void* dst, const CUtensorMap* tm, int x, int y,
@@ -144,7 +166,7 @@ __device__ __forceinline__ void tma_tile(void* dst, const CUtensorMap* tm, int x
 // Returns false when it timed out (here or in another CTA).
 __device__ bool grid_barrier(unsigned* bar, unsigned& epoch, int* status) {
   __shared__ int s_ok;
-  __syncthreads();
+  csync();
   if (threadIdx.x == 0) {
     int ok = 1;
     epoch += 1;
@@ -166,7 +188,7 @@ __device__ bool grid_barrier(unsigned* bar, unsigned& epoch, int* status) {
     }
     s_ok = ok;
   }
-  __syncthreads();
+  csync();
   return s_ok != 0;
 }
 
@@ -210,8 +232,22 @@ __device__ __forceinline__ cplx warp_sum(cplx v) {
 
 constexpr int JB = 8;  // column tiles whose x values are staged per round trip
 
+// Lower 64 x 64 tiles of the trailing block in row-major order; the run that
+// starts at flat index t within its row tile: row I, columns [Jb, Je), ending
+// at t_end at the latest.  Returns the flat index after the run.
+__device__ __forceinline__ long long tile_run(long long t, long long t_end, int& I, int& Jb, int& Je) {
+  int q = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+  while ((long long)(q + 1) * (q + 2) / 2 <= t) ++q;
+  while ((long long)q * (q + 1) / 2 > t) --q;
+  I = q;
+  Jb = (int)(t - (long long)q * (q + 1) / 2);
+  const long long e = min((long long)q * (q + 1) / 2 + q + 1, t_end);
+  Je = Jb + (int)(e - t);
+  return e;
+}
+
 template <typename T2>
-__global__ void __launch_bounds__(TT, 1)
+__global__ void __launch_bounds__(TT + 32, 1)
     k_tridiag_panel(TridArgs<T2> a, const __grid_constant__ CUtensorMap tmap) {
   using R = Ring<T2>;
   extern __shared__ __align__(128) unsigned char dsm[];
@@ -222,13 +258,15 @@ __global__ void __launch_bounds__(TT, 1)
     const unsigned r0 = (b0 + (unsigned)sizeof(PanelSmem<T2>) + 127u) & ~127u;
     ring = reinterpret_cast<T2*>(dsm + (r0 - b0));
   }
-  __shared__ __align__(8) uint64_t s_full[MAX_STAGES];
+  __shared__ __align__(8) uint64_t s_full[MAX_STAGES];   // tile landed (TMA bytes)
+  __shared__ __align__(8) uint64_t s_empty[MAX_STAGES];  // tile consumed by the 8 consumer warps
   __shared__ cplx s_vc[NBT], s_wc[NBT];   // row c+1 of V and W
   __shared__ cplx s_sv[NBT], s_tv[NBT];   // V^H v, W^H v of the current column
-  __shared__ cplx s_acc_s[NBT], s_acc_t[NBT];
   __shared__ T2 s_x[JB * 64];             // staged x values of the trailing column
-  __shared__ cplx s_xr[64];               // x values of the item's rows
-  __shared__ cplx s_part[TT];
+  __shared__ cplx s_xr[64];               // x values of the run's rows
+  __shared__ cplx s_c1[64];               // C(r, c+1) of the run's rows
+  __shared__ cplx s_red[TT / 32][64];     // row sums of the 8 warps
+  __shared__ cplx s_part[TT / 32];        // v^H y partials of the 8 warps
   __shared__ double s_dred[TT / 32];
   __shared__ double s_scal[8];            // tau.re, tau.im, scale.re, scale.im, alpha, beta, vav, y(c+1)
   __shared__ cplx s_y1;
@@ -247,10 +285,47 @@ __global__ void __launch_bounds__(TT, 1)
   unsigned epoch = 0;
   unsigned gtile = 0;  // tiles consumed by this CTA (ring slot and mbarrier phase)
   if (tid == 0) {
-    for (int q = 0; q < R::STAGES; ++q) mbar_init(&s_full[q], 1);
+    for (int q = 0; q < R::STAGES; ++q) {
+      mbar_init(&s_full[q], 1);
+      mbar_init(&s_empty[q], TT / 32);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+
+  // ---- producer warp: TMA tiles of every column of the panel, in the order
+  // the consumers read them, as far ahead as the ring allows.  The lower tiles
+  // read for column c' (rows and columns >= c'+1, or c' for complex64) are not
+  // written during the panel (only column c' itself, with zero weight), so the
+  // tiles of the next column may land while the current one is finished.
+  if (tid >= TT) {
+    if (lane == 0) {
+      unsigned q = 0;
+      for (int i = 0; i < a.nbp; ++i) {
+        const int r0g = a.p + i + 1;
+        const int rb = (sizeof(T2) == 8) ? (r0g & ~1) : r0g;
+        const int nt = (n - rb + 63) / 64;
+        const long long ntri = (long long)nt * (nt + 1) / 2;
+        const long long t_beg = ntri * bid / G, t_end = ntri * (bid + 1) / G;
+        for (long long t = t_beg; t < t_end;) {
+          int I, Jb, Je;
+          t = tile_run(t, t_end, I, Jb, Je);
+          const int colb = rb + Jb * 64;
+          const int ntile = (min(n, rb + Je * 64) - colb + R::BC - 1) / R::BC;
+          for (int b = 0; b < ntile; ++b, ++q) {
+            const unsigned slot = q % R::STAGES;
+            if (q >= (unsigned)R::STAGES &&
+                !mbar_wait_ok(&s_empty[slot], ((q / R::STAGES) - 1u) & 1u, a.status))
+              return;
+            mbar_expect_tx(&s_full[slot], R::BYTES);
+            tma_tile(ring + (size_t)slot * R::TILE, &tmap, 2 * (rb + I * 64), colb + b * R::BC,
+                     &s_full[slot]);
+          }
+        }
+      }
+    }
+    return;
+  }
 
   // ---- prologue: column p needs no update; its norm and diagonal
   {
@@ -274,7 +349,7 @@ __global__ void __launch_bounds__(TT, 1)
     }
     for (int o = 16; o > 0; o >>= 1) nrm_part += __shfl_xor_sync(0xffffffffu, nrm_part, o);
     if (lane == 0) s_dred[warp] = nrm_part;
-    __syncthreads();
+    csync();
     if (tid == 0) {
       double sacc = 0.0;
       for (int w = 0; w < TT / 32; ++w) sacc += s_dred[w];
@@ -291,33 +366,22 @@ __global__ void __launch_bounds__(TT, 1)
     // ================= phase 2: reflector of column c, y = C22 v =================
     // y = C22 v with v(c+1) = 1, v(j) = scale x(j): accumulate C22 x~ (x~(c+1) = 0)
     // and the column c+1 separately, so that the tile loads do not wait for the
-    // reflector.  The tile grid starts at row and column rb (even for complex64:
-    // the TMA row coordinate needs 16-byte alignment); rows and columns below
-    // c+1 carry zero weight.  Every CTA computes the reflector scalars.
+    // reflector.  Only the lower triangle of C22 is read: a 64 x 64 tile (I, J),
+    // I >= J, adds A_IJ x~_J to y_I (row part) and A_IJ^H x~_I to y_J (column
+    // part); diagonal tiles use r >= j for the row part and r > j for the
+    // column part.  The tile grid starts at row and column rb (even for
+    // complex64, as the TMA row coordinate needs 16-byte alignment); rows and
+    // columns below c+1 carry zero weight.  CTA b takes the lower tiles
+    // [b T / G, (b+1) T / G) in row-major order, as runs within one row tile.
     const int r0g = c + 1;
     const int rb = (sizeof(T2) == 8) ? (r0g & ~1) : r0g;
     const int nt = (n - rb + 63) / 64;
-    int Sg = G / nt;
-    if (Sg < 1) Sg = 1;
-    if (Sg > nt) Sg = nt;
-    const int per = (nt + Sg - 1) / Sg;
-    const int items = nt * Sg;
-    const int rr = tid & 63, cg = tid >> 6;
+    const long long ntri = (long long)nt * (nt + 1) / 2;
+    const long long t_beg = ntri * bid / G, t_end = ntri * (bid + 1) / G;
+    constexpr int BPT = 64 / R::BC;    // TMA tiles (boxes) per 64-column tile
+    constexpr int NPASS = R::BC / 16;  // 16-column passes per box
+    const int rg = tid & 15, cq = tid >> 4;
     double vav_re = 0.0, vav_im = 0.0;
-    if (tid < NBT) { s_acc_s[tid] = cmk(0.0, 0.0); s_acc_t[tid] = cmk(0.0, 0.0); }
-    // issue the leading tiles of item `it` (thread 0)
-    auto issue_lead = [&](int it, unsigned g0) {
-      const int I = it / Sg, Jb = (it % Sg) * per, Je = min(nt, Jb + per);
-      if (Jb >= Je) return;
-      const int colb = rb + Jb * 64;
-      const int ntile = (min(n, rb + Je * 64) - colb + R::BC - 1) / R::BC;
-      for (int b = 0; b < min(R::STAGES, ntile); ++b) {
-        const unsigned q = (g0 + b) % R::STAGES;
-        mbar_expect_tx(&s_full[q], R::BYTES);
-        tma_tile(ring + (size_t)q * R::TILE, &tmap, 2 * (rb + I * 64), colb + b * R::BC, &s_full[q]);
-      }
-    };
-    if (tid == 0 && bid < items) issue_lead(bid, gtile);
     if (tid == 0) {
       const cplx alpha = ldT(C + (c + 1) + ld * c);
       const double xn2 = ldd(red_norm + i);
@@ -336,93 +400,137 @@ __global__ void __launch_bounds__(TT, 1)
       }
       s_scal[0] = tr; s_scal[1] = ti; s_scal[2] = scr; s_scal[3] = sci; s_scal[5] = beta;
     }
-    for (int it = bid; it < items; it += G) {
-      const int I = it / Sg, Jb = (it % Sg) * per, Je = min(nt, Jb + per);
-      if (Jb >= Je) continue;
+    for (long long t = t_beg; t < t_end;) {
+      int I, Jb, Je;
+      t = tile_run(t, t_end, I, Jb, Je);
       const int row0 = rb + I * 64;
       const int colb = rb + Jb * 64;
       const int ntile = (min(n, rb + Je * 64) - colb + R::BC - 1) / R::BC;
-      if (tid == 0 && it != bid) issue_lead(it, gtile);
-      const int r = row0 + rr;
-      cplx acc = cmk(0.0, 0.0), acc1 = cmk(0.0, 0.0);
+      csync();  // the previous run's row sums are consumed
+      if (tid < 64) {
+        const int r2 = row0 + tid;
+        s_xr[tid] = (r2 < n && r2 > c + 1) ? ldT(C + r2 + ld * c) : cmk(0.0, 0.0);
+      } else if (tid < 128) {
+        const int r2 = row0 + tid - 64;
+        s_c1[tid - 64] = (Jb == 0 && r2 < n && r2 >= c + 1) ? ldT(C + r2 + ld * (c + 1)) : cmk(0.0, 0.0);
+      }
+      cplx rowp[4], xr[4];
+      T2 xrT[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) rowp[u] = cmk(0.0, 0.0);
+      cplx scale = cmk(0.0, 0.0);
       int b = 0;
       for (int g0 = Jb; g0 < Je; g0 += JB) {
         const int g1 = min(Je, g0 + JB);
-        __syncthreads();  // the previous group's x values are consumed
+        T2 rowf[4];  // complex64: row sums of this group in FP32 (at most 32 terms)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) rowf[u] = fromD<T2>(cmk(0.0, 0.0));
+        if (g0 != Jb) csync();  // the previous group's x values are consumed
         {
           const int j_a = rb + g0 * 64 + tid, j_b = j_a + TT;
           const int lim = min(n, rb + g1 * 64);
           s_x[tid] = fromD<T2>((j_a < lim && j_a > c + 1) ? ldT(C + j_a + ld * c) : cmk(0.0, 0.0));
           s_x[tid + TT] = fromD<T2>((j_b < lim && j_b > c + 1) ? ldT(C + j_b + ld * c) : cmk(0.0, 0.0));
-          if (g0 == Jb && tid < 64) {
-            const int r2 = row0 + tid;
-            s_xr[tid] = (r2 < n && r2 > c + 1) ? ldT(C + r2 + ld * c) : cmk(0.0, 0.0);
-          }
         }
-        __syncthreads();
-        const int bend = min(ntile, (g1 - Jb) * (64 / R::BC));
+        csync();
+        if (g0 == Jb) {
+          scale = cmk(s_scal[2], s_scal[3]);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) { xr[u] = s_xr[rg + 16 * u]; xrT[u] = fromD<T2>(xr[u]); }
+        }
+        const int bend = min(ntile, (g1 - Jb) * BPT);
         for (; b < bend; ++b) {
           const unsigned q = gtile + b;
           const unsigned slot = q % R::STAGES;
           mbar_wait(&s_full[slot], (q / R::STAGES) & 1u, a.status);
           const T2* tile = ring + (size_t)slot * R::TILE;
-          constexpr int CPT = R::BC / 4;         // columns per thread
-          const int cl = cg * CPT;                // first column of this thread in the tile
-          const int xo = b * R::BC - (g0 - Jb) * 64 + cl;
-          const int j0 = colb + b * R::BC + cl;
-          if constexpr (sizeof(T2) == 16) {
+          const int jt = Jb + b / BPT;                 // column tile of this box
+          const bool diag = (jt == I);
 #pragma unroll
-            for (int u = 0; u < CPT; ++u) {
-              const cplx av = toD(tile[(cl + u) * RCH + rr]);
-              const cplx xv = toD(s_x[xo + u]);
-              acc.x += av.x * xv.x - av.y * xv.y;
-              acc.y += av.x * xv.y + av.y * xv.x;
-              if (j0 + u == c + 1) acc1 = av;
-            }
-          } else {
-            float pr = 0.f, pi = 0.f;
+          for (int ps = 0; ps < NPASS; ++ps) {
+            const int cb = ps * 16 + cq;                // column within the box
+            const int jl = (b % BPT) * R::BC + cb;      // column within the 64-wide tile
+            const T2 xj = s_x[(jt - g0) * 64 + jl];
+            T2 cp = fromD<T2>(cmk(0.0, 0.0));
 #pragma unroll
-            for (int u = 0; u < CPT; ++u) {
-              const T2 av = tile[(cl + u) * RCH + rr];
-              const T2 xv = s_x[xo + u];
-              pr = fmaf(av.x, xv.x, fmaf(-av.y, xv.y, pr));
-              pi = fmaf(av.x, xv.y, fmaf(av.y, xv.x, pi));
-              if (j0 + u == c + 1) acc1 = toD(av);
+            for (int u = 0; u < 4; ++u) {
+              const int rl = rg + 16 * u;
+              const T2 av = tile[cb * RCH + rl];
+              if (!diag || rl >= jl) {  // row part: A(r, j) x~(j)
+                if constexpr (sizeof(T2) == 16) {
+                  rowp[u].x += av.x * xj.x - av.y * xj.y;
+                  rowp[u].y += av.x * xj.y + av.y * xj.x;
+                } else {
+                  rowf[u].x = fmaf(av.x, xj.x, fmaf(-av.y, xj.y, rowf[u].x));
+                  rowf[u].y = fmaf(av.x, xj.y, fmaf(av.y, xj.x, rowf[u].y));
+                }
+              }
+              if (!diag || rl > jl) {   // column part: conj(A(r, j)) x~(r)
+                cp.x += av.x * xrT[u].x + av.y * xrT[u].y;
+                cp.y += av.x * xrT[u].y - av.y * xrT[u].x;
+              }
             }
-            acc.x += (double)pr;
-            acc.y += (double)pi;
+#pragma unroll
+            for (int o = 1; o < 16; o <<= 1) {
+              cp.x += __shfl_xor_sync(0xffffffffu, cp.x, o);
+              cp.y += __shfl_xor_sync(0xffffffffu, cp.y, o);
+            }
+            const int j = rb + jt * 64 + jl;
+            if (rg == 0 && j >= r0g && j < n) {
+              const cplx sc = cmul(scale, toD(cp));
+              atomicAdd(&ycur[j].x, sc.x);
+              atomicAdd(&ycur[j].y, sc.y);
+              const cplx vj = (j == c + 1) ? cmk(1.0, 0.0) : cmul(toD(xj), scale);
+              vav_re += vj.x * sc.x + vj.y * sc.y;  // conj(v_j) * contribution
+              vav_im += vj.x * sc.y - vj.y * sc.x;
+            }
           }
           // The slot is refilled by the async proxy (TMA): order this thread's
-          // generic reads of it before that write, then release it to thread 0.
+          // generic reads of it before that write, then release it (one
+          // arrival per consumer warp).
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          __syncthreads();
-          if (tid == 0 && b + R::STAGES < ntile) {
-            mbar_expect_tx(&s_full[slot], R::BYTES);
-            tma_tile(ring + (size_t)slot * R::TILE, &tmap, 2 * row0,
-                     colb + (b + R::STAGES) * R::BC, &s_full[slot]);
-          }
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&s_empty[slot]);
+        }
+        if constexpr (sizeof(T2) == 8) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) rowp[u] = cadd(rowp[u], toD(rowf[u]));
         }
       }
       gtile += ntile;
-      const cplx scale = cmk(s_scal[2], s_scal[3]);
-      s_part[tid] = cadd(cmul(scale, acc), acc1);
-      __syncthreads();
-      if (tid < 64 && r < n && r >= r0g) {
-        cplx sum = cadd(cadd(s_part[tid], s_part[tid + 64]), cadd(s_part[tid + 128], s_part[tid + 192]));
-        atomicAdd(&ycur[r].x, sum.x);
-        atomicAdd(&ycur[r].y, sum.y);
-        const cplx vr = (r == c + 1) ? cmk(1.0, 0.0) : cmul(s_xr[tid], scale);
-        vav_re += vr.x * sum.x + vr.y * sum.y;  // conj(v_r) * sum
-        vav_im += vr.x * sum.y - vr.y * sum.x;
+      // row sums: the two column threads of a warp, then the 8 warps
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        rowp[u].x += __shfl_xor_sync(0xffffffffu, rowp[u].x, 16);
+        rowp[u].y += __shfl_xor_sync(0xffffffffu, rowp[u].y, 16);
+      }
+      if (lane < 16) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s_red[warp][rg + 16 * u] = rowp[u];
+      }
+      csync();
+      if (tid < 64) {
+        const int r = row0 + tid;
+        if (r >= r0g && r < n) {
+          cplx sum = s_red[0][tid];
+#pragma unroll
+          for (int w = 1; w < TT / 32; ++w) sum = cadd(sum, s_red[w][tid]);
+          sum = cadd(cmul(scale, sum), s_c1[tid]);
+          atomicAdd(&ycur[r].x, sum.x);
+          atomicAdd(&ycur[r].y, sum.y);
+          const cplx vr = (r == c + 1) ? cmk(1.0, 0.0) : cmul(s_xr[tid], scale);
+          vav_re += vr.x * sum.x + vr.y * sum.y;  // conj(v_r) * sum
+          vav_im += vr.x * sum.y - vr.y * sum.x;
+        }
       }
     }
-    __syncthreads();  // the scalars of thread 0 are visible
+    csync();  // the scalars of thread 0 are visible
     const cplx scale = cmk(s_scal[2], s_scal[3]);
     for (int o = 16; o > 0; o >>= 1) {
       vav_re += __shfl_xor_sync(0xffffffffu, vav_re, o);
       vav_im += __shfl_xor_sync(0xffffffffu, vav_im, o);
     }
-    __syncthreads();
+    csync();
     if (lane == 0) { s_part[warp].x = vav_re; s_part[warp].y = vav_im; }
     // own rows: clear y of the next column, V^H v and W^H v partials
     {
@@ -448,36 +556,44 @@ __global__ void __launch_bounds__(TT, 1)
           }
         }
       }
-      if (i > 0) {
+      // Reduce over the 8 rows of the warp (lane bits 2..4) and scatter: after
+      // three halving exchanges lane l holds the warp's sum for
+      // j = rsub + 4 u(l), u(l) = 4 b4 + 2 b3 + b2 of its lane bits.
+      const bool h1 = (lane >> 4) & 1, h2 = (lane >> 3) & 1, h3 = (lane >> 2) & 1;
 #pragma unroll
-        for (int u = 0; u < NBT / 4; ++u) {
-          for (int o = 4; o < 32; o <<= 1) {
-            ps[u].x += __shfl_xor_sync(0xffffffffu, ps[u].x, o);
-            ps[u].y += __shfl_xor_sync(0xffffffffu, ps[u].y, o);
-            pt[u].x += __shfl_xor_sync(0xffffffffu, pt[u].x, o);
-            pt[u].y += __shfl_xor_sync(0xffffffffu, pt[u].y, o);
-          }
-        }
-        if (lane < 4) {
-#pragma unroll
-          for (int u = 0; u < NBT / 4; ++u) {
-            const int j = lane + 4 * u;
-            if (j < i) {
-              atomicAdd(&s_acc_s[j].x, ps[u].x);
-              atomicAdd(&s_acc_s[j].y, ps[u].y);
-              atomicAdd(&s_acc_t[j].x, pt[u].x);
-              atomicAdd(&s_acc_t[j].y, pt[u].y);
-            }
-          }
-        }
+      for (int k = 0; k < 4; ++k) {
+        const cplx sa = h1 ? ps[k] : ps[k + 4], ka = h1 ? ps[k + 4] : ps[k];
+        const cplx ta = h1 ? pt[k] : pt[k + 4], kb = h1 ? pt[k + 4] : pt[k];
+        ps[k] = cmk(ka.x + __shfl_xor_sync(0xffffffffu, sa.x, 16), ka.y + __shfl_xor_sync(0xffffffffu, sa.y, 16));
+        pt[k] = cmk(kb.x + __shfl_xor_sync(0xffffffffu, ta.x, 16), kb.y + __shfl_xor_sync(0xffffffffu, ta.y, 16));
       }
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const cplx sa = h2 ? ps[k] : ps[k + 2], ka = h2 ? ps[k + 2] : ps[k];
+        const cplx ta = h2 ? pt[k] : pt[k + 2], kb = h2 ? pt[k + 2] : pt[k];
+        ps[k] = cmk(ka.x + __shfl_xor_sync(0xffffffffu, sa.x, 8), ka.y + __shfl_xor_sync(0xffffffffu, sa.y, 8));
+        pt[k] = cmk(kb.x + __shfl_xor_sync(0xffffffffu, ta.x, 8), kb.y + __shfl_xor_sync(0xffffffffu, ta.y, 8));
+      }
+      {
+        const cplx sa = h3 ? ps[0] : ps[1], ka = h3 ? ps[1] : ps[0];
+        const cplx ta = h3 ? pt[0] : pt[1], kb = h3 ? pt[1] : pt[0];
+        ps[0] = cmk(ka.x + __shfl_xor_sync(0xffffffffu, sa.x, 4), ka.y + __shfl_xor_sync(0xffffffffu, sa.y, 4));
+        pt[0] = cmk(kb.x + __shfl_xor_sync(0xffffffffu, ta.x, 4), kb.y + __shfl_xor_sync(0xffffffffu, ta.y, 4));
+      }
+      csync();  // the last run's row sums in s_red are consumed
+      const int jl = rsub + 4 * (4 * (int)h1 + 2 * (int)h2 + (int)h3);
+      s_red[warp][jl] = ps[0];
+      s_red[warp][NBT + jl] = pt[0];
     }
-    __syncthreads();
-    if (tid < i) {
-      atomicAdd(&red_s[2 * (NBT * i + tid)], s_acc_s[tid].x);
-      atomicAdd(&red_s[2 * (NBT * i + tid) + 1], s_acc_s[tid].y);
-      atomicAdd(&red_t[2 * (NBT * i + tid)], s_acc_t[tid].x);
-      atomicAdd(&red_t[2 * (NBT * i + tid) + 1], s_acc_t[tid].y);
+    csync();
+    if (tid < 2 * NBT && (tid & (NBT - 1)) < i) {
+      cplx sum = s_red[0][tid];
+#pragma unroll
+      for (int w = 1; w < TT / 32; ++w) sum = cadd(sum, s_red[w][tid]);
+      double* dst = (tid < NBT) ? red_s : red_t;
+      const int j = tid & (NBT - 1);
+      atomicAdd(&dst[2 * (NBT * i + j)], sum.x);
+      atomicAdd(&dst[2 * (NBT * i + j) + 1], sum.y);
     }
     if (tid == 32) {
       double sr = 0.0, si = 0.0;
@@ -516,7 +632,7 @@ __global__ void __launch_bounds__(TT, 1)
         if (upd && rsub == 0) cn[ch] = ldT(C + r + ld * c1);
       }
     }
-    __syncthreads();
+    csync();
     const cplx tau = cmk(s_scal[0], s_scal[1]);
     if (warp == 0) {
       // alpha = -1/2 |tau|^2 (v^H C v - 2 Re(t^H s))
@@ -538,7 +654,7 @@ __global__ void __launch_bounds__(TT, 1)
         }
       }
     }
-    __syncthreads();
+    csync();
     const double alpha = s_scal[4];
     double nrm_part = 0.0;
     for (int ch = 0; ch < MAXCH; ++ch) {
@@ -593,7 +709,7 @@ __global__ void __launch_bounds__(TT, 1)
     if (i + 1 < a.nbp) {
       for (int o = 16; o > 0; o >>= 1) nrm_part += __shfl_xor_sync(0xffffffffu, nrm_part, o);
       if (lane == 0) s_dred[warp] = nrm_part;
-      __syncthreads();
+      csync();
       if (tid == 0) {
         double sacc = 0.0;
         for (int w = 0; w < TT / 32; ++w) sacc += s_dred[w];
@@ -609,7 +725,7 @@ __global__ void k_tail_scalar(const T2* C, double* d) {
   if (threadIdx.x == 0 && blockIdx.x == 0) d[0] = toD(C[0]).x;
 }
 
-// C (m x m, complex64) -= A B^H with A, B m x 2NBT (leading dimension ld):
+// Lower 64 x 64 tiles of C (m x m, complex64) -= A B^H, A and B m x 2NBT (leading dimension ld):
 // the trailing update of the complex64 reduction, FP32 products.  64 x 64
 // tiles of C per CTA, 16 x 16 threads with 4 x 4 outputs each (rows on the
 // fast thread index for coalesced stores), K staged in two chunks of NBT.
@@ -620,6 +736,7 @@ __global__ void __launch_bounds__(256) k_her2k_f32(int m, const float2* __restri
   __shared__ float2 sB[NBT][64 + 1];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
+  if (c0 > r0) return;  // the reduction reads the lower triangle only
   float accr[4][4], acci[4][4];
 #pragma unroll
   for (int u = 0; u < 4; ++u)
@@ -669,7 +786,8 @@ __global__ void __launch_bounds__(256) k_her2k_f32(int m, const float2* __restri
 int her2k_update(excfv_handle* h, int m2, const double2* VW, const double2* WV, long long ld,
                  double2* C22) {
   const cplx mone = cmk(-1.0, 0.0), one = cmk(1.0, 0.0);
-  return zgemm1(h->stream, OP_N, OP_C, m2, m2, 2 * NBT, mone, VW, ld, WV, ld, one, C22, ld);
+  return zgemm1(h->stream, OP_N, OP_C, m2, m2, 2 * NBT, mone, VW, ld, WV, ld, one, C22, ld,
+                TRI_LOWER);
 }
 int her2k_update(excfv_handle* h, int m2, const float2* VW, const float2* WV, long long ld,
                  float2* C22) {
@@ -746,7 +864,7 @@ static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
   if (int rc = make_tile_map(&tmap, C, n, ld)) return rc;
   CUDA_TRY(cudaFuncSetAttribute(k_tridiag_panel<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int per_sm = 0;
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tridiag_panel<T2>, TT, smem));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tridiag_panel<T2>, TT + 32, smem));
   if (per_sm < 1) {
     excfv_set_error("tridiag panel kernel cannot be resident");
     return EXCFV_ERR_CUDA;
@@ -771,14 +889,14 @@ static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
     ta.p = p; ta.nbp = nbp; ta.final_panel = final_panel;
     void* args[] = {&ta, &tmap};
     prof_begin(h, PROF_TRD_PANEL);
-    CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_tridiag_panel<T2>, dim3(G), dim3(TT), args,
+    CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_tridiag_panel<T2>, dim3(G), dim3(TT + 32), args,
                                          (size_t)smem, s));
     count_launch();
     prof_end(h, PROF_TRD_PANEL);
     if (!final_panel) {
       prof_begin(h, PROF_TRD_UPDATE);
       const int q = p + nbp;
-      // C22 -= [V W] [W V]^H (both triangles; the next panel's y = C22 v reads both)
+      // C22 -= [V W] [W V]^H on the lower triangle (all the next panel reads)
       int rc = her2k_update(h, n - q, VW + q, WV + q, ld, C + q + ld * q);
       if (rc) return rc;
       prof_end(h, PROF_TRD_UPDATE);
