@@ -387,14 +387,6 @@ int excfv_create(int device, excfv_handle** out) {
   return EXCFV_OK;
 }
 
-// the nested Rayleigh-Ritz context of the precision form (shares the stream)
-static void destroy_sub(excfv_handle* h) {
-  if (!h->sub) return;
-  free_workspace(h->sub->ws);
-  delete h->sub;
-  h->sub = nullptr;
-}
-
 int excfv_destroy(excfv_handle* h) {
   if (!h) return EXCFV_OK;
   DeviceGuard g(h->device);
@@ -403,14 +395,12 @@ int excfv_destroy(excfv_handle* h) {
     for (cudaEvent_t e : h->prof.ev[c]) cudaEventDestroy(e);
   for (excfv_handle* c : h->lanes) {
     cudaStreamSynchronize(c->stream);
-    destroy_sub(c);
     free_workspace(c->ws);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
   }
   h->lanes.clear();
   if (h->kinfo) cudaFree(h->kinfo);
-  destroy_sub(h);
   free_workspace(h->ws);
   if (h->owns_static) free_static(h->st);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);

@@ -39,7 +39,7 @@ EXCFV_HD double cabs2(cplx a) { return a.x * a.x + a.y * a.y; }
 //   [1] grid barrier timeout count
 //   [2] stein: number of eigenvectors that failed to converge
 //   [3] stebz: bisection did not converge for some eigenvalue
-enum { ST_POTRF = 0, ST_BARRIER = 1, ST_STEIN = 2, ST_STEBZ = 3, ST_NWORDS = 8 };
+enum { ST_POTRF = 0, ST_BARRIER = 1, ST_STEIN = 2, ST_STEBZ = 3, ST_REFINE = 4, ST_NWORDS = 8 };
 
 #define CUDA_TRY(expr)                                                          \
   do {                                                                          \

@@ -111,7 +111,6 @@ struct excfv_handle {
   int kinfo_cap = 0;
   int last_nk = 0;
   std::vector<int> batch_nmat;  // nmatp of the last batch (info offsets)
-  excfv_handle* sub = nullptr;  // nested context of the precision form's Rayleigh-Ritz solve
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
   int prec = EXCFV_PREC_FP64;

@@ -21,7 +21,6 @@ int tridiag_eig(excfv_handle* h, int n, int k, double abstol, const double* d, c
                 double* w, cplx* Z, long long ldz, double* scratch, int* iscratch);
 int mirror_upper(cudaStream_t s, int n, cplx* M, long long ld);
 int tridiag_reduce_f32(excfv_handle* h, int n, float2* C, long long ld);
-int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax);
 
 namespace {
 
@@ -89,11 +88,241 @@ __global__ void k_lower_to_f64(int n, const float2* __restrict__ in, long long l
   out[r + ldo * c] = cmk((double)v.x, (double)v.y);
 }
 
-// status words of the nested Rayleigh-Ritz solve added into the caller's
-// (its Cholesky-QR word is not an overlap failure of the caller's problem)
-__global__ void k_or_status(const int* from, int* to) {
-  const int i = threadIdx.x;
-  if (i < ST_NWORDS && i != ST_POTRF && from[i]) to[i] += from[i];
+// ---------------------------------------------------------------------------
+// Precision form: refinement of the k' x k' Rayleigh-Ritz matrix Hk = X0^H C X0.
+// X0 comes from the complex64 reduction, so Hk = diag + E with |E| at the
+// FP32 level.  States whose Rayleigh quotients lie within tau = max|E| / RR_RHO
+// of each other form clusters (contiguous in sorted order), each diagonalised
+// exactly by complex Jacobi rotations; between clusters every coupling is at
+// most RR_RHO times the gap, and second-order perturbation theory gives the
+// eigenvalues (error ~ |E| RR_RHO^2) and first-order the vectors, which a
+// Cholesky-QR pass re-orthonormalises afterwards.
+// ---------------------------------------------------------------------------
+constexpr double RR_RHO = 1e-3;
+constexpr int RR_MAXC = 64;  // largest cluster diagonalised by the Jacobi kernel
+
+struct RRScratch {
+  double* D;      // kx: Rayleigh quotients
+  double* lam;    // kx: refined eigenvalues
+  int* perm;      // kx: sorted position -> state
+  int* cid;       // kx: cluster of each state
+  int* cstart;    // kx: first sorted position of each cluster
+  int* csize;     // kx
+  int* sel;       // k : state of the r-th lowest refined eigenvalue
+  int* nclust;    // 1
+};
+
+__device__ __forceinline__ double cabsd(cplx a) { return hypot(a.x, a.y); }
+
+__device__ __forceinline__ double block_max(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (l < (int)(blockDim.x >> 5)) ? red[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (l == 0) red[0] = v;
+  }
+  __syncthreads();
+  return red[0];
+}
+
+// One CTA of 1024 threads: Rayleigh quotients, max coupling, sort, clusters.
+__global__ void __launch_bounds__(1024) k_rr_clusters(int kx, const cplx* __restrict__ Hk, RRScratch s) {
+  __shared__ double red[32];
+  __shared__ int wsum[32];
+  const int tid = threadIdx.x;
+  double emax = 0.0, dmax = 0.0;
+  for (int i = tid; i < kx; i += blockDim.x) {
+    const double d = Hk[i + (long long)kx * i].x;
+    s.D[i] = d;
+    dmax = fmax(dmax, fabs(d));
+  }
+  for (long long e = tid; e < (long long)kx * kx; e += blockDim.x) {
+    const int i = (int)(e % kx), j = (int)(e / kx);
+    if (i != j) emax = fmax(emax, cabsd(Hk[e]));
+  }
+  emax = block_max(emax, red);
+  dmax = block_max(dmax, red);
+  const double tau = fmax(emax / RR_RHO, 64.0 * 2.220446049250313e-16 * dmax);
+  // rank of each state in ascending order (ties by index)
+  for (int i = tid; i < kx; i += blockDim.x) {
+    const double di = s.D[i];
+    int r = 0;
+    for (int j = 0; j < kx; ++j) {
+      const double dj = s.D[j];
+      r += (dj < di) || (dj == di && j < i);
+    }
+    s.perm[r] = i;
+  }
+  __syncthreads();
+  // cluster ids: inclusive scan of the start flags over sorted positions
+  const int per = (kx + blockDim.x - 1) / blockDim.x;
+  const int r0 = tid * per;
+  int cnt = 0;
+  for (int r = r0; r < min(kx, r0 + per); ++r)
+    cnt += (r == 0) || (s.D[s.perm[r]] - s.D[s.perm[r - 1]] > tau);
+  int incl = cnt;
+  const int lane = tid & 31, w = tid >> 5;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) wsum[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    int v = (lane < (int)(blockDim.x >> 5)) ? wsum[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += u;
+    }
+    wsum[lane] = v;
+  }
+  __syncthreads();
+  int c = (w > 0 ? wsum[w - 1] : 0) + incl - cnt - 1;  // cluster before this thread's range
+  for (int r = r0; r < min(kx, r0 + per); ++r) {
+    if ((r == 0) || (s.D[s.perm[r]] - s.D[s.perm[r - 1]] > tau)) {
+      ++c;
+      s.cstart[c] = r;
+    }
+    s.cid[s.perm[r]] = c;
+  }
+  if (tid == blockDim.x - 1) *s.nclust = wsum[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  for (int r = tid; r < kx; r += blockDim.x) {
+    const int cc = s.cid[s.perm[r]];
+    if (r == s.cstart[cc]) {
+      int e = r + 1;
+      while (e < kx && s.cid[s.perm[e]] == cc) ++e;
+      s.csize[cc] = e - r;
+    }
+  }
+}
+
+// Cyclic Jacobi on the Hermitian m x m matrix A (column-major, ld m); V gets
+// the eigenvectors.  Rotation on (p, q): with A(p,q) = g e^{i phi} and
+// t = tan(theta) from tau = (A(q,q) - A(p,p)) / 2g, U = [[c, s], [-s e^{-i phi},
+// c e^{-i phi}]]; A <- U^H A U, V <- V U.
+__device__ void jacobi_herm(int m, cplx* A, cplx* V) {
+  for (int i = 0; i < m * m; ++i) V[i] = cmk(0.0, 0.0);
+  for (int i = 0; i < m; ++i) V[i + m * i] = cmk(1.0, 0.0);
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    double off = 0.0, sc = 0.0;
+    for (int q = 0; q < m; ++q) {
+      sc = fmax(sc, fabs(A[q + m * q].x));
+      for (int p = 0; p < q; ++p) off = fmax(off, cabsd(A[p + m * q]));
+    }
+    if (off <= 1e-15 * sc || off == 0.0) break;
+    for (int p = 0; p < m; ++p)
+      for (int q = p + 1; q < m; ++q) {
+        const cplx apq = A[p + m * q];
+        const double g = cabsd(apq);
+        if (g <= 1e-300) continue;
+        const cplx ph = cmk(apq.x / g, apq.y / g);
+        const double tu = (A[q + m * q].x - A[p + m * p].x) / (2.0 * g);
+        const double t = (tu >= 0.0 ? 1.0 : -1.0) / (fabs(tu) + sqrt(1.0 + tu * tu));
+        const double cs = 1.0 / sqrt(1.0 + t * t), sn = t * cs;
+        const cplx phc = cmk(ph.x, -ph.y);
+        const cplx up0 = cmk(cs, 0.0), up1 = cscale(phc, -sn);
+        const cplx uq0 = cmk(sn, 0.0), uq1 = cscale(phc, cs);
+        for (int k = 0; k < m; ++k) {
+          const cplx akp = A[k + m * p], akq = A[k + m * q];
+          A[k + m * p] = cadd(cmul(akp, up0), cmul(akq, up1));
+          A[k + m * q] = cadd(cmul(akp, uq0), cmul(akq, uq1));
+        }
+        for (int k = 0; k < m; ++k) {
+          const cplx apk = A[p + m * k], aqk = A[q + m * k];
+          A[p + m * k] = cadd(cmulc(up0, apk), cmulc(up1, aqk));
+          A[q + m * k] = cadd(cmulc(uq0, apk), cmulc(uq1, aqk));
+        }
+        for (int k = 0; k < m; ++k) {
+          const cplx vkp = V[k + m * p], vkq = V[k + m * q];
+          V[k + m * p] = cadd(cmul(vkp, up0), cmul(vkq, up1));
+          V[k + m * q] = cadd(cmul(vkp, uq0), cmul(vkq, uq1));
+        }
+      }
+  }
+}
+
+// One thread per cluster: Q (kx x kx, zeroed) gets the cluster rotations on
+// the cluster's own state indices.  Scratch: the cluster at sorted start r
+// uses A at sa + r kx and V at sv + r kx (m^2 <= (kx - r) kx entries).
+__global__ void k_rr_jacobi(int kx, const cplx* __restrict__ Hk, RRScratch s, cplx* __restrict__ Q,
+                            cplx* __restrict__ sa, cplx* __restrict__ sv, int* status) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= *s.nclust) return;
+  const int r0 = s.cstart[c], m = s.csize[c];
+  if (m == 1) {
+    const int i = s.perm[r0];
+    Q[i + (long long)kx * i] = cmk(1.0, 0.0);
+    return;
+  }
+  if (m > RR_MAXC) {
+    atomicMax(&status[ST_REFINE], m);
+    for (int p = 0; p < m; ++p) {
+      const int i = s.perm[r0 + p];
+      Q[i + (long long)kx * i] = cmk(1.0, 0.0);
+    }
+    return;
+  }
+  cplx* A = sa + (long long)r0 * kx;
+  cplx* V = sv + (long long)r0 * kx;
+  for (int q = 0; q < m; ++q)
+    for (int p = 0; p < m; ++p)
+      A[p + m * q] = Hk[s.perm[r0 + p] + (long long)kx * s.perm[r0 + q]];
+  jacobi_herm(m, A, V);
+  for (int q = 0; q < m; ++q)
+    for (int p = 0; p < m; ++p)
+      Q[s.perm[r0 + p] + (long long)kx * s.perm[r0 + q]] = V[p + m * q];
+}
+
+// One warp per state a of the rotated basis (Hp = Q^H Hk Q): second-order
+// eigenvalue and first-order vector T(:, a) from the couplings to other clusters.
+__global__ void k_rr_perturb(int kx, const cplx* __restrict__ Hp, RRScratch s, cplx* __restrict__ T) {
+  const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (a >= kx) return;
+  const double mua = Hp[a + (long long)kx * a].x;
+  const int ca = s.cid[a];
+  double corr = 0.0;
+  for (int b = lane; b < kx; b += 32) {
+    cplx t = cmk(b == a ? 1.0 : 0.0, 0.0);
+    if (s.cid[b] != ca) {
+      const cplx hba = Hp[b + (long long)kx * a];
+      const double d = mua - Hp[b + (long long)kx * b].x;
+      corr += (hba.x * hba.x + hba.y * hba.y) / d;
+      t = cmk(hba.x / d, hba.y / d);
+    }
+    T[b + (long long)kx * a] = t;
+  }
+  for (int o = 16; o > 0; o >>= 1) corr += __shfl_xor_sync(0xffffffffu, corr, o);
+  if (lane == 0) s.lam[a] = mua + corr;
+}
+
+// One CTA: the k lowest refined eigenvalues (ascending) and their states.
+__global__ void __launch_bounds__(1024) k_rr_select(int kx, int k, RRScratch s, double* w) {
+  for (int a = threadIdx.x; a < kx; a += blockDim.x) {
+    const double la = s.lam[a];
+    int r = 0;
+    for (int b = 0; b < kx; ++b) {
+      const double lb = s.lam[b];
+      r += (lb < la) || (lb == la && b < a);
+    }
+    if (r < k) {
+      s.sel[r] = a;
+      w[r] = la;
+    }
+  }
+}
+
+// Tsel(:, r) = T(:, sel[r])
+__global__ void k_rr_gather(int kx, int k, const cplx* __restrict__ T, const int* __restrict__ sel,
+                            cplx* __restrict__ Ts) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (b < kx && r < k) Ts[b + (long long)kx * r] = T[b + (long long)kx * sel[r]];
 }
 
 __global__ void k_copy_eval(int k, const double* w, double* out) {
@@ -234,22 +463,6 @@ int stage_solve(excfv_handle* h, int n, int k, double evaltol, double* d_eval, c
   return EXCFV_OK;
 }
 
-// Standard Hermitian eigenproblem on ws.H (n x n, both triangles, destroyed):
-// lowest k eigenpairs -> ws.w and Z (n x k, ld n; returned pointer, one of
-// ws.Z / ws.Z2).  The k' x k' Rayleigh-Ritz problem of the precision form.
-static int solve_standard(excfv_handle* h, int n, int k, double evaltol, cplx** Zout) {
-  Workspace& ws = h->ws;
-  int rc;
-  if ((rc = tridiag_reduce(h, n, ws.H, n))) return rc;
-  cplx* Z = ws.Z;
-  if ((rc = tridiag_eig(h, n, k, evaltol, ws.d, ws.e, ws.w, Z, n, ws.stein_ws, ws.icl))) return rc;
-  if ((rc = cholqr(h, n, k, Z, n))) return rc;
-  if ((rc = apply_q(h, n, k, ws.H, n, Z, n))) return rc;
-  ws.Z = Z;
-  *Zout = Z;
-  return EXCFV_OK;
-}
-
 // The precision form: FP64 Cholesky and reduction to C = U^-H H U^-1; the
 // Householder tridiagonal reduction of a complex64 copy of C; eigenpairs of T
 // for k' = k + extra states and their back-transform; then Rayleigh-Ritz in
@@ -301,41 +514,52 @@ static int stage_solve_mixed(excfv_handle* h, int n, int k, double evaltol, doub
   prof_begin(h, PROF_BACKTR);
   if ((rc = apply_q(h, n, kx, ws.O, ld, Z, ld))) return rc;
   if ((rc = cholqr(h, n, kx, Z, ld))) return rc;
-  // R = C X0 (FP64, full C)
+  // Rayleigh-Ritz matrix in FP64: R = C X0, Hk = X0^H R (k' x k', into ws.T)
   cplx* R = ws.Z2;
   if ((rc = zgemm1(s, OP_N, OP_N, n, kx, n, one, ws.H, ld, Z, ld, zero, R, ld))) return rc;
-  // the k' x k' problem runs on a nested context with its own workspace
-  if (!h->sub) {
-    h->sub = new excfv_handle();
-    h->sub->owns_static = false;
+  cplx* Hk = ws.T;
+  if ((rc = zgemm1(s, OP_C, OP_N, kx, kx, n, one, Z, ld, R, ld, zero, Hk, kx, TRI_UPPER))) return rc;
+  if ((rc = mirror_upper(s, kx, Hk, kx))) return rc;
+  // clusters, their exact rotations Q (ws.O), Hp = Q^H Hk Q, perturbation
+  RRScratch rs;
+  {
+    double* dp = ws.stein_ws;
+    rs.D = dp; rs.lam = dp + kx;
+    int* ip = reinterpret_cast<int*>(dp + 2 * kx);
+    rs.perm = ip; rs.cid = ip + kx; rs.cstart = ip + 2 * kx; rs.csize = ip + 3 * kx;
+    rs.sel = ip + 4 * kx; rs.nclust = ip + 5 * kx;
   }
-  excfv_handle* sub = h->sub;
-  sub->device = h->device;
-  sub->nsm = h->nsm;
-  sub->grid_ctas = h->grid_ctas;
-  sub->stream = s;
-  sub->st = h->st;
-  sub->have_static = h->have_static;
-  sub->prec = EXCFV_PREC_FP64;
-  sub->prof.on = false;
-  if ((rc = stage_reserve(sub, kx, 1, k))) return rc;
-  if ((rc = zgemm1(s, OP_C, OP_N, kx, kx, n, one, Z, ld, R, ld, zero, sub->ws.H, kx, TRI_UPPER)))
-    return rc;
-  if ((rc = mirror_upper(s, kx, sub->ws.H, kx))) return rc;
-  CUDA_TRY(cudaMemsetAsync(sub->ws.status, 0, ST_NWORDS * sizeof(int), s));
-  cplx* Y = nullptr;
-  if ((rc = solve_standard(sub, kx, k, evaltol, &Y))) return rc;
-  bind_gemm_ctx(h);
-  // X = X0 Y (n x k) into R's buffer, then the back-transform with U^-1
-  if ((rc = zgemm1(s, OP_N, OP_N, n, k, kx, one, Z, ld, Y, kx, zero, R, ld))) return rc;
-  if ((rc = zgemm1(s, OP_N, OP_N, n, k, n, one, ws.Ui, ld, R, ld, zero, d_evec, ldevec, TRI_NONE,
+  cplx* Q = ws.O;
+  CUDA_TRY(cudaMemsetAsync(Q, 0, sizeof(cplx) * (size_t)kx * kx, s));
+  k_rr_clusters<<<1, 1024, 0, s>>>(kx, Hk, rs); count_launch();
+  CUDA_TRY(cudaGetLastError());
+  k_rr_jacobi<<<(kx + 127) / 128, 128, 0, s>>>(kx, Hk, rs, Q, ws.Gk, ws.Gki, ws.status); count_launch();
+  CUDA_TRY(cudaGetLastError());
+  cplx* W = ws.H;
+  if ((rc = zgemm1(s, OP_N, OP_N, kx, kx, kx, one, Hk, kx, Q, kx, zero, W, kx))) return rc;
+  cplx* Hp = ws.T;  // Hk is consumed
+  if ((rc = zgemm1(s, OP_C, OP_N, kx, kx, kx, one, Q, kx, W, kx, zero, Hp, kx))) return rc;
+  cplx* T = ws.H;   // W is consumed
+  k_rr_perturb<<<(kx * 32 + 255) / 256, 256, 0, s>>>(kx, Hp, rs, T); count_launch();
+  CUDA_TRY(cudaGetLastError());
+  k_rr_select<<<1, 1024, 0, s>>>(kx, k, rs, d_eval); count_launch();
+  CUDA_TRY(cudaGetLastError());
+  cplx* Ts = R;     // R is consumed
+  k_rr_gather<<<dim3((kx + 255) / 256, k), 256, 0, s>>>(kx, k, T, rs.sel, Ts); count_launch();
+  CUDA_TRY(cudaGetLastError());
+  cplx* Y = ws.T;   // Hp is consumed
+  if ((rc = zgemm1(s, OP_N, OP_N, kx, k, kx, one, Q, kx, Ts, kx, zero, Y, kx))) return rc;
+  // X = X0 Y (n x k, into ws.O: Q is consumed), Cholesky-QR, back-transform with U^-1
+  cplx* X = ws.O;
+  if ((rc = zgemm1(s, OP_N, OP_N, n, k, kx, one, Z, ld, Y, kx, zero, X, ld))) return rc;
+  cplx* const z_keep = Z;
+  cplx* const z2_keep = ws.Z2;
+  if ((rc = cholqr(h, n, k, X, ld))) return rc;  // X now points at the old ws.Z2 buffer
+  if ((rc = zgemm1(s, OP_N, OP_N, n, k, n, one, ws.Ui, ld, X, ld, zero, d_evec, ldevec, TRI_NONE,
                    TRI_UPPER, TRI_NONE)))
     return rc;
-  ws.Z = Z;
-  k_copy_eval<<<(k + 127) / 128, 128, 0, s>>>(k, sub->ws.w, d_eval); count_launch();
-  CUDA_TRY(cudaGetLastError());
-  k_or_status<<<1, ST_NWORDS, 0, s>>>(sub->ws.status, ws.status); count_launch();
-  CUDA_TRY(cudaGetLastError());
+  ws.Z = z_keep;
+  ws.Z2 = z2_keep;
   prof_end(h, PROF_BACKTR);
   return EXCFV_OK;
 }
@@ -358,5 +582,10 @@ int status_to_info(const int* st, int n) {
     return EXCFV_ERR_NOCONV;
   }
   if (st[ST_STEIN]) return st[ST_STEIN];
+  if (st[ST_REFINE]) {
+    excfv_set_error("precision form: %d near-degenerate states in one cluster exceed the "
+                    "refinement's limit; solve this k-point with EXCFV_PREC_FP64", st[ST_REFINE]);
+    return EXCFV_ERR_NOCONV;
+  }
   return EXCFV_OK;
 }

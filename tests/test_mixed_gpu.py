@@ -2,7 +2,9 @@
 
 The precision form reduces C = U^-H H U^-1 to tridiagonal form in complex64
 storage, carries k' = k + max(16, k/8) states through the eigensolver and
-restores FP64 accuracy with a Rayleigh-Ritz step in FP64.  Its bar is the
+restores FP64 accuracy with a Rayleigh-Ritz step in FP64: the k' x k' matrix
+X0^H C X0 is diagonalised exactly within clusters of near-degenerate states
+and by perturbation theory between them.  Its bar is the
 metric's: eigenvalues within 1e-8 Ha of ZHEGVX.  Eigenvectors are O-orthonormal
 to FP64 rounding (both the Ritz basis and the Ritz vectors are orthonormalised
 in FP64); their residuals are those of Ritz vectors from a complex64 basis,
@@ -67,6 +69,31 @@ def test_mixed_diamond2_state_counts(mixed_fv, nstfv):
     mixed_fv.set_static(st)
     w, X = mixed_fv.seceqn(kp)
     _check(H, O, w, X, w_ref)
+
+
+def test_mixed_degenerate_clusters(mixed_fv):
+    """Exactly degenerate triples and pairs, a near pair (1e-9) and a tight group:
+    the refinement diagonalises them as clusters; O != I."""
+    p = syn.make_problem("diamond2", ngk=60, nstfv=12)
+    mixed_fv.set_static(p.static)
+    rng = np.random.default_rng(3)
+    n = 150
+    lam = np.sort(rng.uniform(-1, 3, size=n))
+    lam[2:5] = lam[2]
+    lam[7:9] = lam[7]
+    lam[10] = lam[9] + 1e-9
+    lam[12:16] = lam[12] + 1e-6 * np.arange(4)
+    Q, _ = np.linalg.qr(rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n)))
+    A = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    B = np.eye(n) + 0.1 * (A + A.conj().T) / 2 / np.sqrt(n)
+    H = B.conj().T @ Q @ np.diag(lam) @ Q.conj().T @ B
+    O = B.conj().T @ B
+    w, X = mixed_fv.solvewithlapack(H, O, 20, 1e-14)
+    w_ref, _, info = fvref.solvewithlapack(H, O, 20, 1e-14)
+    assert info == 0
+    assert np.abs(w - w_ref).max() < EIG_TOL
+    assert fvref.residuals(H, O, w, X).max() < RES_TOL
+    assert fvref.o_orthonormality(O, X) < ORTH_TOL
 
 
 def test_mixed_small_matrix_uses_fp64(mixed_fv):
