@@ -421,9 +421,10 @@ def main():
     g_ms, g_cnt = prof["setup_gemm"]
     g_flops = 8.0 * (N * (N + 1) / 2) * AM
     g_ach = (g_flops / (g_ms / g_cnt / 1e3) / 1e12) if g_cnt else None
-    # tridiagonal panel: bytes of the trailing blocks read by y = C22 v, per launch
+    # tridiagonal panel: bytes of the lower triangle of the trailing block read
+    # by y = C22 v for every reduced column, per launch
     p_ms, p_cnt = prof["trd_panel"]
-    tot_bytes = sum(16.0 * (n - c - 1) ** 2 for c in range(n - 1))
+    tot_bytes = sum(16.0 * (n - c - 1) * (n - c) / 2 for c in range(n - 1))
     p_ach = (tot_bytes / p_cnt / (p_ms / p_cnt / 1e3) / 1e9) if p_cnt else None
     hbm = peaks.get("hbm_gbs") or 6650.0
     hbm_src = "measured" if peaks.get("hbm_gbs") else "fallback"
@@ -431,7 +432,7 @@ def main():
         roof = {"kernel": "k_tridiag_panel", "bound": "hbm", "achieved": p_ach, "peak": hbm,
                 "unit": "GB/s", "frac": (p_ach / hbm) if p_ach else None,
                 "traffic": traffic.get("k_tridiag_panel"),
-                "algorithmic": "16*m^2 bytes of the trailing block per column (y = C22 v), summed over the panel",
+                "algorithmic": "16*m(m+1)/2 bytes (lower triangle of the m x m trailing block, y = C22 v) per reduced column, summed over the launch's columns",
                 "peak_source": f"{hbm_src} HBM copy (MEASURED_PEAKS.json)"}
     else:
         roof = {"kernel": "zgemm_kernel (H/O setup)", "bound": "tensor", "achieved": g_ach,

@@ -7,6 +7,7 @@
 #include <chrono>
 #include <atomic>
 
+#include <algorithm>
 #include "handle.cuh"
 
 int match_compute_zdinv(DevStatic& st, const double* d_sprwin, const double* d_apwfrwin,
@@ -756,7 +757,8 @@ static int check_batch(excfv_handle* h, const BatchArgs& b, int* nmax) {
   return EXCFV_OK;
 }
 
-// Enqueues the whole batch on L lanes (round-robin), fork/join on h->stream.
+// Enqueues the whole batch on L lanes (largest k-points first, each to the
+// least-loaded lane), fork/join on h->stream.
 static int run_batch(excfv_handle* h, const BatchArgs& b, int L) {
   int nmax = 0;
   int rc = check_batch(h, b, &nmax);
@@ -779,8 +781,24 @@ static int run_batch(excfv_handle* h, const BatchArgs& b, int L) {
   const cudaMemcpyKind in = b.host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   const cudaMemcpyKind out = b.host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
   const int k_st = h->st.nstfv;
-  for (int k = 0; k < b.nk && rc == EXCFV_OK; ++k) {
-    excfv_handle* c = h->lanes[k % L];
+  // Longest-processing-time-first: k-points by decreasing nmatp^3 (the
+  // eigensolver's cost), each to the lane with the least work so far, so the
+  // lanes finish together although the basis sizes differ.
+  std::vector<int> order(b.nk), lane_of(b.nk);
+  for (int k = 0; k < b.nk; ++k) order[k] = k;
+  auto cost = [&](int k) { const double x = b.nmatp[k]; return x * x * x; };
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
+  {
+    std::vector<double> load(L, 0.0);
+    for (int k : order) {
+      const int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      lane_of[k] = l;
+      load[l] += cost(k);
+    }
+  }
+  for (int idx = 0; idx < b.nk && rc == EXCFV_OK; ++idx) {
+    const int k = order[idx];
+    excfv_handle* c = h->lanes[lane_of[k]];
     Workspace& ws = c->ws;
     cudaStream_t s = c->stream;
     const int ngp = b.ngp[k], n = b.nmatp[k];

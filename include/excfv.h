@@ -181,7 +181,9 @@ int excfv_seceqn_dev(excfv_handle* h, int32_t nmatp, int32_t ngp, int32_t ngkmax
 int excfv_sync(excfv_handle* h);
 
 /* ---- many k-points at once (the batching form) --------------------------
- * The k-points are dealt round-robin to "lanes": child contexts with their own
+ * The k-points are dealt to "lanes", largest nmatp first and each to the lane
+ * with the least work so far (nmatp^3), so that the lanes finish together;
+ * lanes are child contexts with their own
  * stream and workspace that share the handle's per-SCF-iteration data, each
  * running its k-points' match + setup + eigensolve with an SM budget of
  * (number of SMs / lanes) for the cooperative tridiagonal kernel, so several
