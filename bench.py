@@ -242,6 +242,46 @@ def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn, prec)
             "all_info_zero": bool(np.all(info == 0))}, evals
 
 
+def time_single_k(torch, np, dev, syn, name, prec, steps, warmup):
+    """Device-resident timing of one k-point of a workload (CUDA events on the
+    library's stream); returns (ms per k-point, eigenvalues, workload text)."""
+    from exciting_b200.fv import FirstVariational
+    p = syn.make_problem(name)
+    st, kp = p.static, p.kpts[0]
+    fv = FirstVariational(dev.index or 0, precision=prec)
+    fv.set_static(st)
+    fv.reserve(p.nmatmax, p.ngkmax)
+    stream = torch.cuda.Stream(device=dev)
+    fv.set_stream(stream.cuda_stream)
+
+    def dv(a, dt):
+        return torch.from_numpy(np.asfortranarray(np.asarray(a, dtype=dt)).ravel(order="F")).to(dev)
+
+    d = {nm: dv(getattr(kp, nm), dt) for nm, dt in (("gpc", np.float64), ("tpgpc", np.float64),
+                                                    ("sfacgp", np.complex128), ("igpig", np.int32),
+                                                    ("vgpc", np.float64))}
+    ptrs = {kk: v.data_ptr() for kk, v in d.items()}
+    ev = torch.zeros(st.nstfv, dtype=torch.float64, device=dev)
+    X = torch.zeros(st.nstfv * p.nmatmax, dtype=torch.complex128, device=dev)
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            fv.seceqn_dev(kp.nmat, kp.ngp, kp.ngkmax, ptrs, p.nmatmax, ev.data_ptr(), X.data_ptr())
+        fv.sync(kp.nmat)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(steps):
+            fv.seceqn_dev(kp.nmat, kp.ngp, kp.ngkmax, ptrs, p.nmatmax, ev.data_ptr(), X.data_ptr())
+        e.record(stream)
+        fv.sync(kp.nmat)
+        torch.cuda.synchronize()
+    w = ev.cpu().numpy()
+    fv.close()
+    del X, d
+    torch.cuda.empty_cache()
+    return s.elapsed_time(e) / steps, w, workload_desc(name, p)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -254,6 +294,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-nk", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=3)
+    ap.add_argument("--no-large", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -486,6 +527,16 @@ def main():
                    "mixed_batched_over_fp64_single": bmx["value"] / value,
                    "mixed_batched_over_fp64_batched": bmx["value"] / b64["value"]}
 
+    # ---- the large single-k-point workloads, both forms (rank 0, N = 1) ------
+    large = None
+    if rank == 0 and world == 1 and not args.no_large:
+        large = {}
+        for name, steps in (("cell16", 2), ("super64", 1)):
+            ms64, w64_, desc = time_single_k(torch, np, dev, syn, name, EXCFV_PREC_FP64, steps, 1)
+            msm, wm_, _ = time_single_k(torch, np, dev, syn, name, EXCFV_PREC_MIXED, steps, 1)
+            large[name] = {"workload": desc, "fp64_ms_per_k": ms64, "mixed_ms_per_k": msm,
+                           "mixed_eig_err_vs_fp64_gpu": float(np.abs(wm_ - w64_).max())}
+
     # ---- CPU baseline (rank 0, N = 1); its first k-point is the timed one ----
     cpu = None
     oracle_err = None
@@ -516,6 +567,7 @@ def main():
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "batched": batched,
+        "large_single_k": large,
         "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
     }
     if rank == 0:
