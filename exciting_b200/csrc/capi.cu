@@ -687,9 +687,10 @@ long long excfv_launch_count(void) { return g_launches.load(); }
 // ---------------------------------------------------------------------------
 
 // Largest lane count whose per-lane CTA budget still holds an n x n panel
-// (the panel kernel keeps 128 rows per CTA in shared memory).
+// (a CTA of the reduction owns 128 rows, 192 in complex64 storage).
 static int max_lanes_for(const excfv_handle* h, int nmax) {
-  const int need = (nmax + 127) / 128;
+  const int rows = tridiag_rows_per_cta(h->prec == EXCFV_PREC_MIXED);
+  const int need = (nmax + rows - 1) / rows;
   return std::max(1, h->nsm / std::max(1, need));
 }
 
@@ -914,7 +915,7 @@ int excfv_batch_info(excfv_handle* h, int32_t nk, int32_t* info) {
   return batch_info(h, nk, info);
 }
 
-// Times the batch with 1, 2, 4, 8, 16 lanes (those the SM budget allows) and
+// Times the batch with 1, 2, 4, 6, 8, 12, ... lanes (those the SM budget allows) and
 // keeps the fastest for later batched calls.  Device pointers; the outputs of
 // the last timed run are valid.  best_ms (optional) receives the winning time.
 int excfv_autotune_lanes(excfv_handle* h, int32_t nk, const int32_t* nmatp, const int32_t* ngp,
@@ -935,7 +936,9 @@ int excfv_autotune_lanes(excfv_handle* h, int32_t nk, const int32_t* nmatp, cons
   CUDA_TRY(cudaEventCreate(&e1));
   float best = 1e30f;
   int bestL = 1;
-  for (int L = 1; L <= lmax; L *= 2) {
+  const int cand[] = {1, 2, 4, 6, 8, 12, 16, 24, 32};
+  for (int L : cand) {
+    if (L > lmax) break;
     for (int rep = 0; rep < 2; ++rep) {  // the first run of a lane count sizes its workspaces
       CUDA_TRY(cudaEventRecord(e0, h->stream));
       if ((rc = run_batch(h, b, L))) break;

@@ -154,6 +154,8 @@ int stage_solve(excfv_handle* h, int n, int nstfv, double evaltol, double* d_eva
 // per-k status -> LAPACK-style info
 // states carried by the precision form (k plus a Rayleigh-Ritz buffer)
 int mixed_states(int n, int k);
+// rows one CTA of the tridiagonal reduction can own (FP64 or complex64 storage)
+int tridiag_rows_per_cta(bool complex64);
 int status_to_info(const int* st, int n);
 // device status -> LAPACK-style info (synchronises the stream)
 int stage_status(excfv_handle* h, int n);

@@ -35,7 +35,8 @@ namespace {
 constexpr int NBT = 32;
 constexpr int TT = 256;
 constexpr int RCH = 64;
-constexpr int MAXCH = 2;  // row chunks per CTA held in shared memory
+constexpr int MAXCH = 2;   // row chunks per CTA held in shared memory (FP64 storage)
+constexpr int MAXCH_C64 = 3;  // complex64 storage: up to three, for more concurrent lanes
 constexpr long long BARRIER_NS = 2000000000LL;  // 2 s
 
 // Storage type T2 of C, V and W: double2 (FP64 form) or float2 (the precision
@@ -55,11 +56,11 @@ template <> __device__ __forceinline__ float2 fromD<float2>(cplx v) {
   return make_float2((float)v.x, (float)v.y);
 }
 
-template <typename T2>
+template <typename T2, int MC>
 struct PanelSmem {
-  T2 V[MAXCH][NBT][RCH];
-  T2 W[MAXCH][NBT][RCH];
-  cplx X[MAXCH][RCH];
+  T2 V[MC][NBT][RCH];
+  T2 W[MC][NBT][RCH];
+  cplx X[MC][RCH];
 };
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -77,18 +78,18 @@ __device__ __forceinline__ double ldd(const double* p) { return __ldcg(p); }
 
 // Tiles of the trailing matrix for y = C22 v: 64 rows x BC columns (16 KB),
 // streamed through a ring of STAGES shared-memory slots by TMA.
-template <typename T2>
+template <typename T2, int MC>
 struct Ring {
   static constexpr int BC = (sizeof(T2) == 16) ? 16 : 32;
-  static constexpr int STAGES = (sizeof(T2) == 16) ? 4 : 8;
+  static constexpr int STAGES = (sizeof(T2) == 16) ? 4 : (MC <= 2 ? 8 : 6);
   static constexpr int TILE = RCH * BC;  // elements
   static constexpr unsigned BYTES = TILE * sizeof(T2);
 };
 constexpr int MAX_STAGES = 8;
 
-template <typename T2>
+template <typename T2, int MC>
 constexpr size_t panel_smem_bytes() {
-  return sizeof(PanelSmem<T2>) + 128 + (size_t)Ring<T2>::STAGES * Ring<T2>::BYTES;
+  return sizeof(PanelSmem<T2, MC>) + 128 + (size_t)Ring<T2, MC>::STAGES * Ring<T2, MC>::BYTES;
 }
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -246,16 +247,16 @@ __device__ __forceinline__ long long tile_run(long long t, long long t_end, int&
   return e;
 }
 
-template <typename T2>
+template <typename T2, int MC>
 __global__ void __launch_bounds__(TT + 32, 1)
     k_tridiag_panel(TridArgs<T2> a, const __grid_constant__ CUtensorMap tmap) {
-  using R = Ring<T2>;
+  using R = Ring<T2, MC>;
   extern __shared__ __align__(128) unsigned char dsm[];
-  PanelSmem<T2>& S = *reinterpret_cast<PanelSmem<T2>*>(dsm);
+  PanelSmem<T2, MC>& S = *reinterpret_cast<PanelSmem<T2, MC>*>(dsm);
   T2* ring;
   {
     const unsigned b0 = smem_u32(dsm);
-    const unsigned r0 = (b0 + (unsigned)sizeof(PanelSmem<T2>) + 127u) & ~127u;
+    const unsigned r0 = (b0 + (unsigned)sizeof(PanelSmem<T2, MC>) + 127u) & ~127u;
     ring = reinterpret_cast<T2*>(dsm + (r0 - b0));
   }
   __shared__ __align__(8) uint64_t s_full[MAX_STAGES];   // tile landed (TMA bytes)
@@ -331,7 +332,7 @@ __global__ void __launch_bounds__(TT + 32, 1)
   {
     const int c = a.p;
     double nrm_part = 0.0;
-    for (int ch = 0; ch < MAXCH; ++ch) {
+    for (int ch = 0; ch < MC; ++ch) {
       const int q = bid + ch * G;
       if (q >= nch) break;
       const int r = q * RCH + rloc;
@@ -537,7 +538,7 @@ __global__ void __launch_bounds__(TT + 32, 1)
       cplx ps[NBT / 4], pt[NBT / 4];
 #pragma unroll
       for (int u = 0; u < NBT / 4; ++u) { ps[u] = cmk(0.0, 0.0); pt[u] = cmk(0.0, 0.0); }
-      for (int ch = 0; ch < MAXCH; ++ch) {
+      for (int ch = 0; ch < MC; ++ch) {
         const int q = bid + ch * G;
         if (q >= nch) break;
         const int r = q * RCH + rloc;
@@ -620,8 +621,8 @@ __global__ void __launch_bounds__(TT + 32, 1)
       if (lane < i) s_wc[lane] = ldT(a.VW + c1 + ld * (NBT + lane));
       if (lane == 31) s_y1 = ldc(ycur + c1);
     }
-    cplx yr[MAXCH], cn[MAXCH];
-    for (int ch = 0; ch < MAXCH; ++ch) {
+    cplx yr[MC], cn[MC];
+    for (int ch = 0; ch < MC; ++ch) {
       yr[ch] = cmk(0.0, 0.0);
       cn[ch] = cmk(0.0, 0.0);
       const int q = bid + ch * G;
@@ -657,7 +658,7 @@ __global__ void __launch_bounds__(TT + 32, 1)
     csync();
     const double alpha = s_scal[4];
     double nrm_part = 0.0;
-    for (int ch = 0; ch < MAXCH; ++ch) {
+    for (int ch = 0; ch < MC; ++ch) {
       const int q = bid + ch * G;
       if (q >= nch) break;
       const int r = q * RCH + rloc;
@@ -830,7 +831,7 @@ static int make_tile_map(CUtensorMap* tm, const T2* C, int n, long long ld) {
   }
   const cuuint64_t dims[2] = {2ull * (cuuint64_t)n, (cuuint64_t)n};
   const cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(T2)};
-  const cuuint32_t box[2] = {2u * RCH, (cuuint32_t)Ring<T2>::BC};
+  const cuuint32_t box[2] = {2u * RCH, (cuuint32_t)Ring<T2, 2>::BC};
   const cuuint32_t estr[2] = {1u, 1u};
   const CUtensorMapDataType dt =
       (sizeof(T2) == 16) ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
@@ -844,7 +845,7 @@ static int make_tile_map(CUtensorMap* tm, const T2* C, int n, long long ld) {
   return EXCFV_OK;
 }
 
-template <typename T2>
+template <typename T2, int MC>
 static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
   Workspace& ws = h->ws;
   cudaStream_t s = h->stream;
@@ -855,16 +856,16 @@ static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
   }
   const int G = (h->grid_ctas > 0) ? h->grid_ctas : h->nsm;  // one CTA per SM of the budget
   const int nch = (n + RCH - 1) / RCH;
-  if (nch > MAXCH * G) {
-    excfv_set_error("tridiagonal reduction supports n <= %d on this GPU", MAXCH * G * RCH);
+  if (nch > MC * G) {
+    excfv_set_error("tridiagonal reduction supports n <= %d with %d CTAs", MC * G * RCH, G);
     return EXCFV_ERR_UNSUPPORTED;
   }
-  const int smem = (int)panel_smem_bytes<T2>();
+  const int smem = (int)panel_smem_bytes<T2, MC>();
   CUtensorMap tmap;
   if (int rc = make_tile_map(&tmap, C, n, ld)) return rc;
-  CUDA_TRY(cudaFuncSetAttribute(k_tridiag_panel<T2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  CUDA_TRY(cudaFuncSetAttribute(k_tridiag_panel<T2, MC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int per_sm = 0;
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tridiag_panel<T2>, TT + 32, smem));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tridiag_panel<T2, MC>, TT + 32, smem));
   if (per_sm < 1) {
     excfv_set_error("tridiag panel kernel cannot be resident");
     return EXCFV_ERR_CUDA;
@@ -889,7 +890,7 @@ static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
     ta.p = p; ta.nbp = nbp; ta.final_panel = final_panel;
     void* args[] = {&ta, &tmap};
     prof_begin(h, PROF_TRD_PANEL);
-    CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_tridiag_panel<T2>, dim3(G), dim3(TT + 32), args,
+    CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_tridiag_panel<T2, MC>, dim3(G), dim3(TT + 32), args,
                                          (size_t)smem, s));
     count_launch();
     prof_end(h, PROF_TRD_PANEL);
@@ -908,10 +909,16 @@ static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
 // Reduces C (n x n, both triangles) to tridiagonal d, e with reflectors
 // stored below the diagonal of C (unit entry stored explicitly).
 int tridiag_reduce(excfv_handle* h, int n, cplx* C, long long ld) {
-  return tridiag_reduce_t<double2>(h, n, C, ld);
+  return tridiag_reduce_t<double2, MAXCH>(h, n, C, ld);
 }
 
+// Rows one CTA of the reduction can own (its shared-memory row chunks).
+int tridiag_rows_per_cta(bool complex64) { return (complex64 ? MAXCH_C64 : MAXCH) * RCH; }
+
 // The same on a complex64 matrix (d, e and tau stay FP64).
+// Two row chunks per CTA (eight ring stages) when they suffice, else three.
 int tridiag_reduce_f32(excfv_handle* h, int n, float2* C, long long ld) {
-  return tridiag_reduce_t<float2>(h, n, C, ld);
+  const int G = (h->grid_ctas > 0) ? h->grid_ctas : h->nsm;
+  if ((n + RCH - 1) / RCH <= MAXCH * G) return tridiag_reduce_t<float2, MAXCH>(h, n, C, ld);
+  return tridiag_reduce_t<float2, MAXCH_C64>(h, n, C, ld);
 }
