@@ -440,58 +440,90 @@ __global__ void __launch_bounds__(TT + 32, 1)
           for (int u = 0; u < 4; ++u) { xr[u] = s_xr[rg + 16 * u]; xrT[u] = fromD<T2>(xr[u]); }
         }
         const int bend = min(ntile, (g1 - Jb) * BPT);
-        for (; b < bend; ++b) {
-          const unsigned q = gtile + b;
-          const unsigned slot = q % R::STAGES;
-          mbar_wait(&s_full[slot], (q / R::STAGES) & 1u, a.status);
-          const T2* tile = ring + (size_t)slot * R::TILE;
-          const int jt = Jb + b / BPT;                 // column tile of this box
-          const bool diag = (jt == I);
+        // Two tiles per step: their products and shuffle reductions are
+        // independent, so each warp has two chains in flight.
+        constexpr int NB = 2;
+        for (; b < bend;) {
+          const int nb = min(NB, bend - b);
+          T2 cp[NB][NPASS];
+          int jcol[NB][NPASS];
+          T2 xjv[NB][NPASS];
 #pragma unroll
-          for (int ps = 0; ps < NPASS; ++ps) {
-            const int cb = ps * 16 + cq;                // column within the box
-            const int jl = (b % BPT) * R::BC + cb;      // column within the 64-wide tile
-            const T2 xj = s_x[(jt - g0) * 64 + jl];
-            T2 cp = fromD<T2>(cmk(0.0, 0.0));
+          for (int z = 0; z < NB; ++z) {
+            if (z >= nb) break;
+            const unsigned q = gtile + b + z;
+            mbar_wait(&s_full[q % R::STAGES], (q / R::STAGES) & 1u, a.status);
+          }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const int rl = rg + 16 * u;
-              const T2 av = tile[cb * RCH + rl];
-              if (!diag || rl >= jl) {  // row part: A(r, j) x~(j)
-                if constexpr (sizeof(T2) == 16) {
-                  rowp[u].x += av.x * xj.x - av.y * xj.y;
-                  rowp[u].y += av.x * xj.y + av.y * xj.x;
-                } else {
-                  rowf[u].x = fmaf(av.x, xj.x, fmaf(-av.y, xj.y, rowf[u].x));
-                  rowf[u].y = fmaf(av.x, xj.y, fmaf(av.y, xj.x, rowf[u].y));
+          for (int z = 0; z < NB; ++z) {
+#pragma unroll
+            for (int ps = 0; ps < NPASS; ++ps) { cp[z][ps] = fromD<T2>(cmk(0.0, 0.0)); jcol[z][ps] = -1; }
+            if (z >= nb) continue;
+            const int bz = b + z;
+            const T2* tile = ring + (size_t)((gtile + bz) % R::STAGES) * R::TILE;
+            const int jt = Jb + bz / BPT;              // column tile of this box
+            const bool diag = (jt == I);
+#pragma unroll
+            for (int ps = 0; ps < NPASS; ++ps) {
+              const int cb = ps * 16 + cq;              // column within the box
+              const int jl = (bz % BPT) * R::BC + cb;   // column within the 64-wide tile
+              const T2 xj = s_x[(jt - g0) * 64 + jl];
+              xjv[z][ps] = xj;
+              jcol[z][ps] = rb + jt * 64 + jl;
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const int rl = rg + 16 * u;
+                const T2 av = tile[cb * RCH + rl];
+                if (!diag || rl >= jl) {  // row part: A(r, j) x~(j)
+                  if constexpr (sizeof(T2) == 16) {
+                    rowp[u].x += av.x * xj.x - av.y * xj.y;
+                    rowp[u].y += av.x * xj.y + av.y * xj.x;
+                  } else {
+                    rowf[u].x = fmaf(av.x, xj.x, fmaf(-av.y, xj.y, rowf[u].x));
+                    rowf[u].y = fmaf(av.x, xj.y, fmaf(av.y, xj.x, rowf[u].y));
+                  }
+                }
+                if (!diag || rl > jl) {   // column part: conj(A(r, j)) x~(r)
+                  cp[z][ps].x += av.x * xrT[u].x + av.y * xrT[u].y;
+                  cp[z][ps].y += av.x * xrT[u].y - av.y * xrT[u].x;
                 }
               }
-              if (!diag || rl > jl) {   // column part: conj(A(r, j)) x~(r)
-                cp.x += av.x * xrT[u].x + av.y * xrT[u].y;
-                cp.y += av.x * xrT[u].y - av.y * xrT[u].x;
-              }
-            }
-#pragma unroll
-            for (int o = 1; o < 16; o <<= 1) {
-              cp.x += __shfl_xor_sync(0xffffffffu, cp.x, o);
-              cp.y += __shfl_xor_sync(0xffffffffu, cp.y, o);
-            }
-            const int j = rb + jt * 64 + jl;
-            if (rg == 0 && j >= r0g && j < n) {
-              const cplx sc = cmul(scale, toD(cp));
-              atomicAdd(&ycur[j].x, sc.x);
-              atomicAdd(&ycur[j].y, sc.y);
-              const cplx vj = (j == c + 1) ? cmk(1.0, 0.0) : cmul(toD(xj), scale);
-              vav_re += vj.x * sc.x + vj.y * sc.y;  // conj(v_j) * contribution
-              vav_im += vj.x * sc.y - vj.y * sc.x;
             }
           }
-          // The slot is refilled by the async proxy (TMA): order this thread's
-          // generic reads of it before that write, then release it (one
+          // The slots are refilled by the async proxy (TMA): order this thread's
+          // generic reads of them before that write, then release them (one
           // arrival per consumer warp).
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
           __syncwarp();
-          if (lane == 0) mbar_arrive(&s_empty[slot]);
+          if (lane == 0) {
+            for (int z = 0; z < nb; ++z) mbar_arrive(&s_empty[(gtile + b + z) % R::STAGES]);
+          }
+#pragma unroll
+          for (int o = 1; o < 16; o <<= 1)
+#pragma unroll
+            for (int z = 0; z < NB; ++z)
+#pragma unroll
+              for (int ps = 0; ps < NPASS; ++ps) {
+                cp[z][ps].x += __shfl_xor_sync(0xffffffffu, cp[z][ps].x, o);
+                cp[z][ps].y += __shfl_xor_sync(0xffffffffu, cp[z][ps].y, o);
+              }
+          if (rg == 0) {
+#pragma unroll
+            for (int z = 0; z < NB; ++z)
+#pragma unroll
+              for (int ps = 0; ps < NPASS; ++ps) {
+                const int j = jcol[z][ps];
+                if (j >= r0g && j < n) {
+                  const cplx sc = cmul(scale, toD(cp[z][ps]));
+                  atomicAdd(&ycur[j].x, sc.x);
+                  atomicAdd(&ycur[j].y, sc.y);
+                  const cplx vj = (j == c + 1) ? cmk(1.0, 0.0) : cmul(toD(xjv[z][ps]), scale);
+                  vav_re += vj.x * sc.x + vj.y * sc.y;  // conj(v_j) * contribution
+                  vav_im += vj.x * sc.y - vj.y * sc.x;
+                }
+              }
+          }
+          b += nb;
         }
         if constexpr (sizeof(T2) == 8) {
 #pragma unroll
