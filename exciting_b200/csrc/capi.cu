@@ -137,6 +137,7 @@ void free_workspace(Workspace& ws) {
 
 int stage_set_static(excfv_handle* h, const excfv_static* s) {
   DevStatic& st = h->st;
+  h->static_gen++;
   free_static(st);
   h->have_static = false;
   if (!s || s->natmtot <= 0 || s->nspecies <= 0 || s->lmaxapw < 0 || s->apwordmax <= 0 ||
@@ -388,6 +389,8 @@ int excfv_create(int device, excfv_handle** out) {
   return EXCFV_OK;
 }
 
+static void drop_graph(excfv_handle* h);
+
 int excfv_destroy(excfv_handle* h) {
   if (!h) return EXCFV_OK;
   DeviceGuard g(h->device);
@@ -401,6 +404,7 @@ int excfv_destroy(excfv_handle* h) {
     delete c;
   }
   h->lanes.clear();
+  drop_graph(h);
   if (h->kinfo) cudaFree(h->kinfo);
   free_workspace(h->ws);
   if (h->owns_static) free_static(h->st);
@@ -758,6 +762,9 @@ static int check_batch(excfv_handle* h, const BatchArgs& b, int* nmax) {
   return EXCFV_OK;
 }
 
+static int enqueue_batch(excfv_handle* h, const BatchArgs& b, int L);
+static int run_batch_graph(excfv_handle* h, const BatchArgs& b, int L);
+
 // Enqueues the whole batch on L lanes (largest k-points first, each to the
 // least-loaded lane), fork/join on h->stream.
 static int run_batch(excfv_handle* h, const BatchArgs& b, int L) {
@@ -775,6 +782,14 @@ static int run_batch(excfv_handle* h, const BatchArgs& b, int L) {
   }
   h->batch_nmat.assign(b.nmatp, b.nmatp + b.nk);
   h->last_nk = b.nk;
+  if (!b.host && h->graph_on && !h->prof.on) return run_batch_graph(h, b, L);
+  return enqueue_batch(h, b, L);
+}
+
+// Stream work of one batch (no allocation, no host synchronisation), so that
+// it can also be captured into a CUDA graph.
+static int enqueue_batch(excfv_handle* h, const BatchArgs& b, int L) {
+  int rc = EXCFV_OK;
   cudaEvent_t fork;
   CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
   CUDA_TRY(cudaEventRecord(fork, h->stream));
@@ -864,6 +879,66 @@ int excfv_set_lanes(excfv_handle* h, int32_t nlanes) {
 
 int excfv_get_lanes(excfv_handle* h) { return h ? h->nlanes_pref : EXCFV_ERR_ARG; }
 
+static std::vector<unsigned long long> batch_key(const excfv_handle* h, const BatchArgs& b, int L) {
+  std::vector<unsigned long long> k = {(unsigned long long)b.nk, (unsigned long long)L,
+                                       (unsigned long long)h->prec, h->static_gen,
+                                       (unsigned long long)b.nmatmax, (unsigned long long)b.ngkmax,
+                                       (unsigned long long)(uintptr_t)h->stream};
+  for (int i = 0; i < b.nk; ++i) {
+    k.push_back((unsigned long long)b.nmatp[i]);
+    k.push_back((unsigned long long)b.ngp[i]);
+    for (const void* ptr : {(const void*)b.gpc[i], (const void*)b.tpgpc[i], (const void*)b.sfacgp[i],
+                            (const void*)b.igpig[i], (const void*)b.vgpc[i], (const void*)b.evalfv[i],
+                            (const void*)b.evecfv[i]})
+      k.push_back((unsigned long long)(uintptr_t)ptr);
+  }
+  return k;
+}
+
+static void drop_graph(excfv_handle* h) {
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  h->gexec = nullptr;
+}
+
+// A device-pointer batch that repeats the previous call exactly (same sizes,
+// pointers, lanes, precision and per-SCF-iteration data) replays a CUDA graph
+// captured on its second occurrence; the first occurrence runs eagerly and
+// sizes every workspace.  If capture or instantiation fails, the batch runs
+// eagerly and capture is not tried again for this key.
+static int run_batch_graph(excfv_handle* h, const BatchArgs& b, int L) {
+  std::vector<unsigned long long> key = batch_key(h, b, L);
+  if (key != h->gkey) {
+    drop_graph(h);
+    h->gkey.swap(key);
+    h->gseen = 0;
+  }
+  if (h->gexec) {
+    CUDA_TRY(cudaGraphLaunch(h->gexec, h->stream));
+    return EXCFV_OK;
+  }
+  if (h->gseen == 1) {
+    h->gseen = 2;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      const int rc = enqueue_batch(h, b, L);
+      const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+      cudaGraphExec_t ex = nullptr;
+      if (rc == EXCFV_OK && e == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess) {
+        cudaGraphDestroy(g);
+        h->gexec = ex;
+        CUDA_TRY(cudaGraphLaunch(h->gexec, h->stream));
+        return EXCFV_OK;
+      }
+      if (g) cudaGraphDestroy(g);
+      (void)cudaGetLastError();
+      g_err[0] = 0;
+    }
+    return enqueue_batch(h, b, L);
+  }
+  if (h->gseen < 2) h->gseen++;
+  return enqueue_batch(h, b, L);
+}
+
 static BatchArgs make_batch(int32_t nk, const int32_t* nmatp, const int32_t* ngp, int32_t ngkmax,
                             const double* const* gpc, const double* const* tpgpc,
                             const double* const* sfacgp, const int32_t* const* igpig,
@@ -907,6 +982,18 @@ int excfv_seceqn_batched(excfv_handle* h, int32_t nk, const int32_t* nmatp, cons
   int rc = run_batch(h, b, default_lanes(h, b));
   if (rc) return rc;
   return batch_info(h, nk, info);
+}
+
+int excfv_set_batch_graph(excfv_handle* h, int enable) {
+  if (!h) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  h->graph_on = enable != 0;
+  if (!h->graph_on) {
+    drop_graph(h);
+    h->gkey.clear();
+    h->gseen = 0;
+  }
+  return EXCFV_OK;
 }
 
 int excfv_batch_info(excfv_handle* h, int32_t nk, int32_t* info) {

@@ -111,6 +111,14 @@ struct excfv_handle {
   int kinfo_cap = 0;
   int last_nk = 0;
   std::vector<int> batch_nmat;  // nmatp of the last batch (info offsets)
+  unsigned static_gen = 0;      // incremented by every excfv_set_static
+  // CUDA graph of the last device-pointer batch: its key (sizes, pointers,
+  // lanes, precision, static generation), how often it ran eagerly, the
+  // instantiated graph once captured
+  bool graph_on = true;
+  std::vector<unsigned long long> gkey;
+  int gseen = 0;
+  cudaGraphExec_t gexec = nullptr;
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
   int prec = EXCFV_PREC_FP64;

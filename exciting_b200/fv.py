@@ -283,6 +283,10 @@ class FirstVariational:
             raise ExcfvError(rc, "excfv_batch_info")
         return info
 
+    def set_batch_graph(self, enable: bool = True) -> None:
+        """Replay repeated device-pointer batches as one captured CUDA graph."""
+        self._check(self._L.excfv_set_batch_graph(self._h, int(enable)), "excfv_set_batch_graph")
+
     def set_lanes(self, nlanes: int) -> None:
         self._check(self._L.excfv_set_lanes(self._h, nlanes), "excfv_set_lanes")
 

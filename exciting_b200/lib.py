@@ -55,6 +55,7 @@ SIGNATURES = {
     "excfv_destroy": (C.c_int, [C.c_void_p]),
     "excfv_last_error": (C.c_char_p, []),
     "excfv_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
+    "excfv_set_batch_graph": (C.c_int, [C.c_void_p, C.c_int]),
     "excfv_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "excfv_reserve": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "excfv_set_static": (C.c_int, [C.c_void_p, C.POINTER(ExcfvStatic)]),

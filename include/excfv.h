@@ -209,6 +209,11 @@ int excfv_seceqn_batched(excfv_handle* h, int32_t nk, const int32_t* nmatp, cons
                          double* const* evecfv, int32_t* info);
 /* Waits for the last batch and returns per-k status (info may be NULL). */
 int excfv_batch_info(excfv_handle* h, int32_t nk, int32_t* info);
+/* Device-pointer batches that repeat the previous call exactly (same sizes,
+ * pointers, lanes, precision and per-SCF-iteration data) run as one CUDA graph,
+ * captured on the second occurrence (default on; 0 = always launch eagerly).
+ * Profiling (excfv_profile) runs batches eagerly. */
+int excfv_set_batch_graph(excfv_handle* h, int enable);
 /* Lane count for the batched calls (0 = heuristic default). */
 int excfv_set_lanes(excfv_handle* h, int32_t nlanes);
 int excfv_get_lanes(excfv_handle* h);
