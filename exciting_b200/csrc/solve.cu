@@ -317,6 +317,12 @@ __global__ void __launch_bounds__(1024) k_rr_select(int kx, int k, RRScratch s, 
   }
 }
 
+// M (m x m, leading dimension ld) -= I
+__global__ void k_sub_identity(int m, cplx* M, long long ld) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) M[i + ld * i].x -= 1.0;
+}
+
 // Tsel(:, r) = T(:, sel[r])
 __global__ void k_rr_gather(int kx, int k, const cplx* __restrict__ T, const int* __restrict__ sel,
                             cplx* __restrict__ Ts) {
@@ -509,18 +515,35 @@ static int stage_solve_mixed(excfv_handle* h, int n, int k, double evaltol, doub
   CUDA_TRY(cudaGetLastError());
   cplx* Z = ws.Z;
   prof_begin(h, PROF_STEIG);
-  if ((rc = tridiag_eig(h, n, kx, evaltol, ws.d, ws.e, ws.w, Z, ld, ws.stein_ws, ws.icl))) return rc;
+  // T's eigenvalues only seed inverse iteration and are replaced by the
+  // refinement's, so bisection stops at 1e-10 (evaltol if looser)
+  if ((rc = tridiag_eig(h, n, kx, fmax(evaltol, 1e-10), ws.d, ws.e, ws.w, Z, ld, ws.stein_ws, ws.icl)))
+    return rc;
   prof_end(h, PROF_STEIG);
   prof_begin(h, PROF_BACKTR);
   if ((rc = apply_q(h, n, kx, ws.O, ld, Z, ld))) return rc;
-  if ((rc = cholqr(h, n, kx, Z, ld))) return rc;
-  // Rayleigh-Ritz matrix in FP64: R = C X0, Hk = X0^H R (k' x k', into ws.T)
+  // X0 = Z: orthonormal up to the complex64 rounding of the reflectors,
+  // S = X0^H X0 = I + D with |D| ~ 1e-7.  Rayleigh-Ritz in FP64 on
+  // S^-1/2 Hk S^-1/2 with S^-1/2 = I - D/2 (error O(D^2)):
+  //   Hm = Hk - (D Hk + Hk D)/2,  refine Hm -> (lambda, Y),  Y <- (I - D/2) Y,
+  // then one first-order Loewdin step Y <- Y (I - (Y^H S Y - I)/2) makes
+  // X = X0 Y orthonormal (error O(|Y^H S Y - I|^2) ~ 1e-12).
+  const cplx mhalf = cmk(-0.5, 0.0);
   cplx* R = ws.Z2;
   if ((rc = zgemm1(s, OP_N, OP_N, n, kx, n, one, ws.H, ld, Z, ld, zero, R, ld))) return rc;
   cplx* Hk = ws.T;
   if ((rc = zgemm1(s, OP_C, OP_N, kx, kx, n, one, Z, ld, R, ld, zero, Hk, kx, TRI_UPPER))) return rc;
   if ((rc = mirror_upper(s, kx, Hk, kx))) return rc;
-  // clusters, their exact rotations Q (ws.O), Hp = Q^H Hk Q, perturbation
+  cplx* Dm = ws.Gk;  // S - I
+  if ((rc = zgemm1(s, OP_C, OP_N, kx, kx, n, one, Z, ld, Z, ld, zero, Dm, kx, TRI_UPPER))) return rc;
+  if ((rc = mirror_upper(s, kx, Dm, kx))) return rc;
+  k_sub_identity<<<(kx + 127) / 128, 128, 0, s>>>(kx, Dm, kx); count_launch();
+  CUDA_TRY(cudaGetLastError());
+  cplx* Hm = ws.O;   // the reflectors are consumed
+  CUDA_TRY(cudaMemcpyAsync(Hm, Hk, sizeof(cplx) * (size_t)kx * kx, cudaMemcpyDeviceToDevice, s));
+  if ((rc = zgemm1(s, OP_N, OP_N, kx, kx, kx, mhalf, Dm, kx, Hk, kx, one, Hm, kx))) return rc;
+  if ((rc = zgemm1(s, OP_N, OP_N, kx, kx, kx, mhalf, Hk, kx, Dm, kx, one, Hm, kx))) return rc;
+  // clusters, their exact rotations Q, Hp = Q^H Hm Q, perturbation
   RRScratch rs;
   {
     double* dp = ws.stein_ws;
@@ -529,37 +552,48 @@ static int stage_solve_mixed(excfv_handle* h, int n, int k, double evaltol, doub
     rs.perm = ip; rs.cid = ip + kx; rs.cstart = ip + 2 * kx; rs.csize = ip + 3 * kx;
     rs.sel = ip + 4 * kx; rs.nclust = ip + 5 * kx;
   }
-  cplx* Q = ws.O;
+  cplx* Q = ws.T;    // Hk is consumed
   CUDA_TRY(cudaMemsetAsync(Q, 0, sizeof(cplx) * (size_t)kx * kx, s));
-  k_rr_clusters<<<1, 1024, 0, s>>>(kx, Hk, rs); count_launch();
+  k_rr_clusters<<<1, 1024, 0, s>>>(kx, Hm, rs); count_launch();
   CUDA_TRY(cudaGetLastError());
-  k_rr_jacobi<<<(kx + 127) / 128, 128, 0, s>>>(kx, Hk, rs, Q, ws.Gk, ws.Gki, ws.status); count_launch();
+  k_rr_jacobi<<<(kx + 127) / 128, 128, 0, s>>>(kx, Hm, rs, Q, ws.Z2, ws.H, ws.status); count_launch();
   CUDA_TRY(cudaGetLastError());
-  cplx* W = ws.H;
-  if ((rc = zgemm1(s, OP_N, OP_N, kx, kx, kx, one, Hk, kx, Q, kx, zero, W, kx))) return rc;
-  cplx* Hp = ws.T;  // Hk is consumed
+  cplx* W = ws.H;    // Jacobi scratch is consumed
+  if ((rc = zgemm1(s, OP_N, OP_N, kx, kx, kx, one, Hm, kx, Q, kx, zero, W, kx))) return rc;
+  cplx* Hp = ws.Z2;
   if ((rc = zgemm1(s, OP_C, OP_N, kx, kx, kx, one, Q, kx, W, kx, zero, Hp, kx))) return rc;
-  cplx* T = ws.H;   // W is consumed
-  k_rr_perturb<<<(kx * 32 + 255) / 256, 256, 0, s>>>(kx, Hp, rs, T); count_launch();
+  cplx* Tm = ws.O;   // Hm is consumed
+  k_rr_perturb<<<(kx * 32 + 255) / 256, 256, 0, s>>>(kx, Hp, rs, Tm); count_launch();
   CUDA_TRY(cudaGetLastError());
   k_rr_select<<<1, 1024, 0, s>>>(kx, k, rs, d_eval); count_launch();
   CUDA_TRY(cudaGetLastError());
-  cplx* Ts = R;     // R is consumed
-  k_rr_gather<<<dim3((kx + 255) / 256, k), 256, 0, s>>>(kx, k, T, rs.sel, Ts); count_launch();
+  cplx* Ts = ws.H;   // W is consumed
+  k_rr_gather<<<dim3((kx + 255) / 256, k), 256, 0, s>>>(kx, k, Tm, rs.sel, Ts); count_launch();
   CUDA_TRY(cudaGetLastError());
-  cplx* Y = ws.T;   // Hp is consumed
+  cplx* Y = ws.Z2;   // Hp is consumed
   if ((rc = zgemm1(s, OP_N, OP_N, kx, k, kx, one, Q, kx, Ts, kx, zero, Y, kx))) return rc;
-  // X = X0 Y (n x k, into ws.O: Q is consumed), Cholesky-QR, back-transform with U^-1
-  cplx* X = ws.O;
-  if ((rc = zgemm1(s, OP_N, OP_N, n, k, kx, one, Z, ld, Y, kx, zero, X, ld))) return rc;
-  cplx* const z_keep = Z;
-  cplx* const z2_keep = ws.Z2;
-  if ((rc = cholqr(h, n, k, X, ld))) return rc;  // X now points at the old ws.Z2 buffer
+  // Y1 = (I - D/2) Y
+  cplx* Y1 = ws.T;   // Q is consumed
+  CUDA_TRY(cudaMemcpyAsync(Y1, Y, sizeof(cplx) * (size_t)kx * k, cudaMemcpyDeviceToDevice, s));
+  if ((rc = zgemm1(s, OP_N, OP_N, kx, k, kx, mhalf, Dm, kx, Y, kx, one, Y1, kx))) return rc;
+  // E = Y1^H S Y1 - I = Y1^H (Y1 + D Y1) - I
+  cplx* SY = ws.O;   // Tm is consumed
+  CUDA_TRY(cudaMemcpyAsync(SY, Y1, sizeof(cplx) * (size_t)kx * k, cudaMemcpyDeviceToDevice, s));
+  if ((rc = zgemm1(s, OP_N, OP_N, kx, k, kx, one, Dm, kx, Y1, kx, one, SY, kx))) return rc;
+  cplx* E = ws.H;    // Ts is consumed
+  if ((rc = zgemm1(s, OP_C, OP_N, k, k, kx, one, Y1, kx, SY, kx, zero, E, k))) return rc;
+  k_sub_identity<<<(k + 127) / 128, 128, 0, s>>>(k, E, k); count_launch();
+  CUDA_TRY(cudaGetLastError());
+  // Y2 = Y1 (I - E/2)
+  cplx* Y2 = ws.Z2;  // Y is consumed
+  CUDA_TRY(cudaMemcpyAsync(Y2, Y1, sizeof(cplx) * (size_t)kx * k, cudaMemcpyDeviceToDevice, s));
+  if ((rc = zgemm1(s, OP_N, OP_N, kx, k, k, mhalf, Y1, kx, E, k, one, Y2, kx))) return rc;
+  // X = X0 Y2 (n x k, into ws.O), back-transform with U^-1
+  cplx* X = ws.O;    // SY is consumed
+  if ((rc = zgemm1(s, OP_N, OP_N, n, k, kx, one, Z, ld, Y2, kx, zero, X, ld))) return rc;
   if ((rc = zgemm1(s, OP_N, OP_N, n, k, n, one, ws.Ui, ld, X, ld, zero, d_evec, ldevec, TRI_NONE,
                    TRI_UPPER, TRI_NONE)))
     return rc;
-  ws.Z = z_keep;
-  ws.Z2 = z2_keep;
   prof_end(h, PROF_BACKTR);
   return EXCFV_OK;
 }
