@@ -4,15 +4,17 @@
 // Blocked in panels of NBT columns (the zlatrd/zher2k split of LAPACK's
 // blocked ZHETRD, restated): one persistent cooperative kernel reduces the
 // NBT columns of a panel, then one GEMM applies the rank-2*NBT update
-// C22 -= [V W] [W V]^H to the trailing matrix.  Inside the panel kernel every
-// column costs two grid-wide barriers:
+// C22 -= [V W] [W V]^H to the lower triangle of the trailing matrix (the only
+// part the reduction reads).  Inside the panel kernel every column costs two
+// grid-wide barriers:
 //
 //   phase 1 (row owners)  finish W(:, i-1); update column c with the panel's
 //                         previous reflectors; partial |x|^2 for the norm
 //   --- barrier ---
-//   phase 2 (all)         reflector (beta, tau) from the norm; y = C22 v
-//                         (the memory-bound Hermitian matrix-vector product,
-//                         tiled 64x64 over all CTAs, row sums by atomics);
+//   phase 2 (all)         reflector (beta, tau) from the norm; y = C22 v from
+//                         the lower 64 x 64 tiles (row part A x and column part
+//                         A^H x, equal tile counts per CTA), tiles streamed by
+//                         TMA into a shared-memory ring by a producer warp;
 //                         partial v^H C v, V^H v, W^H v
 //   --- barrier ---
 //   phase 3 (row owners)  store v; every CTA derives alpha = -1/2 |tau|^2 (v^H w)
@@ -23,8 +25,10 @@
 // panel's V and W rows of the rows it owns in shared memory, so the row
 // phases touch global memory once per row.  All loads of data written by
 // other CTAs inside the kernel use ld.global.cg (L2), since L1 is not
-// coherent across SMs.  Barrier waits are bounded in time; a timeout sets
-// status[ST_BARRIER] and every CTA then leaves the kernel.
+// coherent across SMs.  Every wait (grid barrier, TMA tile, free ring slot) is
+// bounded in time; a timeout sets status[ST_BARRIER] and every CTA then
+// leaves the kernel.  The kernel is instantiated for FP64 storage and for
+// complex64 storage (the precision form), with FP64 reflector arithmetic.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
