@@ -394,14 +394,15 @@ __global__ void __launch_bounds__(TT + 32, 1)
       if (xn2 == 0.0 && alpha.y == 0.0) {
         beta = alpha.x;
       } else {
+        // one square root, then two independent reciprocals (short dependent chain)
         const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
         beta = (alpha.x >= 0.0) ? -nrm : nrm;
-        tr = (beta - alpha.x) / beta;
-        ti = -alpha.y / beta;
         const double dr = alpha.x - beta, di = alpha.y;  // scale = 1 / (alpha - beta)
-        const double den = dr * dr + di * di;
-        scr = dr / den;
-        sci = -di / den;
+        const double rb = 1.0 / beta, rd = 1.0 / (dr * dr + di * di);
+        tr = 1.0 - alpha.x * rb;
+        ti = -alpha.y * rb;
+        scr = dr * rd;
+        sci = -di * rd;
       }
       s_scal[0] = tr; s_scal[1] = ti; s_scal[2] = scr; s_scal[3] = sci; s_scal[5] = beta;
     }
