@@ -211,26 +211,38 @@ int stage_setup(excfv_handle* h, int nmatp, int ngp, bool mirror_o) {
   prof_end(h, PROF_SETUP_OTHER);
   CUDA_TRY(cudaGetLastError());
   // H_GG = sum_a A_a^H Z_a (hamiltonsetup.f90:90-103), upper triangle
-  prof_begin(h, PROF_SETUP_GEMM);
-  if ((rc = zgemm1(s, OP_C, OP_N, N, N, (int)AM, one, ws.Apk, AM, ws.Zpk, AM, zero, ws.H, ld,
-                   TRI_UPPER)))
-    return rc;
-  prof_end(h, PROF_SETUP_GEMM);
   // O_GG = sum_a A_a^H (I + H1) A_a (overlapsetup.f90:82-108), upper triangle
-  const cplx* rhs = ws.Apk;
-  if (st.have_h1aa) {
+  if (!st.have_h1aa) {
+    // both contractions share A^H: one launch of two batch entries
+    // (B = Z or A, C = H or O; the strides are the distances between the buffers)
+    ZgemmArgs g;
+    g.m = N; g.n = N; g.k = (int)AM; g.kdec = 0; g.alpha = one; g.beta = zero;
+    g.A = ws.Apk; g.lda = AM; g.strideA = 0;
+    g.B = ws.Zpk; g.ldb = AM; g.strideB = ws.Apk - ws.Zpk;
+    g.C = ws.H; g.ldc = ld; g.strideC = ws.O - ws.H;
+    g.batch = 2; g.uplo_c = TRI_UPPER; g.tri_a = TRI_NONE; g.tri_b = TRI_NONE;
+    g.splitk = 1; g.part = nullptr;
+    prof_begin(h, PROF_SETUP_GEMM);
+    if ((rc = zgemm(s, OP_C, OP_N, g))) return rc;
+    prof_end(h, PROF_SETUP_GEMM);
+  } else {
+    // IORA*: Z is overwritten by (I + H1) A after the H contraction
+    prof_begin(h, PROF_SETUP_GEMM);
+    if ((rc = zgemm1(s, OP_C, OP_N, N, N, (int)AM, one, ws.Apk, AM, ws.Zpk, AM, zero, ws.H, ld,
+                     TRI_UPPER)))
+      return rc;
+    prof_end(h, PROF_SETUP_GEMM);
     const long long tot = AM * N;
     k_apply_h1<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(
         N, st.natmtot, st.maxaa, st.apwordmax, st.lmaxapw, st.idxis, st.flist, st.fofl,
         st.lmmaxapw, st.h1aa, ws.Apk, ws.Zpk); count_launch();
     CUDA_TRY(cudaGetLastError());
-    rhs = ws.Zpk;
+    prof_begin(h, PROF_SETUP_GEMM);
+    if ((rc = zgemm1(s, OP_C, OP_N, N, N, (int)AM, one, ws.Apk, AM, ws.Zpk, AM, zero, ws.O, ld,
+                     TRI_UPPER)))
+      return rc;
+    prof_end(h, PROF_SETUP_GEMM);
   }
-  prof_begin(h, PROF_SETUP_GEMM);
-  if ((rc = zgemm1(s, OP_C, OP_N, N, N, (int)AM, one, ws.Apk, AM, rhs, AM, zero, ws.O, ld,
-                   TRI_UPPER)))
-    return rc;
-  prof_end(h, PROF_SETUP_GEMM);
   CUDA_TRY(cudaGetLastError());
   prof_begin(h, PROF_SETUP_OTHER);
   // local-orbital band (columns N..n-1)
