@@ -21,13 +21,29 @@ namespace {
 
 constexpr double CLUSTER_REL = 1e-9;
 
+// 1/q from the hardware approximation refined by two Newton-Raphson steps
+// r <- r (2 - q r) (each roughly doubles the correct bits).
+__device__ __forceinline__ double recip_nr(double q) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(q));
+  r = fma(r, fma(-q, r, 1.0), r);
+  r = fma(r, fma(-q, r, 1.0), r);
+  return r;
+}
+
+// Number of eigenvalues of T below x (Sturm sequence of the LDL^T pivots).
+// The pivot recurrence q_i = d_i - x - e_{i-1}^2 / q_{i-1} uses recip_nr
+// instead of a division: within an ulp or so of the quotient, i.e. a relative
+// perturbation of e^2 of the order of the rounding the count already carries
+// (the count stays that of a nearby tridiagonal matrix), on a dependent chain
+// much shorter than a correctly rounded division.
 __device__ __forceinline__ int sturm_count(int n, const double* __restrict__ d,
                                            const double* __restrict__ e2, double x, double pivmin) {
   double q = d[0] - x;
   if (fabs(q) <= pivmin) q = -pivmin;
   int cnt = q < 0.0;
   for (int i = 1; i < n; ++i) {
-    q = d[i] - x - e2[i - 1] / q;
+    q = fma(-e2[i - 1], recip_nr(q), d[i] - x);
     if (fabs(q) <= pivmin) q = -pivmin;
     cnt += q < 0.0;
   }
