@@ -478,10 +478,11 @@ def main():
     g_flops = 2 * 8.0 * (N * (N + 1) / 2) * AM
     g_ach = (g_flops / (g_ms / args.steps / 1e3) / 1e12) if g_cnt else None
     # tridiagonal panel: bytes of the lower triangle of the trailing block read
-    # by y = C22 v for every reduced column, per launch
+    # by y = C22 v for every reduced column; p_ms and p_cnt cover all timed
+    # steps, so per launch: (steps * bytes per step / p_cnt) / (p_ms / p_cnt)
     p_ms, p_cnt = prof["trd_panel"]
     tot_bytes = sum(16.0 * (n - c - 1) * (n - c) / 2 for c in range(n - 1))
-    p_ach = (tot_bytes / p_cnt / (p_ms / p_cnt / 1e3) / 1e9) if p_cnt else None
+    p_ach = (args.steps * tot_bytes / p_cnt / (p_ms / p_cnt / 1e3) / 1e9) if p_cnt else None
     hbm = peaks.get("hbm_gbs") or 6650.0
     hbm_src = "measured" if peaks.get("hbm_gbs") else "fallback"
     if p_ms >= g_ms:
