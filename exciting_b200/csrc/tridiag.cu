@@ -85,7 +85,7 @@ __device__ __forceinline__ double ldd(const double* p) { return __ldcg(p); }
 template <typename T2, int MC>
 struct Ring {
   static constexpr int BC = (sizeof(T2) == 16) ? 16 : 32;
-  static constexpr int STAGES = (sizeof(T2) == 16) ? 4 : (MC <= 2 ? 8 : 6);
+  static constexpr int STAGES = (sizeof(T2) == 16) ? (MC == 1 ? 8 : 4) : (MC <= 2 ? 8 : 6);
   static constexpr int TILE = RCH * BC;  // elements
   static constexpr unsigned BYTES = TILE * sizeof(T2);
 };
@@ -237,16 +237,36 @@ __device__ __forceinline__ cplx warp_sum(cplx v) {
 
 constexpr int JB = 8;  // column tiles whose x values are staged per round trip
 
-// Lower 64 x 64 tiles of the trailing block in row-major order; the run that
-// starts at flat index t within its row tile: row I, columns [Jb, Je), ending
-// at t_end at the latest.  Returns the flat index after the run.
-__device__ __forceinline__ long long tile_run(long long t, long long t_end, int& I, int& Jb, int& Je) {
-  int q = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-  while ((long long)(q + 1) * (q + 2) / 2 <= t) ++q;
-  while ((long long)q * (q + 1) / 2 > t) --q;
-  I = q;
-  Jb = (int)(t - (long long)q * (q + 1) / 2);
-  const long long e = min((long long)q * (q + 1) / 2 + q + 1, t_end);
+// Lower 64 x 64 tiles of an nt x nt tile grid in folded row order: row k is
+// followed by row nt-1-k (k < nt/2; nt+1 tiles per pair), then the middle row
+// when nt is odd, so that equal shares of tiles hold a similar number of runs
+// (a run is the part of one row tile in a share).  Returns the run that starts
+// at flat index t: row I, columns [Jb, Je), ending at t_end at the latest, and
+// the flat index after it.
+__device__ __forceinline__ long long tile_run(long long t, long long t_end, int nt, int& I, int& Jb,
+                                              int& Je) {
+  const long long P = nt + 1;
+  const int npair = nt >> 1;
+  long long rs, re;
+  if (t < (long long)npair * P) {
+    const int k = (int)(t / P);
+    const long long base = (long long)k * P;
+    if (t < base + k + 1) {
+      I = k;
+      rs = base;
+      re = base + k + 1;
+    } else {
+      I = nt - 1 - k;
+      rs = base + k + 1;
+      re = base + P;
+    }
+  } else {
+    I = npair;
+    rs = (long long)npair * P;
+    re = rs + npair + 1;
+  }
+  Jb = (int)(t - rs);
+  const long long e = min(re, t_end);
   Je = Jb + (int)(e - t);
   return e;
 }
@@ -314,7 +334,7 @@ __global__ void __launch_bounds__(TT + 32, 1)
         const long long t_beg = ntri * bid / G, t_end = ntri * (bid + 1) / G;
         for (long long t = t_beg; t < t_end;) {
           int I, Jb, Je;
-          t = tile_run(t, t_end, I, Jb, Je);
+          t = tile_run(t, t_end, nt, I, Jb, Je);
           const int colb = rb + Jb * 64;
           const int ntile = (min(n, rb + Je * 64) - colb + R::BC - 1) / R::BC;
           for (int b = 0; b < ntile; ++b, ++q) {
@@ -377,7 +397,7 @@ __global__ void __launch_bounds__(TT + 32, 1)
     // column part.  The tile grid starts at row and column rb (even for
     // complex64, as the TMA row coordinate needs 16-byte alignment); rows and
     // columns below c+1 carry zero weight.  CTA b takes the lower tiles
-    // [b T / G, (b+1) T / G) in row-major order, as runs within one row tile.
+    // [b T / G, (b+1) T / G) in folded row order, as runs within one row tile.
     const int r0g = c + 1;
     const int rb = (sizeof(T2) == 8) ? (r0g & ~1) : r0g;
     const int nt = (n - rb + 63) / 64;
@@ -408,7 +428,7 @@ __global__ void __launch_bounds__(TT + 32, 1)
     }
     for (long long t = t_beg; t < t_end;) {
       int I, Jb, Je;
-      t = tile_run(t, t_end, I, Jb, Je);
+      t = tile_run(t, t_end, nt, I, Jb, Je);
       const int row0 = rb + I * 64;
       const int colb = rb + Jb * 64;
       const int ntile = (min(n, rb + Je * 64) - colb + R::BC - 1) / R::BC;
@@ -945,7 +965,11 @@ static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
 
 // Reduces C (n x n, both triangles) to tridiagonal d, e with reflectors
 // stored below the diagonal of C (unit entry stored explicitly).
+// One row chunk per CTA (eight ring stages, 128 KB of tiles in flight) when
+// that covers n, else two (four stages).
 int tridiag_reduce(excfv_handle* h, int n, cplx* C, long long ld) {
+  const int G = (h->grid_ctas > 0) ? h->grid_ctas : h->nsm;
+  if ((n + RCH - 1) / RCH <= G) return tridiag_reduce_t<double2, 1>(h, n, C, ld);
   return tridiag_reduce_t<double2, MAXCH>(h, n, C, ld);
 }
 

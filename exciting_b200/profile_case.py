@@ -1,9 +1,13 @@
 """Small, self-contained solve for kernel captures (ncu) and quick checks.
 
     python -m exciting_b200.profile_case [workload] [--mixed] [--solves N]
+                                         [--nk K --lanes L]
 
 Builds one k-point of a synthetic workload (exciting_b200.synthetic) and runs
-``FirstVariational.seceqn`` N times on cuda:0 (host buffers in and out).
+``FirstVariational.seceqn`` N times on cuda:0 (host buffers in and out).  With
+``--nk K`` the workload has K k-points (nmat uniform in 1800..2300 for cubic8)
+and ``seceqn_batched`` runs them over L lanes N times; a profiler serialises
+the lanes' kernels, so each captured launch shows one lane's grid alone.
 """
 import argparse
 
@@ -17,10 +21,22 @@ def main(argv=None):
     ap.add_argument("workload", nargs="?", default="cubic8")
     ap.add_argument("--mixed", action="store_true")
     ap.add_argument("--solves", type=int, default=2)
+    ap.add_argument("--nk", type=int, default=0)
+    ap.add_argument("--lanes", type=int, default=8)
     a = ap.parse_args(argv)
+    prec = EXCFV_PREC_MIXED if a.mixed else EXCFV_PREC_FP64
+    if a.nk > 0:
+        p = syn.make_problem(a.workload, nk=a.nk, ngk_range=(1800 - 64, 2300 - 64))
+        with FirstVariational(0, precision=prec) as fv:
+            fv.set_static(p.static)
+            fv.set_lanes(a.lanes)
+            for _ in range(a.solves):
+                res, info = fv.seceqn_batched(p.kpts, p.nmatmax)
+        print("lanes", a.lanes, "info", list(info), "lowest eigenvalues", res[0][0][:3])
+        return
     p = syn.make_problem(a.workload)
     kp = p.kpts[0]
-    with FirstVariational(0, precision=EXCFV_PREC_MIXED if a.mixed else EXCFV_PREC_FP64) as fv:
+    with FirstVariational(0, precision=prec) as fv:
         fv.set_static(p.static)
         for _ in range(a.solves):
             w, _ = fv.seceqn(kp)
