@@ -783,36 +783,89 @@ __global__ void k_tail_scalar(const T2* C, double* d) {
   if (threadIdx.x == 0 && blockIdx.x == 0) d[0] = toD(C[0]).x;
 }
 
-// Lower 64 x 64 tiles of C (m x m, complex64) -= A B^H, A and B m x 2NBT (leading dimension ld):
-// the trailing update of the complex64 reduction, FP32 products.  64 x 64
-// tiles of C per CTA, 16 x 16 threads with 4 x 4 outputs each (rows on the
-// fast thread index for coalesced stores), K staged in two chunks of NBT.
-__global__ void __launch_bounds__(256) k_her2k_f32(int m, const float2* __restrict__ A,
-                                                   const float2* __restrict__ B, long long ld,
-                                                   float2* __restrict__ C) {
-  __shared__ float2 sA[NBT][64 + 1];
-  __shared__ float2 sB[NBT][64 + 1];
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Lower 64 x 64 tiles of C (m x m, complex64) -= A B^H, A and B m x 2NBT
+// (leading dimension ld, even): the trailing update of the complex64
+// reduction, FP32 products.  Persistent, one CTA per SM: CTA b takes the
+// lower tiles b, b + G, ... (row-major over the lower triangle).  A tile's
+// 64 rows of A and B over the whole K = 2 NBT land in shared memory by
+// cp.async (k-major, 64 KB), and the next tile's are copied into the other
+// stage while this one is computed; the tile of C is read into registers
+// before the products.  16 x 16 threads with 4 x 4 outputs each (rows on the
+// fast thread index for coalesced accesses).
+constexpr int HK = 2 * NBT;
+constexpr int HER2K_SMEM = 2 * 2 * HK * 64 * (int)sizeof(float2);
+
+__device__ __forceinline__ void lower_tile(int t, int& I, int& J) {
+  int q = (int)((sqrtf(8.f * (float)t + 1.f) - 1.f) * 0.5f);
+  while ((q + 1) * (q + 2) / 2 <= t) ++q;
+  while (q * (q + 1) / 2 > t) --q;
+  I = q;
+  J = t - q * (q + 1) / 2;
+}
+
+__global__ void __launch_bounds__(256, 1) k_her2k_f32(int m, const float2* __restrict__ A,
+                                                      const float2* __restrict__ B, long long ld,
+                                                      float2* __restrict__ C) {
+  extern __shared__ __align__(16) float2 hsm[];  // [stage][A | B][k][64 rows]
+  const int nt = (m + 63) / 64;
+  const int T = nt * (nt + 1) / 2;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int r0 = blockIdx.x * 64, c0 = blockIdx.y * 64;
-  if (c0 > r0) return;  // the reduction reads the lower triangle only
-  float accr[4][4], acci[4][4];
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) { accr[u][v] = 0.f; acci[u][v] = 0.f; }
-  for (int kc = 0; kc < 2 * NBT; kc += NBT) {
-    for (int e = threadIdx.x; e < 64 * NBT; e += 256) {
-      const int rr = e & 63, kk = e >> 6;
-      const int ra = r0 + rr, cb = c0 + rr;
-      sA[kk][rr] = (ra < m) ? A[ra + ld * (kc + kk)] : make_float2(0.f, 0.f);
-      sB[kk][rr] = (cb < m) ? B[cb + ld * (kc + kk)] : make_float2(0.f, 0.f);
+  int t = blockIdx.x;
+  if (t >= T) return;
+  // rows r0.. of A and c0.. of B over all K into stage st; 16-byte chunks
+  // (two rows), rows past m zero-filled
+  auto issue = [&](int tt, int st) {
+    int I, J;
+    lower_tile(tt, I, J);
+    float2* sA = hsm + (size_t)st * 2 * HK * 64;
+    float2* sB = sA + HK * 64;
+    for (int e = threadIdx.x; e < HK * 32; e += 256) {
+      const int kk = e >> 5, ch = e & 31;
+      const int ra = I * 64 + 2 * ch, cb = J * 64 + 2 * ch;
+      const int na = max(0, min(2, m - ra)), nb = max(0, min(2, m - cb));
+      cp_async16(sA + kk * 64 + 2 * ch, na ? (const void*)(A + ra + ld * kk) : (const void*)A, 8 * na);
+      cp_async16(sB + kk * 64 + 2 * ch, nb ? (const void*)(B + cb + ld * kk) : (const void*)B, 8 * nb);
     }
+  };
+  issue(t, 0);
+  cp_async_commit();
+  for (int it = 0; t < T; t += gridDim.x, ++it) {
+    const int st = it & 1;
+    if (t + (int)gridDim.x < T) issue(t + gridDim.x, st ^ 1);
+    cp_async_commit();
+    int I, J;
+    lower_tile(t, I, J);
+    const int r0 = I * 64, c0 = J * 64;
+    float2 cv[4][4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int rr = r0 + tx + 16 * u, cc = c0 + ty + 16 * v;
+        cv[u][v] = (rr < m && cc < m) ? C[rr + ld * cc] : make_float2(0.f, 0.f);
+      }
+    float accr[4][4], acci[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) { accr[u][v] = 0.f; acci[u][v] = 0.f; }
+    cp_async_wait1();  // this stage's copies (the newest group may still be in flight)
     __syncthreads();
-#pragma unroll 4
-    for (int kk = 0; kk < NBT; ++kk) {
+    const float2* sA = hsm + (size_t)st * 2 * HK * 64;
+    const float2* sB = sA + HK * 64;
+#pragma unroll 8
+    for (int kk = 0; kk < HK; ++kk) {
       float2 av[4], bv[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) { av[u] = sA[kk][tx + 16 * u]; bv[u] = sB[kk][ty + 16 * u]; }
+      for (int u = 0; u < 4; ++u) { av[u] = sA[kk * 64 + tx + 16 * u]; bv[u] = sB[kk * 64 + ty + 16 * u]; }
 #pragma unroll
       for (int u = 0; u < 4; ++u)
 #pragma unroll
@@ -821,22 +874,17 @@ __global__ void __launch_bounds__(256) k_her2k_f32(int m, const float2* __restri
           acci[u][v] = fmaf(av[u].y, bv[v].x, fmaf(-av[u].x, bv[v].y, acci[u][v]));
         }
     }
-    __syncthreads();
-  }
 #pragma unroll
-  for (int v = 0; v < 4; ++v) {
-    const int cc = c0 + ty + 16 * v;
-    if (cc >= m) continue;
+    for (int v = 0; v < 4; ++v) {
+      const int cc = c0 + ty + 16 * v;
+      if (cc >= m) continue;
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int rr = r0 + tx + 16 * u;
-      if (rr < m) {
-        float2 x = C[rr + ld * cc];
-        x.x -= accr[u][v];
-        x.y -= acci[u][v];
-        C[rr + ld * cc] = x;
+      for (int u = 0; u < 4; ++u) {
+        const int rr = r0 + tx + 16 * u;
+        if (rr < m) C[rr + ld * cc] = make_float2(cv[u][v].x - accr[u][v], cv[u][v].y - acci[u][v]);
       }
     }
+    __syncthreads();  // this stage is refilled two tiles later
   }
 }
 
@@ -849,8 +897,15 @@ int her2k_update(excfv_handle* h, int m2, const double2* VW, const double2* WV, 
 }
 int her2k_update(excfv_handle* h, int m2, const float2* VW, const float2* WV, long long ld,
                  float2* C22) {
-  const dim3 grid((m2 + 63) / 64, (m2 + 63) / 64);
-  k_her2k_f32<<<grid, 256, 0, h->stream>>>(m2, VW, WV, ld, C22); count_launch();
+  if ((ld & 1) || (reinterpret_cast<uintptr_t>(VW) & 15) || (reinterpret_cast<uintptr_t>(WV) & 15)) {
+    excfv_set_error("complex64 trailing update: panels not 16-byte aligned (ld=%lld)", ld);
+    return EXCFV_ERR_ARG;
+  }
+  CUDA_TRY(cudaFuncSetAttribute(k_her2k_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, HER2K_SMEM));
+  // one CTA per SM of the handle's budget (a lane of a batch gets its share)
+  const int nt = (m2 + 63) / 64;
+  const int grid = min(nt * (nt + 1) / 2, (h->grid_ctas > 0) ? h->grid_ctas : h->nsm);
+  k_her2k_f32<<<grid, 256, HER2K_SMEM, h->stream>>>(m2, VW, WV, ld, C22); count_launch();
   CUDA_TRY(cudaGetLastError());
   return EXCFV_OK;
 }
