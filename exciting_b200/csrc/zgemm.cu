@@ -37,8 +37,13 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(ZgemmArgs p) {
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
-  const int i0 = blockIdx.x * BM;
-  const int j0 = blockIdx.y * BN;
+  // Tiles whose K range grows with the row (tri_a lower) or the column
+  // (tri_b upper) index are dispatched heaviest first, so that the last wave
+  // holds the short ones.
+  const bool rev_x = p.tri_a == TRI_LOWER;
+  const bool rev_y = p.tri_b == TRI_UPPER || (p.tri_a == TRI_LOWER && p.uplo_c == TRI_UPPER);
+  const int i0 = (rev_x ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x) * BM;
+  const int j0 = (rev_y ? (int)(gridDim.y - 1 - blockIdx.y) : (int)blockIdx.y) * BN;
   if (p.uplo_c == TRI_UPPER && i0 > j0 + BN - 1) return;
   if (p.uplo_c == TRI_LOWER && j0 > i0 + BM - 1) return;
   const long long bz = (p.splitk > 1) ? blockIdx.z / p.splitk : blockIdx.z;
