@@ -13,9 +13,9 @@
 //   --- barrier ---
 //   phase 2 (all)         reflector (beta, tau) from the norm; y = C22 v from
 //                         the lower 64 x 64 tiles (row part A x and column part
-//                         A^H x, equal tile counts per CTA), tiles streamed by
-//                         TMA into a shared-memory ring by a producer warp;
-//                         partial v^H C v, V^H v, W^H v
+//                         A^H x, equal tile counts per CTA in a folded row
+//                         order), tiles streamed by TMA into a shared-memory
+//                         ring by a producer warp; partial v^H C v, V^H v, W^H v
 //   --- barrier ---
 //   phase 3 (row owners)  store v; every CTA derives alpha = -1/2 |tau|^2 (v^H w)
 //                         from the reduced scalars, so the row of W needed by the
