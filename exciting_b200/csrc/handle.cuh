@@ -128,6 +128,7 @@ struct excfv_handle {
   double timings[4] = {0, 0, 0, 0};
   int nsm = 148;
   Prof prof;
+  bool her2k_smem_set = false;  // k_her2k_f32's shared-memory limit raised on this device
 };
 
 // makes the handle's split-K scratch current for this thread's GEMMs

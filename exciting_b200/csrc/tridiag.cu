@@ -901,7 +901,10 @@ int her2k_update(excfv_handle* h, int m2, const float2* VW, const float2* WV, lo
     excfv_set_error("complex64 trailing update: panels not 16-byte aligned (ld=%lld)", ld);
     return EXCFV_ERR_ARG;
   }
-  CUDA_TRY(cudaFuncSetAttribute(k_her2k_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, HER2K_SMEM));
+  if (!h->her2k_smem_set) {  // once per handle (handles are per device)
+    CUDA_TRY(cudaFuncSetAttribute(k_her2k_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, HER2K_SMEM));
+    h->her2k_smem_set = true;
+  }
   // one CTA per SM of the handle's budget (a lane of a batch gets its share)
   const int nt = (m2 + 63) / 64;
   const int grid = min(nt * (nt + 1) / 2, (h->grid_ctas > 0) ? h->grid_ctas : h->nsm);
