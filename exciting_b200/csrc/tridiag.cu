@@ -208,7 +208,8 @@ struct TridArgs {
   double* e;
   cplx* tau;
   cplx* ybuf;    // 2 x n
-  double* red;   // norm[NBT] | vav[2 NBT] | s[2 NBT NBT] | t[2 NBT NBT]
+  double* red;   // norm[NBT] | vav[2 NBT] | s[2 NBT NBT] | t[2 NBT NBT], zero at launch
+  double* red_next;  // the next panel's, zeroed by this launch
   unsigned* bar;
   int* status;
   int p, nbp, final_panel;
@@ -236,6 +237,7 @@ __device__ __forceinline__ cplx warp_sum(cplx v) {
 }
 
 constexpr int JB = 8;  // column tiles whose x values are staged per round trip
+constexpr int RED_DOUBLES = NBT + 2 * NBT + 4 * NBT * NBT;  // one panel's reduction slots
 
 // Lower 64 x 64 tiles of an nt x nt tile grid in folded row order: row k is
 // followed by row nt-1-k (k < nt/2; nt+1 tiles per pair), then the middle row
@@ -307,7 +309,9 @@ __global__ void __launch_bounds__(TT + 32, 1)
   double* red_s = a.red + 3 * NBT;
   double* red_t = a.red + 3 * NBT + 2 * NBT * NBT;
   const int nch = (n + RCH - 1) / RCH;
-  unsigned epoch = 0;
+  // the arrival counter runs on over the panels of one reduction: the
+  // panels before column p took two barriers per column
+  unsigned epoch = 2u * (unsigned)a.p;
   unsigned gtile = 0;  // tiles consumed by this CTA (ring slot and mbarrier phase)
   if (tid == 0) {
     for (int q = 0; q < R::STAGES; ++q) {
@@ -351,6 +355,9 @@ __global__ void __launch_bounds__(TT + 32, 1)
     }
     return;
   }
+
+  if (bid == 0)  // the next launch's reduction slots (its launch is stream-ordered after this one)
+    for (int t = tid; t < RED_DOUBLES; t += TT) a.red_next[t] = 0.0;
 
   // ---- prologue: column p needs no update; its norm and diagonal
   {
@@ -915,7 +922,7 @@ int her2k_update(excfv_handle* h, int m2, const float2* VW, const float2* WV, lo
 
 }  // namespace
 
-int tridiag_workspace_doubles() { return NBT + 2 * NBT + 4 * NBT * NBT; }
+int tridiag_workspace_doubles() { return 2 * RED_DOUBLES; }
 int tridiag_nb() { return NBT; }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point
@@ -994,14 +1001,19 @@ static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
   }
   T2* VW = reinterpret_cast<T2*>(ws.Wp);
   T2* WV = VW + (size_t)ld * 2 * NBT;
+  // once per reduction: both panels' reduction slots and the barrier counter;
+  // each panel launch then zeroes the slots of the next
+  CUDA_TRY(cudaMemsetAsync(ws.red, 0, sizeof(double) * tridiag_workspace_doubles(), s));
+  CUDA_TRY(cudaMemsetAsync(ws.bar, 0, 2 * sizeof(unsigned), s));
   for (int p = 0; p < n - 1; p += NBT) {
     const int nbp = min(NBT, n - 1 - p);
     const int final_panel = (p + nbp == n - 1) ? 1 : 0;
-    CUDA_TRY(cudaMemsetAsync(ws.red, 0, sizeof(double) * tridiag_workspace_doubles(), s));
-    CUDA_TRY(cudaMemsetAsync(ws.bar, 0, 2 * sizeof(unsigned), s));
+    const int pi = p / NBT;
     TridArgs<T2> ta;
     ta.n = n; ta.ld = ld; ta.C = C; ta.VW = VW; ta.WV = WV; ta.d = ws.d; ta.e = ws.e;
-    ta.tau = ws.tau; ta.ybuf = ws.ybuf; ta.red = ws.red; ta.bar = ws.bar; ta.status = ws.status;
+    ta.tau = ws.tau; ta.ybuf = ws.ybuf; ta.bar = ws.bar; ta.status = ws.status;
+    ta.red = ws.red + (size_t)(pi & 1) * RED_DOUBLES;
+    ta.red_next = ws.red + (size_t)((pi + 1) & 1) * RED_DOUBLES;
     ta.p = p; ta.nbp = nbp; ta.final_panel = final_panel;
     void* args[] = {&ta, &tmap};
     prof_begin(h, PROF_TRD_PANEL);
