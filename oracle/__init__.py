@@ -19,4 +19,8 @@ The eigensolve is LAPACK's own ZHEGVX (the routine the reference links).
 The setup restatement itself is unpinned by reference fixtures; it is checked
 against independent formulations (A^H aa A built from the definition, the
 interstitial matrix built from the Fourier coefficients directly).
+
+``two_stage`` restates the published two-stage Householder tridiagonal
+reduction (dense -> band -> tridiagonal) with explicit reflectors, the
+checker for a GPU reduction that follows the same reflector order.
 """

@@ -1,0 +1,132 @@
+"""Two-stage Householder reduction of a Hermitian matrix to real tridiagonal form.
+
+TEST INFRASTRUCTURE ONLY (like the rest of ``oracle/``).  The reference's
+eigensolve reduces in one stage: ZHEEVX -> ZHETRD -> ZHETD2/ZLATRD
+(``external/LAPACK/zheevx.f:441``, LAPACK 3.4.0).  The two-stage scheme
+restated here is the published one of LAPACK 3.7's ZHETRD_2STAGE
+(ZHETRD_HE2HB + ZHETRD_HB2ST; Haidar, Ltaief and Dongarra, SC'11): the same
+similarity transform C = Q T Q^H split into
+
+1. ``he2hb``: dense -> band of lower bandwidth b.  For each block column
+   [j, j+b) the QR of the panel C[j+b:, j:j+b] (b Householder reflectors)
+   leaves [R; 0] there, and the trailing block C[j+b:, j+b:] is updated
+   two-sidedly; the work is matrix-matrix (a GPU does it as GEMMs).
+2. ``hb2st``: band -> tridiagonal by bulge chasing.  Sweep i annihilates
+   column i below the subdiagonal with one reflector on rows [i+1, i+1+b);
+   the two-sided application spills a bulge one block further down, which the
+   next reflector of the sweep (on rows [j0+b, j0+2b), column j0) removes,
+   until the bulge leaves the matrix.  Every step touches O(b^2) entries.
+3. A diagonal phase makes the subdiagonal real and non-negative.
+
+In exact arithmetic T has the eigenvalues of C and Q maps T's eigenvectors to
+C's, as with the one-stage reduction; the reflectors differ, so T does not
+equal ZHETRD's T entry by entry.  Dense storage and explicit reflectors keep
+this a readable specification: a GPU version following the same order of
+reflectors reproduces the band matrix, the tridiagonal and the back-transform
+of these functions to rounding.
+
+Reflector convention (ZLARFG): H = I - tau v v^H with v[0] = 1 and
+H^H x = beta e_1, beta real.
+"""
+from __future__ import annotations
+
+from typing import List, Tuple
+
+import numpy as np
+
+
+def householder(x: np.ndarray) -> Tuple[np.ndarray, complex, float]:
+    """v, tau, beta with (I - tau v v^H)^H x = beta e_1, v[0] = 1, beta real (ZLARFG)."""
+    x = np.asarray(x, dtype=np.complex128)
+    alpha = x[0]
+    xnorm = float(np.linalg.norm(x[1:])) if len(x) > 1 else 0.0
+    v = np.zeros_like(x)
+    v[0] = 1.0
+    if xnorm == 0.0 and alpha.imag == 0.0:
+        return v, 0.0 + 0.0j, float(alpha.real)
+    beta = -np.copysign(np.hypot(abs(alpha), xnorm), alpha.real)
+    tau = complex((beta - alpha.real) / beta, -alpha.imag / beta)
+    v[1:] = x[1:] / (alpha - beta)
+    return v, tau, float(beta)
+
+
+def _apply_two_sided(C: np.ndarray, lo: int, v: np.ndarray, tau: complex) -> None:
+    """C <- H^H C H on rows and columns [lo, lo+len(v)) of the Hermitian C, H = I - tau v v^H."""
+    hi = lo + len(v)
+    # left: rows lo:hi of every column; right: columns lo:hi of every row
+    C[lo:hi, :] -= np.conj(tau) * np.outer(v, v.conj() @ C[lo:hi, :])
+    C[:, lo:hi] -= tau * np.outer(C[:, lo:hi] @ v, v.conj())
+
+
+def he2hb(C: np.ndarray, b: int) -> Tuple[np.ndarray, np.ndarray, List[Tuple[int, np.ndarray, np.ndarray]]]:
+    """Dense Hermitian C (lower triangle read) -> band of lower bandwidth b.
+
+    Returns the band matrix B (dense storage, Hermitian, zero outside
+    |r - c| <= b), Q1 with Q1^H C Q1 = B, and per block column j the panel's
+    reflectors (j, V, taus): V[:, t] is reflector t of rows [j+b+t, n), stored
+    from row j+b with its unit entry.
+    """
+    n = C.shape[0]
+    A = np.tril(C) + np.tril(C, -1).conj().T
+    A = A.astype(np.complex128)
+    Q1 = np.eye(n, dtype=np.complex128)
+    panels = []
+    for j in range(0, n - b - 1, b):
+        r0 = j + b
+        m = n - r0
+        nb = min(b, m - 1) if m > 1 else 0
+        V = np.zeros((m, nb), dtype=np.complex128)
+        taus = np.zeros(nb, dtype=np.complex128)
+        for t in range(nb):
+            # column j+t of the panel, rows r0+t .. n-1 (the rows above are R's)
+            v, tau, _ = householder(A[r0 + t:, j + t])
+            V[t:, t] = v
+            taus[t] = tau
+            _apply_two_sided(A, r0 + t, v, tau)
+            Q1[:, r0 + t:] -= tau * np.outer(Q1[:, r0 + t:] @ v, v.conj())
+        panels.append((j, V, taus))
+    # exact zeros outside the band (what the reflectors annihilated)
+    band = np.abs(np.subtract.outer(np.arange(n), np.arange(n))) <= b
+    return np.where(band, A, 0.0), Q1, panels
+
+
+def hb2st(B: np.ndarray, b: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray, list]:
+    """Band Hermitian B (lower bandwidth b) -> real symmetric tridiagonal (d, e).
+
+    Returns d (n), e (n-1, real, >= 0), Q2 with Q2^H B Q2 = tridiag(d, e) and
+    the reflectors in application order as (sweep i, first row lo, v, tau).
+    """
+    n = B.shape[0]
+    A = np.array(B, dtype=np.complex128)
+    Q2 = np.eye(n, dtype=np.complex128)
+    refl = []
+    for i in range(n - 2):
+        col, lo = i, i + 1
+        while lo < n - 1:
+            hi = min(lo + b, n)
+            if hi - lo < 2:
+                break
+            v, tau, _ = householder(A[lo:hi, col])
+            if tau != 0.0:
+                _apply_two_sided(A, lo, v, tau)
+                Q2[:, lo:hi] -= tau * np.outer(Q2[:, lo:hi] @ v, v.conj())
+            refl.append((i, lo, v, tau))
+            # the bulge sits in column lo, rows [lo+b, lo+2b): the next step's target
+            col, lo = lo, lo + b
+    # real, non-negative subdiagonal by a diagonal phase D: T = D^H A D
+    ph = np.ones(n, dtype=np.complex128)
+    sub = np.diag(A, -1).copy()
+    for k in range(n - 1):  # (D^H A D)[k+1, k] = conj(ph[k+1]) A[k+1, k] ph[k] = |A[k+1, k]|
+        s = sub[k] * ph[k]
+        a = abs(s)
+        ph[k + 1] = s / a if a > 0.0 else 1.0
+    d = np.real(np.diag(A)).copy()
+    e = np.abs(sub)
+    return d, e, Q2 * ph[None, :], refl
+
+
+def two_stage(C: np.ndarray, b: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """d, e and Q (= Q1 Q2 diag(phase)) with Q^H C Q = tridiag(d, e)."""
+    B, Q1, _ = he2hb(C, b)
+    d, e, Q2, _ = hb2st(B, b)
+    return d, e, Q1 @ Q2

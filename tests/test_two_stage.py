@@ -1,0 +1,77 @@
+"""The two-stage Householder reduction restated in ``oracle/two_stage.py``.
+
+Checks, on CPU, that each stage is a unitary similarity with the advertised
+structure (band of width b after the first stage, real tridiagonal after the
+second) and that the tridiagonal has the Hermitian matrix's eigenvalues, on
+random complex Hermitian and real symmetric matrices, a matrix with repeated
+eigenvalues, and the edge sizes (n <= b + 1, n = 1, 2).
+"""
+import numpy as np
+import pytest
+
+from oracle import two_stage as ts
+
+
+def _herm(n, rng, real=False):
+    X = rng.standard_normal((n, n))
+    if not real:
+        X = X + 1j * rng.standard_normal((n, n))
+    return (X + X.conj().T) / 2
+
+
+def _check(C, b):
+    n = C.shape[0]
+    scale = max(1.0, np.abs(C).max())
+    B, Q1, panels = ts.he2hb(C, b)
+    I = np.eye(n)
+    assert np.abs(Q1.conj().T @ Q1 - I).max() < 1e-13
+    full = Q1.conj().T @ C @ Q1
+    outside = np.abs(np.subtract.outer(np.arange(n), np.arange(n))) > b
+    if outside.any():
+        assert np.abs(full[outside]).max() < 1e-13 * scale * n
+    assert np.abs(full - B).max() < 1e-13 * scale * n
+    d, e, Q2, refl = ts.hb2st(B, b)
+    assert np.all(e >= 0.0)
+    T = np.diag(d) + np.diag(e, -1) + np.diag(e, 1)
+    Q = Q1 @ Q2
+    assert np.abs(Q.conj().T @ Q - I).max() < 1e-13
+    assert np.abs(Q.conj().T @ C @ Q - T).max() < 1e-13 * scale * n
+    assert np.abs(np.linalg.eigvalsh(T) - np.linalg.eigvalsh(C)).max() < 1e-13 * scale * n
+    return d, e, Q
+
+
+@pytest.mark.parametrize("n,b", [(37, 2), (37, 8), (64, 16), (100, 32), (130, 5), (50, 48)])
+def test_two_stage_random_hermitian(n, b):
+    _check(_herm(n, np.random.default_rng(n * 100 + b)), b)
+
+
+def test_two_stage_real_symmetric():
+    _check(_herm(80, np.random.default_rng(7), real=True), 12)
+
+
+def test_two_stage_repeated_eigenvalues():
+    rng = np.random.default_rng(11)
+    n = 60
+    lam = np.repeat(np.array([-2.0, 0.5, 0.5 + 1e-12, 3.0]), 15)
+    U, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    C = (U * lam) @ U.conj().T
+    d, e, Q = _check(C, 8)
+    w, Z = np.linalg.eigh(np.diag(d) + np.diag(e, -1) + np.diag(e, 1))
+    X = Q @ Z  # back-transformed eigenvectors of C
+    assert np.abs(C @ X - X * w).max() < 1e-12
+
+
+@pytest.mark.parametrize("n,b", [(1, 4), (2, 4), (5, 4), (6, 4), (9, 8)])
+def test_two_stage_edge_sizes(n, b):
+    _check(_herm(n, np.random.default_rng(n)), b)
+
+
+def test_householder_matches_zlarfg_convention():
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(9) + 1j * rng.standard_normal(9)
+    v, tau, beta = ts.householder(x)
+    H = np.eye(9) - tau * np.outer(v, v.conj())
+    y = H.conj().T @ x
+    assert v[0] == 1.0
+    assert abs(y[0] - beta) < 1e-13 and np.abs(y[1:]).max() < 1e-13
+    assert np.abs(H.conj().T @ H - np.eye(9)).max() < 1e-13
