@@ -90,6 +90,55 @@ def he2hb(C: np.ndarray, b: int) -> Tuple[np.ndarray, np.ndarray, List[Tuple[int
     return np.where(band, A, 0.0), Q1, panels
 
 
+def larft(V: np.ndarray, taus: np.ndarray) -> np.ndarray:
+    """Upper triangular T with H_0 H_1 ... H_{k-1} = I - V T V^H (ZLARFT 'F', 'C')."""
+    k = V.shape[1]
+    T = np.zeros((k, k), dtype=np.complex128)
+    for t in range(k):
+        T[t, t] = taus[t]
+        if t > 0:
+            T[:t, t] = -taus[t] * (T[:t, :t] @ (V[:, :t].conj().T @ V[:, t]))
+    return T
+
+
+def he2hb_blocked(C: np.ndarray, b: int) -> Tuple[np.ndarray, np.ndarray]:
+    """``he2hb`` in the compact-WY form a GPU runs as GEMMs.
+
+    Per block column j: the panel QR applies its reflectors to the panel only
+    (the trailing block does not feed the panel's later columns, so the
+    reflectors are those of ``he2hb``), T = ZLARFT(V, taus), then with
+    X = C22 V T and W = X - 1/2 V (T^H V^H X) the trailing update is the
+    rank-2b C22 -= V W^H + W V^H, i.e. Q^H C22 Q with Q = I - V T V^H.
+    Returns B and Q1 as ``he2hb`` does.
+    """
+    n = C.shape[0]
+    A = np.tril(C) + np.tril(C, -1).conj().T
+    A = A.astype(np.complex128)
+    Q1 = np.eye(n, dtype=np.complex128)
+    for j in range(0, n - b - 1, b):
+        r0 = j + b
+        m = n - r0
+        nb = min(b, m - 1)
+        P = A[r0:, j:j + b].copy()
+        V = np.zeros((m, nb), dtype=np.complex128)
+        taus = np.zeros(nb, dtype=np.complex128)
+        for t in range(nb):
+            v, tau, _ = householder(P[t:, t])
+            V[t:, t] = v
+            taus[t] = tau
+            P[t:, :] -= np.conj(tau) * np.outer(v, v.conj() @ P[t:, :])
+        T = larft(V, taus)
+        A[r0:, j:j + b] = P
+        A[j:j + b, r0:] = P.conj().T
+        A22 = A[r0:, r0:]
+        X = A22 @ V @ T
+        W = X - 0.5 * V @ (T.conj().T @ (V.conj().T @ X))
+        A[r0:, r0:] = A22 - V @ W.conj().T - W @ V.conj().T
+        Q1[:, r0:] -= (Q1[:, r0:] @ V) @ T @ V.conj().T
+    band = np.abs(np.subtract.outer(np.arange(n), np.arange(n))) <= b
+    return np.where(band, A, 0.0), Q1
+
+
 def hb2st(B: np.ndarray, b: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray, list]:
     """Band Hermitian B (lower bandwidth b) -> real symmetric tridiagonal (d, e).
 
@@ -123,6 +172,16 @@ def hb2st(B: np.ndarray, b: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray, li
     d = np.real(np.diag(A)).copy()
     e = np.abs(sub)
     return d, e, Q2 * ph[None, :], refl
+
+
+def apply_q2(refl: list, Z: np.ndarray) -> np.ndarray:
+    """Q2 Z for the chase reflectors of ``hb2st`` (without its diagonal phase):
+    Q2 = H_1 H_2 ... in generation order, so the last reflector acts first."""
+    X = np.array(Z, dtype=np.complex128)
+    for (_i, lo, v, tau) in reversed(refl):
+        hi = lo + len(v)
+        X[lo:hi, :] -= tau * np.outer(v, v.conj() @ X[lo:hi, :])
+    return X
 
 
 def two_stage(C: np.ndarray, b: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:

@@ -75,3 +75,28 @@ def test_householder_matches_zlarfg_convention():
     assert v[0] == 1.0
     assert abs(y[0] - beta) < 1e-13 and np.abs(y[1:]).max() < 1e-13
     assert np.abs(H.conj().T @ H - np.eye(9)).max() < 1e-13
+
+
+@pytest.mark.parametrize("n,b", [(37, 2), (64, 16), (130, 32), (130, 5), (9, 8)])
+def test_blocked_band_stage_matches_reflector_by_reflector(n, b):
+    """The compact-WY form (panel QR, ZLARFT, X = C22 V T, W = X - V (T^H V^H X)/2,
+    C22 -= V W^H + W V^H) gives the same band matrix and Q1."""
+    C = _herm(n, np.random.default_rng(n + 7 * b))
+    B, Q1, _ = ts.he2hb(C, b)
+    Bb, Q1b = ts.he2hb_blocked(C, b)
+    scale = np.abs(C).max()
+    assert np.abs(B - Bb).max() < 1e-13 * scale * n
+    assert np.abs(Q1 - Q1b).max() < 1e-13 * n
+
+
+def test_apply_q2_is_the_product_of_the_chase_reflectors():
+    rng = np.random.default_rng(21)
+    n, b = 90, 12
+    B, _, _ = ts.he2hb(_herm(n, rng), b)
+    _, _, _, refl = ts.hb2st(B, b)
+    Qd = np.eye(n, dtype=np.complex128)
+    for (_i, lo, v, tau) in refl:
+        hi = lo + len(v)
+        Qd[:, lo:hi] -= tau * np.outer(Qd[:, lo:hi] @ v, v.conj())
+    Z = rng.standard_normal((n, 9)) + 1j * rng.standard_normal((n, 9))
+    assert np.abs(ts.apply_q2(refl, Z) - Qd @ Z).max() < 1e-13
