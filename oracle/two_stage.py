@@ -174,6 +174,41 @@ def hb2st(B: np.ndarray, b: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray, li
     return d, e, Q2 * ph[None, :], refl
 
 
+def chase_tasks(n: int, b: int) -> list:
+    """The tasks of ``hb2st`` as (sweep i, step k, column, first row lo, end row hi):
+    step k of sweep i reflects rows [lo, hi) of that column, two-sidedly."""
+    out = []
+    for i in range(n - 2):
+        col, lo, k = i, i + 1, 0
+        while lo < n - 1:
+            hi = min(lo + b, n)
+            if hi - lo < 2:
+                break
+            out.append((i, k, col, lo, hi))
+            col, lo, k = lo, lo + b, k + 1
+    return out
+
+
+def run_chase(B: np.ndarray, tasks: list) -> np.ndarray:
+    """Applies the chase tasks to a copy of B in the given order; returns the result."""
+    A = np.array(B, dtype=np.complex128)
+    for (_i, _k, col, lo, hi) in tasks:
+        v, tau, _ = householder(A[lo:hi, col])
+        if tau != 0.0:
+            _apply_two_sided(A, lo, v, tau)
+    return A
+
+
+def chase_schedule(n: int, b: int, lag: int = 3, reverse_in_slot: bool = True) -> list:
+    """The chase tasks ordered by time slot lag * i + k.  With lag 3 the tasks of
+    one slot touch disjoint entries (task (i, k) needs (i-1, k+2) done), so a
+    slot can run concurrently; ``reverse_in_slot`` orders each slot's tasks by
+    decreasing sweep, which changes the result unless they are independent."""
+    key = (lambda t: (lag * t[0] + t[1], -t[0])) if reverse_in_slot else \
+          (lambda t: (lag * t[0] + t[1], t[0]))
+    return sorted(chase_tasks(n, b), key=key)
+
+
 def apply_q2(refl: list, Z: np.ndarray) -> np.ndarray:
     """Q2 Z for the chase reflectors of ``hb2st`` (without its diagonal phase):
     Q2 = H_1 H_2 ... in generation order, so the last reflector acts first."""

@@ -100,3 +100,14 @@ def test_apply_q2_is_the_product_of_the_chase_reflectors():
         Qd[:, lo:hi] -= tau * np.outer(Qd[:, lo:hi] @ v, v.conj())
     Z = rng.standard_normal((n, 9)) + 1j * rng.standard_normal((n, 9))
     assert np.abs(ts.apply_q2(refl, Z) - Qd @ Z).max() < 1e-13
+
+
+@pytest.mark.parametrize("n,b", [(60, 4), (97, 8), (130, 16)])
+def test_chase_schedule_lag_three_is_concurrency_safe(n, b):
+    """Time slot 3 i + k: each slot's tasks commute (executing them in reverse
+    sweep order gives the sweep-by-sweep result); slot 2 i + k does not."""
+    B, _, _ = ts.he2hb(_herm(n, np.random.default_rng(n)), b)
+    ref = ts.run_chase(B, ts.chase_tasks(n, b))
+    scale = np.abs(B).max()
+    assert np.abs(ts.run_chase(B, ts.chase_schedule(n, b, lag=3)) - ref).max() < 1e-13 * scale
+    assert np.abs(ts.run_chase(B, ts.chase_schedule(n, b, lag=2)) - ref).max() > 1e-3 * scale
