@@ -111,3 +111,58 @@ def test_chase_schedule_lag_three_is_concurrency_safe(n, b):
     scale = np.abs(B).max()
     assert np.abs(ts.run_chase(B, ts.chase_schedule(n, b, lag=3)) - ref).max() < 1e-13 * scale
     assert np.abs(ts.run_chase(B, ts.chase_schedule(n, b, lag=2)) - ref).max() > 1e-3 * scale
+
+
+def _harness(tmp_path):
+    """Builds tests/chase_harness.cu (host code only) with nvcc; skips without nvcc."""
+    import os
+    import shutil
+    import subprocess
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not available")
+    here = os.path.dirname(os.path.abspath(__file__))
+    exe = str(tmp_path / "chase_harness")
+    subprocess.run([nvcc, "-x", "cu", "-std=c++17", "-O2",
+                    "-I", os.path.join(here, "..", "exciting_b200", "csrc"),
+                    os.path.join(here, "chase_harness.cu"), "-o", exe], check=True)
+    return exe
+
+
+@pytest.mark.parametrize("n,b", [(40, 4), (97, 8), (150, 16), (70, 32)])
+def test_chase_task_on_band_storage_matches_dense_chase(tmp_path, n, b):
+    """exciting_b200/csrc/chase.cuh (compact band storage with bulge room),
+    run on the host sweep by sweep, reproduces the dense chase and its
+    reflectors."""
+    import subprocess
+    exe = _harness(tmp_path)
+    C = _herm(n, np.random.default_rng(3 * n + b))
+    B, _, _ = ts.he2hb(C, b)
+    ld = 2 * b + 1
+    ab = np.zeros((n, ld), dtype=np.complex128)  # row c = column c of the storage
+    for c in range(n):
+        for off in range(0, min(b, n - 1 - c) + 1):
+            ab[c, off] = B[c + off, c]
+    (tmp_path / "band.bin").write_bytes(ab.tobytes())
+    subprocess.run([exe, str(n), str(b), str(tmp_path / "band.bin"), str(tmp_path / "out.bin"),
+                    str(tmp_path / "refl.bin")], check=True)
+    out = np.frombuffer((tmp_path / "out.bin").read_bytes(), dtype=np.complex128).reshape(n, ld)
+    dense = ts.run_chase(B, ts.chase_tasks(n, b))
+    scale = np.abs(B).max()
+    for c in range(n):
+        for off in range(0, min(2 * b, n - 1 - c) + 1):
+            assert abs(out[c, off] - dense[c + off, c]) < 1e-12 * scale, (c, off)
+    # tridiagonal: everything below the subdiagonal is gone
+    assert np.abs(out[:, 2:]).max() < 1e-12 * scale
+    # the reflectors agree with hb2st's
+    _, _, _, refl = ts.hb2st(B, b)
+    rec = np.frombuffer((tmp_path / "refl.bin").read_bytes(), dtype=np.complex128)
+    pos = 0
+    for (i, lo, v, tau) in refl:
+        hdr_i, hdr_lo = int(rec[pos].real), int(rec[pos].imag)
+        ln = int(rec[pos + 1].real)
+        assert (hdr_i, hdr_lo, ln) == (i, lo, len(v))
+        assert abs(rec[pos + 2] - tau) < 1e-12
+        assert np.abs(rec[pos + 3:pos + 3 + ln] - v).max() < 1e-10
+        pos += 3 + ln
+    assert pos == len(rec)
