@@ -219,6 +219,50 @@ def apply_q2(refl: list, Z: np.ndarray) -> np.ndarray:
     return X
 
 
+def _chase_steps(refl: list) -> list:
+    """(sweep i, step k) of each reflector of ``hb2st`` in generation order."""
+    out, seen = [], {}
+    for (i, _lo, _v, _tau) in refl:
+        k = seen.get(i, 0)
+        seen[i] = k + 1
+        out.append((i, k))
+    return out
+
+
+def apply_q2_blocked(refl: list, Z: np.ndarray, m: int) -> np.ndarray:
+    """``apply_q2`` as block reflectors (the GEMM form of the chase back-transform).
+
+    Reflector (i, k) acts on rows [i+1+kb, i+1+(k+1)b); it overlaps (i+1, k)
+    (b-1 rows) and (i, k+1) overlaps (i+1, k) (one row), every other pair is
+    disjoint.  Applying by step k ascending, and within a step by sweep
+    descending, therefore gives exactly Q2 Z, and in that order the
+    reflectors of m consecutive sweeps at one step are adjacent: rows
+    [lo_min, lo_max + b), a (b + m - 1) x m lower-trapezoidal V with
+    T = ZLARFT(V, taus), applied as Z -= V (T (V^H Z)).
+    """
+    X = np.array(Z, dtype=np.complex128)
+    steps = _chase_steps(refl)
+    by_step: dict = {}
+    for idx in sorted(range(len(refl)), key=lambda j: (steps[j][1], -steps[j][0])):
+        by_step.setdefault(steps[idx][1], []).append(idx)
+    for k in sorted(by_step):
+        lst = by_step[k]
+        for g0 in range(0, len(lst), m):
+            grp = lst[g0:g0 + m]  # applied first to last
+            r0 = min(refl[j][1] for j in grp)
+            r1 = max(refl[j][1] + len(refl[j][2]) for j in grp)
+            fac = grp[::-1]       # Q = H_fac[0] ... H_fac[-1] = I - V T V^H
+            V = np.zeros((r1 - r0, len(fac)), dtype=np.complex128)
+            taus = np.zeros(len(fac), dtype=np.complex128)
+            for c, j in enumerate(fac):
+                _i, lo, v, tau = refl[j]
+                V[lo - r0:lo - r0 + len(v), c] = v
+                taus[c] = tau
+            T = larft(V, taus)
+            X[r0:r1] -= V @ (T @ (V.conj().T @ X[r0:r1]))
+    return X
+
+
 def two_stage(C: np.ndarray, b: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
     """d, e and Q (= Q1 Q2 diag(phase)) with Q^H C Q = tridiag(d, e)."""
     B, Q1, _ = he2hb(C, b)

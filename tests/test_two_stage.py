@@ -166,3 +166,14 @@ def test_chase_task_on_band_storage_matches_dense_chase(tmp_path, n, b):
         assert np.abs(rec[pos + 3:pos + 3 + ln] - v).max() < 1e-10
         pos += 3 + ln
     assert pos == len(rec)
+
+
+@pytest.mark.parametrize("n,b,m", [(60, 4, 4), (97, 8, 8), (150, 16, 8), (130, 32, 16), (40, 8, 1)])
+def test_chase_back_transform_in_blocks(n, b, m):
+    """Step-ascending, sweep-descending order with m sweeps per block reflector
+    reproduces Q2 Z of the chase reflectors."""
+    rng = np.random.default_rng(n + b + m)
+    B, _, _ = ts.he2hb(_herm(n, rng), b)
+    _, _, _, refl = ts.hb2st(B, b)
+    Z = rng.standard_normal((n, 11)) + 1j * rng.standard_normal((n, 11))
+    assert np.abs(ts.apply_q2_blocked(refl, Z, m) - ts.apply_q2(refl, Z)).max() < 1e-13
