@@ -51,13 +51,16 @@ def cores_used():
 # CPU: the reference algorithm (oracle port) timed on the host cores
 # ---------------------------------------------------------------------------
 
-def time_cpu_reference(p, steps: int, warmup: int, min_seconds: float = 0.0, keep_first=False):
+def time_cpu_reference(p, steps: int, warmup: int, min_seconds: float = 0.0, keep_first=False,
+                       lwork: int = 0):
+    """Seconds per k-point of the oracle (match + setup + ZHEGVX); ``lwork`` 0 is the
+    reference's 2n, -1 LAPACK's optimal workspace."""
     from oracle import fvref
     st = p.static
     times = []
     first = None
     for i in range(warmup):
-        w, X, info = fvref.seceqn(st, p.kpts[i % len(p.kpts)])
+        w, X, info = fvref.seceqn(st, p.kpts[i % len(p.kpts)], lwork=lwork)
         if i == 0:
             first = w
     t_all = time.perf_counter()
@@ -65,7 +68,7 @@ def time_cpu_reference(p, steps: int, warmup: int, min_seconds: float = 0.0, kee
     while i < steps or (time.perf_counter() - t_all) < min_seconds:
         kp = p.kpts[i % len(p.kpts)]
         t0 = time.perf_counter()
-        w, X, info = fvref.seceqn(st, kp)
+        w, X, info = fvref.seceqn(st, kp, lwork=lwork)
         times.append(time.perf_counter() - t0)
         if first is None:
             first = w
@@ -432,7 +435,6 @@ def main():
         torch.cuda.synchronize()
         clocks = ClockSampler(local_rank)
         clocks.start()
-        fv.profile(True)
         l0 = fv.launch_count()
         evs = []
         for _ in range(args.steps):
@@ -445,9 +447,18 @@ def main():
         fv.sync(n)
         torch.cuda.synchronize()
         launches = fv.launch_count() - l0
+        clk = clocks.stop()
+        # stage breakdown and per-kernel-class durations (the roofline's
+        # launch times): the same steps once more with the library's CUDA
+        # events on, outside the timed region that gives ``value``
+        fv.profile(True)
+        for _ in range(args.steps):
+            flush.zero_()
+            step_dev()
+        fv.sync(n)
+        torch.cuda.synchronize()
         prof = fv.profile_read()
         fv.profile(False)
-        clk = clocks.stop()
     total_ms = sum(s.elapsed_time(e) for s, e in evs)
     t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
     if world > 1:
@@ -595,12 +606,19 @@ def main():
 
     # ---- CPU baseline (rank 0, N = 1); its first k-point is the timed one ----
     cpu = None
+    cpu_opt = None
     oracle_err = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         pc = syn.make_problem(args.workload, nk=1)
         times, w_or = time_cpu_reference(pc, 2, 1, min_seconds=10.0, keep_first=True)
         cpu = {"value": len(times) / sum(times), "unit": UNIT, "cores": cores_used(), "kind": "port",
                "sample": f"{len(times)} k-points of {args.workload} (NumPy + OpenBLAS ZHEGVX lwork=2n)"}
+        # the same with LAPACK's optimal workspace (blocked ZHETRD instead of
+        # the unblocked ZHETD2 that the reference's lwork = 2n forces)
+        t_opt = time_cpu_reference(pc, 2, 1, min_seconds=5.0, lwork=-1)
+        cpu_opt = {"value": len(t_opt) / sum(t_opt), "unit": UNIT, "cores": cores_used(), "kind": "port",
+                   "sample": f"{len(t_opt)} k-points of {args.workload} (NumPy + OpenBLAS ZHEGVX, "
+                             "optimal lwork from a workspace query)"}
         oracle_err = {"fp64": float(np.abs(ev_host - w_or).max()),
                       "mixed": float(np.abs(wm_host - w_or).max()),
                       "note": "max |eigenvalue - oracle ZHEGVX| over the lowest nstfv states, Ha"}
@@ -610,8 +628,9 @@ def main():
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator of the named shape)",
+        "eig_err_vs_oracle": oracle_err,
+        "mixed_single_k": mixed_single,
         "config": {"workload": workload_desc(args.workload, p), "form": "plain FP64",
-                   "mixed_single_k": mixed_single, "eig_err_vs_oracle": oracle_err,
                    "l2": "flushed between steps (512 MB write, outside the timed events)",
                    "parallelism": f"k-points over {world} GPU(s), no data-path collective",
                    "stage_ms_per_step": stages, "fp64_tensor_peak_tflops": zpeak,
@@ -619,6 +638,7 @@ def main():
                    "lowest_eigenvalues": [float(x) for x in ev_host[:3]]},
         "roofline": roof,
         "cpu_baseline": cpu,
+        "cpu_baseline_optimal_lwork": cpu_opt,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),

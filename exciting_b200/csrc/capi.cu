@@ -77,6 +77,11 @@ double now_s() {
 static std::atomic<long long> g_launches{0};
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+static std::atomic<long long> g_wait_ns{2000000000LL};
+static std::atomic<int> g_planted{0};
+long long wait_limit_ns() { return g_wait_ns.load(std::memory_order_relaxed); }
+bool take_planted_stall() { return g_planted.exchange(0) != 0; }
+
 void prof_begin(excfv_handle* h, int cls) {
   Prof& p = h->prof;
   if (!p.on) return;
@@ -685,6 +690,14 @@ int excfv_sync(excfv_handle* h) {
 }
 
 long long excfv_launch_count(void) { return g_launches.load(); }
+
+int excfv_test_set_wait_limit(int64_t limit_ns, int32_t plant_stall) {
+  if (limit_ns <= 0) limit_ns = 2000000000LL;
+  if (limit_ns < 100000LL) limit_ns = 100000LL;  // at least 0.1 ms
+  g_wait_ns.store(limit_ns);
+  g_planted.store(plant_stall ? 1 : 0);
+  return EXCFV_OK;
+}
 
 // ---------------------------------------------------------------------------
 // batched k-points: lanes

@@ -52,6 +52,12 @@ enum { ST_POTRF = 0, ST_BARRIER = 1, ST_STEIN = 2, ST_STEBZ = 3, ST_REFINE = 4, 
   } while (0)
 
 void excfv_set_error(const char* fmt, ...);
+// Time limit of every bounded spin-wait in the kernels (default 2 s) and a
+// one-shot planted stall: when armed, the next reduction's first wait gets a
+// target that nothing reaches, so the limit runs out (a test aid; see
+// excfv_test_set_wait_limit in include/excfv.h).
+long long wait_limit_ns();
+bool take_planted_stall();
 // process-wide count of kernel launches made by this library
 void count_launch(int n = 1);
 

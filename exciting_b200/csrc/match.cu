@@ -16,215 +16,11 @@
 #include <mutex>
 
 #include "handle.cuh"
+#include "specfun.cuh"
 
 namespace {
 
-constexpr int LMAX_CAP = 20;   // largest lmaxapw supported by the device path
-constexpr int MAXM = 6;        // highest Bessel derivative (sbesseldm limit)
-
-// ---- special functions ------------------------------------------------------
-
-// Y_lm(theta, phi), l <= lmax, packed lm = l(l+1)+m; Masters & Richards-Dinger
-// recursion with the Condon-Shortley phase (src/src_lib/genylm.f90).
-__device__ void d_genylm(int lmax, double theta, double phi, cplx* ylm, int stride) {
-  ylm[0] = cmk(0.28209479177387814347, 0.0);
-  if (lmax == 0) return;
-  const double sn = sin(theta), cs = cos(theta);
-  double x[LMAX_CAP + 1];
-  for (int l = 1; l <= lmax; ++l) {
-    x[l] = (l % 2 == 0) ? 1.0 : -1.0;
-    double dx = 0.0;
-    for (int m = l; m >= 1; --m) {
-      const double t = sqrt((double)((l + m) * (l - m + 1)));
-      x[m - 1] = -(sn * dx + 2.0 * m * cs * x[m]) / t;
-      dx = sn * x[m] * t;
-    }
-    double sc = sn, acc = 0.0;
-    for (int m = 1; m <= l; ++m) {
-      x[m] *= sc;
-      acc += x[m] * x[m];
-      sc *= sn;
-    }
-    acc = 2.0 * acc + x[0] * x[0];
-    const double nrm = sqrt((2 * l + 1) / (4.0 * M_PI * acc));
-    const int c = l * (l + 1);
-    ylm[c * stride] = cmk(nrm * x[0], 0.0);
-    for (int m = 1; m <= l; ++m) {
-      double sp, cp;
-      sincos(m * phi, &sp, &cp);
-      const cplx v = cmk(nrm * x[m] * cp, nrm * x[m] * sp);
-      ylm[(c + m) * stride] = v;
-      const double sg = (m & 1) ? -1.0 : 1.0;
-      ylm[(c - m) * stride] = cmk(sg * v.x, -sg * v.y);
-    }
-  }
-}
-
-// j_l(x), l = 0..lmax (src/src_lib/sbessel.f90): series for x < 1e-8,
-// Miller's downward recurrence with rescaling for x < lmax, upward otherwise.
-__device__ void d_sbessel(int lmax, double x, double* jl) {
-  if (x < 1e-8) {
-    jl[0] = 1.0;
-    double t1 = 1.0, t2 = 1.0;
-    for (int l = 1; l <= lmax; ++l) {
-      t1 /= (2 * l + 1);
-      t2 *= x;
-      jl[l] = t2 * t1;
-    }
-    return;
-  }
-  const double xi = 1.0 / x;
-  if (x < (double)lmax) {
-    const double rsc = 1e150, rsci = 1e-150;
-    double j0 = 0.6370354636449841609 * rsci, j1 = 0.3532702964695481204 * rsci, jt;
-    for (int l = lmax + 25; l > lmax; --l) {
-      jt = j0 * (2 * l + 1) * xi - j1;
-      j1 = j0;
-      j0 = jt;
-      if (fabs(j0) > rsc) { j1 *= rsci; j0 *= rsci; }
-    }
-    for (int l = lmax; l >= 0; --l) {
-      jt = j0 * (2 * l + 1) * xi - j1;
-      j1 = j0;
-      j0 = jt;
-      if (fabs(j0) > rsc) {
-        j1 *= rsci;
-        j0 *= rsci;
-        for (int q = l + 1; q <= lmax; ++q) jl[q] *= rsci;
-      }
-      jl[l] = j1;
-    }
-    double s, c;
-    sincos(x, &s, &c);
-    const double t1 = 1.0 / ((jl[0] - x * jl[1]) * c + x * jl[0] * s);
-    for (int l = 0; l <= lmax; ++l) jl[l] *= t1;
-    return;
-  }
-  double s, c;
-  sincos(x, &s, &c);
-  jl[0] = s * xi;
-  if (lmax == 0) return;
-  jl[1] = (jl[0] - c) * xi;
-  double j0 = jl[0], j1 = jl[1];
-  for (int l = 2; l <= lmax; ++l) {
-    const double jt = (2 * l - 1) * j1 * xi - j0;
-    j0 = j1;
-    j1 = jt;
-    jl[l] = j1;
-  }
-}
-
-// m-th derivative of j_l(x), l = 0..lmax (src/src_lib/sbesseldm.f90).  For
-// x > 1: d^m j_l = sum_i (a_i j_l + b_i j_{l+1}) / x^i with integer a, b from
-// repeated use of j_l' = (l/x) j_l - j_{l+1}, j_{l+1}' = j_l - ((l+2)/x) j_{l+1}.
-// For x <= 1: the power series.
-__device__ void d_sbesseldm(int m, int lmax, double x, double* djl) {
-  double jl[LMAX_CAP + 2];
-  if (m == 0) { d_sbessel(lmax, x, djl); return; }
-  if (x > 1.0) {
-    d_sbessel(lmax + 1, x, jl);
-    for (int l = 0; l <= lmax; ++l) {
-      long long a[MAXM + 2], b[MAXM + 2], na[MAXM + 2], nb[MAXM + 2];
-      for (int i = 0; i < MAXM + 2; ++i) { a[i] = 0; b[i] = 0; }
-      a[0] = 1;
-      for (int it = 0; it < m; ++it) {
-        for (int i = 0; i < MAXM + 2; ++i) { na[i] = 0; nb[i] = 0; }
-        for (int i = 0; i <= m; ++i) {
-          if (a[i]) { na[i + 1] += a[i] * (l - i); nb[i] -= a[i]; }
-          if (b[i]) { na[i] += b[i]; nb[i + 1] -= b[i] * (l + 2 + i); }
-        }
-        for (int i = 0; i < MAXM + 2; ++i) { a[i] = na[i]; b[i] = nb[i]; }
-      }
-      double acc = (double)a[0] * jl[l] + (double)b[0] * jl[l + 1];
-      double t = 1.0;
-      for (int i = 1; i <= m + 1; ++i) {
-        t *= x;
-        acc += ((double)a[i] * jl[l] + (double)b[i] * jl[l + 1]) / t;
-      }
-      djl[l] = acc;
-    }
-    return;
-  }
-  const double x2 = x * x;
-  for (int l = 0; l <= lmax; ++l) {
-    const int i0 = max((m - l + 1) / 2, 0);
-    const int j = 2 * i0 + l - m;
-    double t = (j == 0) ? 1.0 : pow(x, (double)j);
-    double num = 1.0;  // (j+m)!/j!
-    for (int q = j + 1; q <= j + m; ++q) num *= q;
-    double den = 1.0;  // i0! (2 i0 + 2 l + 1)!! (-2)^i0
-    for (int q = 2; q <= i0; ++q) den *= q;
-    for (int q = 2 * i0 + 2 * l + 1; q > 0; q -= 2) den *= q;
-    for (int q = 0; q < i0; ++q) den *= -2.0;
-    t = num * t / den;
-    double acc = t;
-    for (int i = i0 + 1; i <= 20; ++i) {
-      const int jj = 2 * i + l;
-      t = -t * (double)((jj - 1) * jj) * x2 / (double)((jj - l) * (jj - m - 1) * (jj - m) * (jj + l + 1));
-      if (fabs(t) <= 1e-40) break;
-      acc += t;
-    }
-    djl[l] = acc;
-  }
-}
-
-// m-th derivative at x of the polynomial through np points
-// (src/src_lib/polynom.f90; closed forms for np <= 4, Newton form otherwise).
-__device__ double d_polynom(int m, int np, const double* xa, const double* ya, double x) {
-  if (m >= np) return 0.0;
-  if (np == 1) return m == 0 ? ya[0] : 0.0;
-  if (np == 2) {
-    const double c2 = (ya[1] - ya[0]) / (xa[1] - xa[0]);
-    return m == 0 ? c2 * (x - xa[0]) + ya[0] : c2;
-  }
-  if (np == 3) {
-    const double x1 = xa[1] - xa[0], x2 = xa[2] - xa[0];
-    const double y1 = ya[1] - ya[0], y2 = ya[2] - ya[0];
-    double t1 = 1.0 / (x1 * x2 * (x2 - x1));
-    const double t2 = x1 * y2, t3 = x2 * y1;
-    const double c2 = t1 * (x2 * t3 - x1 * t2), c3 = t1 * (t2 - t3);
-    t1 = x - xa[0];
-    if (m == 0) return ya[0] + t1 * (c2 + c3 * t1);
-    if (m == 1) return 2.0 * c3 * t1 + c2;
-    return 2.0 * c3;
-  }
-  if (np == 4) {
-    const double x1 = xa[1] - xa[0], x2 = xa[2] - xa[0], x3 = xa[3] - xa[0];
-    const double y1 = ya[1] - ya[0], y2 = ya[2] - ya[0], y3 = ya[3] - ya[0];
-    double t1 = 1.0 / (x1 * x2 * x3 * (x1 - x2) * (x1 - x3) * (x2 - x3));
-    const double t2 = x1 * x2 * y3, t3 = x2 * x3 * y1, t4 = x3 * x1 * y2;
-    const double t5 = x1 * x1, t6 = x2 * x2, t7 = x3 * x3;
-    const double c2 = t1 * (t3 * (x3 * t6 - x2 * t7) + t4 * (x1 * t7 - x3 * t5) + t2 * (x2 * t5 - x1 * t6));
-    const double c3 = t1 * (t3 * (t7 - t6) + t4 * (t5 - t7) + t2 * (t6 - t5));
-    const double c4 = t1 * (t3 * (x2 - x3) + t4 * (x3 - x1) + t2 * (x1 - x2));
-    t1 = x - xa[0];
-    if (m == 0) return ya[0] + t1 * (c2 + t1 * (c3 + c4 * t1));
-    if (m == 1) return c2 + t1 * (2.0 * c3 + 3.0 * c4 * t1);
-    if (m == 2) return 6.0 * c4 * t1 + 2.0 * c3;
-    return 6.0 * c4;
-  }
-  double c[16];
-  for (int i = 0; i < np; ++i) c[i] = ya[i];
-  for (int i = 1; i < np; ++i)
-    for (int j = np - 1; j >= i; --j) c[j] = (c[j] - c[j - 1]) / (xa[j] - xa[j - i]);
-  if (m == 0) {
-    double acc = c[0], t = 1.0;
-    for (int i = 1; i < np; ++i) { t *= (x - xa[i - 1]); acc += c[i] * t; }
-    return acc;
-  }
-  const double x0 = xa[0];
-  for (int j = 1; j < np; ++j)
-    for (int i = 1; i <= np - j; ++i) {
-      const int k = np - i;
-      c[k - 1] += (x0 - xa[k - j]) * c[k];
-    }
-  for (int j = 1; j <= m; ++j)
-    for (int i = m; i < np; ++i) c[i] *= (double)(i - j + 1);
-  double t1 = c[np - 1];
-  const double t2 = x - x0;
-  for (int i = np - 2; i >= m; --i) t1 = t1 * t2 + c[i];
-  return t1;
-}
+constexpr int LMAX_CAP = SPECFUN_LMAX;  // largest lmaxapw supported by the device path
 
 // ---- kernels --------------------------------------------------------------
 
@@ -242,7 +38,7 @@ __global__ void k_zdinv(int natmtot, int lmaxapw, int apwordmax, int np, const i
   for (int i = 0; i < nap; ++i)
     for (int j = 0; j < nap; ++j) {
       const double* ya = apwfrwin + (size_t)np * (j + apwordmax * (l + (lmaxapw + 1) * (size_t)ias));
-      zd[i][j] = d_polynom(i, np, sprwin + (size_t)np * is, ya, rmt[is]);
+      zd[i][j] = sf_polynom_deriv(i, np, sprwin + (size_t)np * is, ya, rmt[is]);
       inv[i][j] = (i == j) ? 1.0 : 0.0;
     }
   for (int c = 0; c < nap; ++c) {
@@ -276,7 +72,7 @@ __global__ void k_ylm_bessel(int ngp, int ngkmax, int lmax, int apwordmax, int n
   const int ig = blockIdx.x * blockDim.x + threadIdx.x;
   if (ig >= ngp) return;
   const int lmmax = (lmax + 1) * (lmax + 1);
-  d_genylm(lmax, tpgpc[2 * ig], tpgpc[2 * ig + 1], ylm + (size_t)ig * lmmax, 1);
+  sf_ylm(lmax, tpgpc[2 * ig], tpgpc[2 * ig + 1], ylm + (size_t)ig * lmmax, 1);
   const double g = gpc[ig];
   double buf[LMAX_CAP + 1];
   for (int is = 0; is < nspecies; ++is) {
@@ -285,7 +81,7 @@ __global__ void k_ylm_bessel(int ngp, int ngkmax, int lmax, int apwordmax, int n
     const double x = g * rmt[is];
     double sc = 1.0;
     for (int j = 0; j < omax; ++j) {
-      d_sbesseldm(j, lmax, x, buf);
+      sf_sbessel_deriv(j, lmax, x, buf);
       for (int l = 0; l <= lmax; ++l)
         djl[(((size_t)is * ngkmax + ig) * (lmax + 1) + l) * apwordmax + j] = sc * buf[l];
       sc *= g;

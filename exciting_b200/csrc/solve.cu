@@ -114,6 +114,12 @@ struct RRScratch {
 
 __device__ __forceinline__ double cabsd(cplx a) { return hypot(a.x, a.y); }
 
+// Sort key of a total order on doubles: NaN ranks as +inf, ties go by index,
+// so ranks computed by counting form a permutation whatever the values (a
+// failed earlier stage may leave NaN here; the indices derived from the ranks
+// must stay in range).
+__device__ __forceinline__ double rank_key(double v) { return isnan(v) ? INFINITY : v; }
+
 __device__ __forceinline__ double block_max(double v, double* red) {
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -136,7 +142,7 @@ __global__ void __launch_bounds__(1024) k_rr_clusters(int kx, const cplx* __rest
   const int tid = threadIdx.x;
   double emax = 0.0, dmax = 0.0;
   for (int i = tid; i < kx; i += blockDim.x) {
-    const double d = Hk[i + (long long)kx * i].x;
+    const double d = rank_key(Hk[i + (long long)kx * i].x);
     s.D[i] = d;
     dmax = fmax(dmax, fabs(d));
   }
@@ -304,10 +310,10 @@ __global__ void k_rr_perturb(int kx, const cplx* __restrict__ Hp, RRScratch s, c
 // One CTA: the k lowest refined eigenvalues (ascending) and their states.
 __global__ void __launch_bounds__(1024) k_rr_select(int kx, int k, RRScratch s, double* w) {
   for (int a = threadIdx.x; a < kx; a += blockDim.x) {
-    const double la = s.lam[a];
+    const double la = rank_key(s.lam[a]);
     int r = 0;
     for (int b = 0; b < kx; ++b) {
-      const double lb = s.lam[b];
+      const double lb = rank_key(s.lam[b]);
       r += (lb < la) || (lb == la && b < a);
     }
     if (r < k) {

@@ -41,7 +41,6 @@ constexpr int TT = 256;
 constexpr int RCH = 64;
 constexpr int MAXCH = 2;   // row chunks per CTA held in shared memory (FP64 storage)
 constexpr int MAXCH_C64 = 3;  // complex64 storage: up to three, for more concurrent lanes
-constexpr long long BARRIER_NS = 2000000000LL;  // 2 s
 
 // Storage type T2 of C, V and W: double2 (FP64 form) or float2 (the precision
 // form's complex64 copy).  Arithmetic is FP64 in both.
@@ -117,16 +116,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait for a TMA tile; gives up (status[ST_BARRIER] set) after 2 s or
-// as soon as another wait of the launch has given up.
-__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, int* status) {
+// Bounded wait for a TMA tile; gives up (status[ST_BARRIER] set) after
+// limit_ns or as soon as another wait of the launch has given up.
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, int* status,
+                                          long long limit_ns) {
   if (mbar_try_wait(bar, parity)) return;
   const long long t0 = gtimer();
   unsigned it = 0;
   while (!mbar_try_wait(bar, parity)) {
     if ((++it & 63u) == 0) {
       if (*(volatile int*)&status[ST_BARRIER] != 0) return;
-      if (gtimer() - t0 > BARRIER_NS) {
+      if (gtimer() - t0 > limit_ns) {
         atomicAdd(&status[ST_BARRIER], 1);
         return;
       }
@@ -134,20 +134,36 @@ __device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, int* s
   }
 }
 // Bounded wait that reports whether the phase completed.
-__device__ __forceinline__ bool mbar_wait_ok(uint64_t* bar, unsigned parity, int* status) {
+__device__ __forceinline__ bool mbar_wait_ok(uint64_t* bar, unsigned parity, int* status,
+                                             long long limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = gtimer();
   unsigned it = 0;
   while (!mbar_try_wait(bar, parity)) {
     if ((++it & 63u) == 0) {
       if (*(volatile int*)&status[ST_BARRIER] != 0) return false;
-      if (gtimer() - t0 > BARRIER_NS) {
+      if (gtimer() - t0 > limit_ns) {
         atomicAdd(&status[ST_BARRIER], 1);
         return false;
       }
     }
   }
   return true;
+}
+// Before the producer leaves the kernel: every TMA copy it issued has landed
+// (q copies issued round-robin over the slots), so no copy writes into the
+// shared memory of a finished block.  Bounded by limit_ns per slot; this wait
+// ignores the status word, since the copies land whether or not a wait of the
+// launch gave up.
+template <int STAGES>
+__device__ __forceinline__ void drain_copies(uint64_t* full, unsigned q, long long limit_ns) {
+  for (unsigned s = 0; s < (unsigned)STAGES && s < q; ++s) {
+    const unsigned uses = q / STAGES + (s < q % STAGES ? 1u : 0u);
+    const unsigned parity = (uses - 1u) & 1u;
+    const long long t0 = gtimer();
+    while (!mbar_try_wait(&full[s], parity))
+      if (gtimer() - t0 > limit_ns) break;
+  }
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -167,15 +183,17 @@ __device__ __forceinline__ void tma_tile(void* dst, const CUtensorMap* tm, int x
 }
 
 // Grid barrier on a monotonic arrival counter (zeroed before each launch):
-// barrier number e completes when the counter reaches e * gridDim.x.
+// barrier number e completes when the counter reaches e * gridDim.x (plus
+// `planted`, nonzero only when a test arms a target nothing reaches).
 // Returns false when it timed out (here or in another CTA).
-__device__ bool grid_barrier(unsigned* bar, unsigned& epoch, int* status) {
+__device__ bool grid_barrier(unsigned* bar, unsigned& epoch, int* status, long long limit_ns,
+                             unsigned planted = 0) {
   __shared__ int s_ok;
   csync();
   if (threadIdx.x == 0) {
     int ok = 1;
     epoch += 1;
-    const unsigned target = epoch * gridDim.x;
+    const unsigned target = epoch * gridDim.x + planted;
     // release this CTA's writes and arrive (no return value needed)
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
     if (ld_acquire(&bar[0]) < target) {
@@ -183,7 +201,7 @@ __device__ bool grid_barrier(unsigned* bar, unsigned& epoch, int* status) {
       unsigned it = 0;
       while (ld_acquire(&bar[0]) < target) {
         if ((++it & 255u) == 0) {
-          if (*(volatile int*)&status[ST_BARRIER] != 0 || gtimer() - t0 > BARRIER_NS) {
+          if (*(volatile int*)&status[ST_BARRIER] != 0 || gtimer() - t0 > limit_ns) {
             atomicAdd(&status[ST_BARRIER], 1);
             ok = 0;
             break;
@@ -213,6 +231,8 @@ struct TridArgs {
   unsigned* bar;
   int* status;
   int p, nbp, final_panel;
+  long long wait_ns;  // limit of every bounded wait
+  unsigned planted;   // extra arrivals the first barrier waits for (0; a test aid)
 };
 
 __device__ __forceinline__ cplx shfl4_sum(cplx v) {
@@ -344,14 +364,17 @@ __global__ void __launch_bounds__(TT + 32, 1)
           for (int b = 0; b < ntile; ++b, ++q) {
             const unsigned slot = q % R::STAGES;
             if (q >= (unsigned)R::STAGES &&
-                !mbar_wait_ok(&s_empty[slot], ((q / R::STAGES) - 1u) & 1u, a.status))
+                !mbar_wait_ok(&s_empty[slot], ((q / R::STAGES) - 1u) & 1u, a.status, a.wait_ns)) {
+              drain_copies<R::STAGES>(s_full, q, a.wait_ns);
               return;
+            }
             mbar_expect_tx(&s_full[slot], R::BYTES);
             tma_tile(ring + (size_t)slot * R::TILE, &tmap, 2 * (rb + I * 64), colb + b * R::BC,
                      &s_full[slot]);
           }
         }
       }
+      drain_copies<R::STAGES>(s_full, q, a.wait_ns);
     }
     return;
   }
@@ -393,7 +416,7 @@ __global__ void __launch_bounds__(TT + 32, 1)
     const int c = a.p + i;
     cplx* ycur = a.ybuf + (size_t)(i & 1) * n;
     cplx* ynext = a.ybuf + (size_t)((i + 1) & 1) * n;
-    if (!grid_barrier(a.bar, epoch, a.status)) return;
+    if (!grid_barrier(a.bar, epoch, a.status, a.wait_ns, i == 0 ? a.planted : 0u)) return;
 
     // ================= phase 2: reflector of column c, y = C22 v =================
     // y = C22 v with v(c+1) = 1, v(j) = scale x(j): accumulate C22 x~ (x~(c+1) = 0)
@@ -484,7 +507,7 @@ __global__ void __launch_bounds__(TT + 32, 1)
           for (int z = 0; z < NB; ++z) {
             if (z >= nb) break;
             const unsigned q = gtile + b + z;
-            mbar_wait(&s_full[q % R::STAGES], (q / R::STAGES) & 1u, a.status);
+            mbar_wait(&s_full[q % R::STAGES], (q / R::STAGES) & 1u, a.status, a.wait_ns);
           }
 #pragma unroll
           for (int z = 0; z < NB; ++z) {
@@ -666,7 +689,7 @@ __global__ void __launch_bounds__(TT + 32, 1)
       if (sr != 0.0) atomicAdd(&red_vav[2 * i], sr);
       if (si != 0.0) atomicAdd(&red_vav[2 * i + 1], si);
     }
-    if (!grid_barrier(a.bar, epoch, a.status)) return;
+    if (!grid_barrier(a.bar, epoch, a.status, a.wait_ns)) return;
 
     // ========== phase 3 (finish column c) merged with phase 1 (column c+1) ==========
     const bool upd = (i + 1 < a.nbp) || a.final_panel;  // column c+1 is updated here
@@ -1005,6 +1028,8 @@ static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
   // each panel launch then zeroes the slots of the next
   CUDA_TRY(cudaMemsetAsync(ws.red, 0, sizeof(double) * tridiag_workspace_doubles(), s));
   CUDA_TRY(cudaMemsetAsync(ws.bar, 0, 2 * sizeof(unsigned), s));
+  const long long wait_ns = wait_limit_ns();
+  const unsigned planted = take_planted_stall() ? 1u : 0u;
   for (int p = 0; p < n - 1; p += NBT) {
     const int nbp = min(NBT, n - 1 - p);
     const int final_panel = (p + nbp == n - 1) ? 1 : 0;
@@ -1015,6 +1040,8 @@ static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
     ta.red = ws.red + (size_t)(pi & 1) * RED_DOUBLES;
     ta.red_next = ws.red + (size_t)((pi + 1) & 1) * RED_DOUBLES;
     ta.p = p; ta.nbp = nbp; ta.final_panel = final_panel;
+    ta.wait_ns = wait_ns;
+    ta.planted = (p == 0) ? planted : 0u;
     void* args[] = {&ta, &tmap};
     prof_begin(h, PROF_TRD_PANEL);
     CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_tridiag_panel<T2, MC>, dim3(G), dim3(TT + 32), args,

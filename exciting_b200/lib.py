@@ -80,6 +80,7 @@ SIGNATURES = {
     "excfv_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "excfv_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "excfv_launch_count": (C.c_longlong, []),
+    "excfv_test_set_wait_limit": (C.c_int, [C.c_int64, C.c_int32]),
     "excfv_seceqn_batched_dev": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),

@@ -250,6 +250,18 @@ int excfv_profile_read(excfv_handle* h, double* ms, long long* count, int nclass
 /* Number of kernels this library has launched in the process so far. */
 long long excfv_launch_count(void);
 
+/*
+ * Test aid (no counterpart in the reference): sets the time limit of every
+ * bounded spin-wait in the kernels (grid barriers, TMA tile waits, sweep
+ * progress flags; default 2 s; limit_ns <= 0 restores it) for the whole
+ * process.  plant_stall != 0 arms a one-shot fault on the host side: the next
+ * tridiagonal reduction on any handle gives its first wait a target that no
+ * thread ever reaches, so the wait runs out after limit_ns, every block leaves
+ * the kernel after its in-flight copies have landed, and the call returns
+ * EXCFV_ERR_TIMEOUT with the handle still usable.  Not for production use.
+ */
+int excfv_test_set_wait_limit(int64_t limit_ns, int32_t plant_stall);
+
 /* ---- matching coefficients without device allocation ------------------- */
 
 /* Size of the fixed device array that excfv_match_noalloc uses as scratch. */
@@ -274,8 +286,11 @@ long long excfv_launch_count(void);
  * file-scope device array of EXCFV_NOALLOC_SCRATCH_BYTES (32 MiB) that every
  * GPU loading the library holds until the process exits.  Larger requests
  * are rejected with EXCFV_ERR_ARG and a message.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress); make that
- * first call before any stream capture.  All calls on a device share the
+ * looks up the array's device address (cudaGetSymbolAddress) and keeps it
+ * for the life of the process; make that first call before any stream
+ * capture, and do not use this entry point on a device after
+ * cudaDeviceReset (or any other teardown of its primary context), since the
+ * kept address would then be stale.  All calls on a device share the
  * array, so calls that overlap on the GPU (other streams or handles on the
  * same device) race and must be serialised by the caller. */
 int excfv_match_noalloc(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc,

@@ -247,6 +247,34 @@ def hamiltonandoverlapsetup(st, kp, apwalm) -> Tuple[np.ndarray, np.ndarray]:
     return H, O
 
 
+def setup_sample(st, kp, gsel) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Principal submatrices of H and O on the G+k vectors ``gsel`` and every LO.
+
+    Every entry of H and O depends only on the basis functions of its row and
+    its column: the APW-APW block on apwalm of the two G+k vectors
+    (``hamiltonsetup.f90:75-103``, ``overlapsetup.f90:82-108``), the APW-LO
+    blocks on apwalm of one G+k vector (``hamiltonsetup.f90:131-149``,
+    ``overlapsetup.f90:119-135``), the LO-LO blocks on neither, and the
+    interstitial terms on G_i - G_j and the two G+k vectors
+    (``hmlistln.f90:61-84``, ``olpistln.f90:53-82``).  So the setup of the
+    k-point restricted to ``gsel`` is the principal submatrix of the full one
+    on the rows/columns ``idx`` returned here (the selected APWs, then all
+    LOs), at the cost of a k-point with len(gsel) G+k vectors.
+    """
+    import types
+    gsel = np.asarray(gsel, dtype=np.int64)
+    m = int(gsel.shape[0])
+    sub = types.SimpleNamespace(
+        ngp=m, ngkmax=m, igpig=np.asarray(kp.igpig)[gsel].copy(),
+        vgpc=np.asfortranarray(np.asarray(kp.vgpc)[:, gsel]), gpc=np.asarray(kp.gpc)[gsel].copy(),
+        tpgpc=np.asfortranarray(np.asarray(kp.tpgpc)[:, gsel]),
+        sfacgp=np.asfortranarray(np.asarray(kp.sfacgp)[gsel, :]))
+    A = match(st, sub)
+    H, O = hamiltonandoverlapsetup(st, sub, A)
+    idx = np.concatenate([gsel, kp.ngp + np.arange(st.nlotot)])
+    return H, O, idx
+
+
 # ---------------------------------------------------------------------------
 # eigensolve
 # ---------------------------------------------------------------------------
@@ -256,10 +284,14 @@ def solvewithlapack(H: np.ndarray, O: np.ndarray, nstfv: int, evaltol: float,
     """ZHEGVX(1,'V','I','U', n, H, n, O, n, vl, vu, 1, nstfv, evaltol, ..., lwork=2n).
 
     Returns (evalfv, evecfv(n, nstfv), info).  ``lwork`` 0 means the
-    reference's minimum workspace 2n (``modfvsystem.f90:691-693``).
+    reference's minimum workspace 2n (``modfvsystem.f90:691-693``); -1 asks
+    LAPACK for its optimal workspace (blocked ZHETRD), the fairer CPU line.
     """
     n = H.shape[0]
-    if lwork <= 0:
+    if lwork < 0:
+        opt, qinfo = lapack.zhegvx_lwork(n, uplo="U")
+        lwork = max(2 * n, int(np.real(opt))) if qinfo == 0 else 2 * n
+    elif lwork == 0:
         lwork = 2 * n
     w, z, m, ifail, info = lapack.zhegvx(H, O, itype=1, jobz="V", range="I", uplo="U",
                                          il=1, iu=nstfv, abstol=evaltol, lwork=lwork)

@@ -232,10 +232,15 @@ def _chase_steps(refl: list) -> list:
 def apply_q2_blocked(refl: list, Z: np.ndarray, m: int) -> np.ndarray:
     """``apply_q2`` as block reflectors (the GEMM form of the chase back-transform).
 
-    Reflector (i, k) acts on rows [i+1+kb, i+1+(k+1)b); it overlaps (i+1, k)
-    (b-1 rows) and (i, k+1) overlaps (i+1, k) (one row), every other pair is
-    disjoint.  Applying by step k ascending, and within a step by sweep
-    descending, therefore gives exactly Q2 Z, and in that order the
+    Reflector (i, k) acts on rows [i+1+kb, i+1+(k+1)b).  Q2 Z applies the
+    reflectors by sweep descending and, within a sweep, by step descending.
+    The order used here (step k ascending, within a step sweep descending)
+    changes the relative order only of pairs (i, k), (i', k') with i < i' and
+    k < k' (or i = i', k != k'), and those are row-disjoint: reflector (i', k')
+    starts at row i'+1+k'b >= i+1+(k+1)b, where reflector (i, k) ends (within
+    one sweep the steps are b rows apart).  Every overlapping pair, such as
+    (i, k) and (i+j, k) for j < b, keeps its order, so this gives exactly
+    Q2 Z, and in that order the
     reflectors of m consecutive sweeps at one step are adjacent: rows
     [lo_min, lo_max + b), a (b + m - 1) x m lower-trapezoidal V with
     T = ZLARFT(V, taus), applied as Z -= V (T (V^H Z)).

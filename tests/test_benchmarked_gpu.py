@@ -1,0 +1,95 @@
+"""The benchmarked configurations held to the oracle at the size they are timed.
+
+- The batch (64 k-points of the 8-atom cell, nmat uniform in 1800..2300, the
+  seeded set the benchmark times): autotuned lanes, then three identical
+  device-pointer calls (eager; the call that captures the CUDA graph; a graph
+  replay), in both forms.  Eight k-points, the smallest and the largest nmat
+  among them, are solved by the oracle (setup + ZHEGVX): eigenvalues within
+  1e-10 Ha (FP64) and 1e-8 Ha (precision form), eigenvector residuals and
+  O-orthonormality on the same eight, and the three calls' eigenvalues agree.
+- The 64-atom supercell (n = 12012): H and O from the GPU setup are compared
+  on a strided sample of 311 G+k vectors plus all 512 local orbitals with the
+  oracle's setup of that principal submatrix (oracle.fvref.setup_sample).
+"""
+import numpy as np
+import pytest
+import torch
+
+from exciting_b200 import synthetic as syn
+from exciting_b200.fv import FirstVariational
+from exciting_b200.lib import EXCFV_PREC_FP64, EXCFV_PREC_MIXED
+from oracle import fvref
+
+pytestmark = pytest.mark.gpu
+
+NK = 64
+NSUB = 8
+
+
+def _batch_problem():
+    # the benchmark's batch: nmat = ngk + 64 uniform in [1800, 2300]
+    return syn.make_problem("cubic8", nk=NK, ngk_range=(1800 - 64, 2300 - 64))
+
+
+@pytest.fixture(scope="module")
+def batch():
+    p = _batch_problem()
+    nm = np.array([k.nmat for k in p.kpts])
+    rng = np.random.default_rng(20261203)
+    others = [i for i in rng.permutation(NK) if i not in (int(nm.argmin()), int(nm.argmax()))]
+    sub = sorted({int(nm.argmin()), int(nm.argmax()), *others[:NSUB - 2]})
+    refs = {}
+    for i in sub:
+        kp = p.kpts[i]
+        A = fvref.match(p.static, kp)
+        H, O = fvref.hamiltonandoverlapsetup(p.static, kp, A)
+        w, _, info = fvref.solvewithlapack(H, O, p.static.nstfv, p.static.evaltol)
+        assert info == 0
+        refs[i] = (H, O, w)
+    return p, sub, refs
+
+
+@pytest.mark.parametrize("prec,etol,rtol", [(EXCFV_PREC_FP64, 1e-10, 1e-12),
+                                            (EXCFV_PREC_MIXED, 1e-8, 1e-7)], ids=["fp64", "mixed"])
+def test_batch_as_benchmarked(batch, prec, etol, rtol):
+    p, sub, refs = batch
+    st = p.static
+    dev = torch.device("cuda", 0)
+
+    def dv(a, dt):
+        return torch.from_numpy(np.asfortranarray(np.asarray(a, dtype=dt)).ravel(order="F")).to(dev)
+
+    ins = [{n: dv(getattr(k, n), dt) for n, dt in (("gpc", np.float64), ("tpgpc", np.float64),
+                                                   ("sfacgp", np.complex128), ("igpig", np.int32),
+                                                   ("vgpc", np.float64))} for k in p.kpts]
+    ev = [torch.zeros(st.nstfv, dtype=torch.float64, device=dev) for _ in p.kpts]
+    X = [torch.zeros(p.nmatmax * st.nstfv, dtype=torch.complex128, device=dev) for _ in p.kpts]
+    bargs = ([k.nmat for k in p.kpts], [k.ngp for k in p.kpts], p.ngkmax,
+             [d["gpc"].data_ptr() for d in ins], [d["tpgpc"].data_ptr() for d in ins],
+             [d["sfacgp"].data_ptr() for d in ins], [d["igpig"].data_ptr() for d in ins],
+             [d["vgpc"].data_ptr() for d in ins], p.nmatmax,
+             [e.data_ptr() for e in ev], [x.data_ptr() for x in X])
+    calls = []
+    with FirstVariational(0, precision=prec) as fv:
+        fv.set_static(st)
+        fv.autotune_lanes(*bargs)
+        assert fv.lanes() >= 1
+        for _ in range(3):                    # eager, capture, replay
+            for x in X:
+                x.zero_()
+            fv.seceqn_batched_dev(*bargs)
+            fv.sync()
+            torch.cuda.synchronize()
+            assert np.all(fv.batch_info(NK) == 0)
+            calls.append(np.array([e.cpu().numpy() for e in ev]))
+    for w in calls[1:]:
+        assert np.abs(w - calls[0]).max() < (1e-12 if prec == EXCFV_PREC_FP64 else 1e-9)
+    for i in sub:
+        H, O, w_ref = refs[i]
+        n = p.kpts[i].nmat
+        w = calls[-1][i]
+        assert np.abs(w - w_ref).max() < etol, f"k-point {i} (nmat {n})"
+        Xi = X[i].view(st.nstfv, p.nmatmax).T.cpu().numpy()[:n]
+        assert np.all(X[i].view(st.nstfv, p.nmatmax).T[n:].abs().cpu().numpy() == 0)
+        assert fvref.residuals(H, O, w, Xi).max() < rtol
+        assert fvref.o_orthonormality(O, Xi) < 1e-11

@@ -3,9 +3,12 @@
 - cell16 (16 atoms, two species, n = 5028, lowest 400 states): FP64 and the
   precision form against the oracle's ZHEGVX (a CPU solve of ~30 s).
 - super64 (64 atoms, n = 12012, lowest 1000 states, 2.3 GB per matrix): no
-  CPU solve at this size; the check is through size-independent properties
-  evaluated on the GPU with torch: residuals ||Hx - eOx|| / (||H|| ||x||),
-  O-orthonormality, and the agreement of the two forms' eigenvalues.
+  CPU solve at this size; the setup is held to the oracle on a strided sample
+  (the principal submatrix on every 37th G+k vector and all local orbitals,
+  oracle.fvref.setup_sample), the eigensolve through size-independent
+  properties evaluated on the GPU with torch: residuals
+  ||Hx - eOx|| / (||H|| ||x||), O-orthonormality, and the agreement of the two
+  forms' eigenvalues.
 """
 import numpy as np
 import pytest
@@ -53,6 +56,13 @@ def test_super64_properties():
     wm, Xm = _solve(EXCFV_PREC_MIXED, st, kp)
     assert np.all(np.diff(w64) >= 0)
     assert np.abs(wm - w64).max() < 1e-8
+    # the GPU setup on a strided sample of G+k vectors (and every local
+    # orbital) against the oracle's setup of that principal submatrix
+    gsel = np.arange(0, kp.ngp, 37)
+    Hs, Os, idx = fvref.setup_sample(st, kp, gsel)
+    ix = np.ix_(idx, idx)
+    assert np.abs(H[ix] - Hs).max() < 1e-13 * np.abs(Hs).max()
+    assert np.abs(O[ix] - Os).max() < 1e-13 * np.abs(Os).max()
     dev = torch.device("cuda", 0)
     Hd = torch.from_numpy(H).to(dev)
     Od = torch.from_numpy(O).to(dev)

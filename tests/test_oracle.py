@@ -240,3 +240,19 @@ def test_workload_shapes():
     b = syn.make_problem("diamond2")
     assert np.array_equal(a.static.aa, b.static.aa)
     assert np.array_equal(a.kpts[0].sfacgp, b.kpts[0].sfacgp)
+
+
+def test_setup_sample_is_a_principal_submatrix():
+    """fvref.setup_sample (used to hold the 12012-dimensional setup to the
+    oracle on a strided sample) equals the full setup restricted to its rows."""
+    from exciting_b200 import synthetic as syn
+    for name, kw in (("diamond2", {}), ("cubic8", dict(ngk=300, nstfv=20, complex_aa=True))):
+        p = syn.make_problem(name, **kw)
+        st, kp = p.static, p.kpts[0]
+        A = fvref.match(st, kp)
+        H, O = fvref.hamiltonandoverlapsetup(st, kp, A)
+        gsel = np.arange(5, kp.ngp, 11)
+        Hs, Os, idx = fvref.setup_sample(st, kp, gsel)
+        scale = np.abs(H).max()
+        assert np.abs(H[np.ix_(idx, idx)] - Hs).max() < 1e-13 * scale
+        assert np.abs(O[np.ix_(idx, idx)] - Os).max() < 1e-13 * np.abs(O).max()

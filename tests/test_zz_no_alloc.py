@@ -7,7 +7,10 @@ not pay the device-wide synchronisation cudaMalloc/cudaFree can impose.  Its
 scratch is one fixed device array shared by every call, so the test makes two
 calls in a row on k-points of different size (the second reuses memory the
 first wrote) and compares each result with excfv_match, within the tolerance
-of the other matching-coefficient parity tests.
+of the other matching-coefficient parity tests.  Around the second call the
+device's free memory (cudaMemGetInfo through torch) must not change: the first
+call has loaded the module and looked up the array's address, so nothing is
+left that could allocate.
 
 The file name sorts last, so a run that stops at the first failure has run
 every other test before this one.
@@ -44,8 +47,12 @@ def test_match_noalloc_two_calls_match_excfv_match():
             sf = _dev(kp.sfacgp, np.complex128)
             out = torch.full((ref.size,), complex(np.nan, np.nan), dtype=torch.complex128, device="cuda:0")
             torch.cuda.synchronize()
+            free0 = torch.cuda.mem_get_info(0)[0]
             fv.match_noalloc(kp.ngp, kp.ngkmax, gpc.data_ptr(), tp.data_ptr(), sf.data_ptr(), out.data_ptr())
             torch.cuda.synchronize()
+            free1 = torch.cuda.mem_get_info(0)[0]
+            if kp is not p.kpts[0]:
+                assert free1 == free0, f"device free memory changed by {free0 - free1} bytes"
             got = out.cpu().numpy().reshape(ref.shape, order="F")
             assert np.all(np.isfinite(got))
             err = np.abs(got - ref).max() / np.abs(ref).max()
