@@ -135,7 +135,7 @@ void free_workspace(Workspace& ws) {
   dfree(ws.tpgpc); dfree(ws.sfacgp); dfree(ws.gk_iv); dfree(ws.d); dfree(ws.e); dfree(ws.tau);
   dfree(ws.Wp); dfree(ws.red); dfree(ws.w); dfree(ws.stein_ws); dfree(ws.icl); dfree(ws.ybuf);
   dfree(ws.Z); dfree(ws.Z2); dfree(ws.Gk); dfree(ws.Gki); dfree(ws.Tf); dfree(ws.Xs);
-  dfree(ws.status); dfree(ws.bar); dfree(ws.part);
+  dfree(ws.status); dfree(ws.bar); dfree(ws.part); dfree(ws.prog);
   ws.part_cap = 0;
   ws.nmatmax = ws.ngkmax = ws.kmax = 0;
 }
@@ -344,6 +344,7 @@ int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax) {
       (rc = dalloc(&ws.Z2, n * K)) || (rc = dalloc(&ws.Gk, K * K)) || (rc = dalloc(&ws.Gki, K * K)) ||
       (rc = dalloc(&ws.Tf, 2 * ((n + 63) / 64 + 1) * 64 * 64)) || (rc = dalloc(&ws.Xs, 2 * 64 * K)) ||
       (rc = dalloc(&ws.status, (size_t)ST_NWORDS)) || (rc = dalloc(&ws.bar, (size_t)4)) ||
+      (rc = dalloc(&ws.prog, n)) ||
       (rc = dalloc(&ws.part, std::max((size_t)(8u << 20), n * 64 * 4)))) {
     free_workspace(ws);
     return rc;
@@ -422,6 +423,13 @@ int excfv_set_precision(excfv_handle* h, int prec) {
   if (!h) return EXCFV_ERR_ARG;
   if (prec != EXCFV_PREC_FP64 && prec != EXCFV_PREC_MIXED) return EXCFV_ERR_ARG;
   h->prec = prec;
+  return EXCFV_OK;
+}
+
+int excfv_set_reduction(excfv_handle* h, int reduction) {
+  if (!h || reduction < 0 || reduction > 2) return EXCFV_ERR_ARG;
+  h->reduction = reduction;
+  for (excfv_handle* l : h->lanes) l->reduction = reduction;
   return EXCFV_OK;
 }
 
@@ -690,6 +698,45 @@ int excfv_sync(excfv_handle* h) {
 }
 
 long long excfv_launch_count(void) { return g_launches.load(); }
+
+int excfv_test_reduce_band(excfv_handle* h, int32_t n, const double* c, int32_t stages,
+                           double* band, double* d, double* e, int32_t* bandwidth) {
+  if (!h || !c || n < 1 || (stages != 1 && stages != 2) || (stages == 1 && !band) ||
+      (stages == 2 && (!d || !e)))
+    return EXCFV_ERR_ARG;
+  if (!h->have_static) {
+    excfv_set_error("excfv_set_static must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  const int bw = band_bandwidth();
+  if (bandwidth) *bandwidth = bw;
+  DeviceGuard g(h->device);
+  if (!two_stage_supported(h, n)) {
+    excfv_set_error("two-stage reduction does not support n = %d", n);
+    return EXCFV_ERR_UNSUPPORTED;
+  }
+  int rc = stage_reserve(h, n, std::max(1, h->ws.ngkmax), std::max(1, h->st.nstfv));
+  if (rc) return rc;
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  bind_gemm_ctx(h);
+  CUDA_TRY(cudaMemcpyAsync(ws.H, c, sizeof(cplx) * (size_t)n * n, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemsetAsync(ws.status, 0, ST_NWORDS * sizeof(int), s));
+  if ((rc = he2hb(h, n, ws.H, n))) return rc;
+  cplx* AB = ws.T;
+  if ((rc = two_stage_finish_band(h, n, ws.H, n, AB))) return rc;
+  if (stages == 1) {
+    // compact (2 bw + 1, n) -> (bw + 1, n)
+    CUDA_TRY(cudaMemcpy2DAsync(band, sizeof(cplx) * (bw + 1), AB, sizeof(cplx) * (2 * bw + 1),
+                               sizeof(cplx) * (bw + 1), n, cudaMemcpyDeviceToHost, s));
+  } else {
+    if ((rc = hb2st(h, n, AB, ws.O, ws.ybuf))) return rc;
+    CUDA_TRY(cudaMemcpyAsync(d, ws.d, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    if (n > 1) CUDA_TRY(cudaMemcpyAsync(e, ws.e, sizeof(double) * (n - 1), cudaMemcpyDeviceToHost, s));
+  }
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return stage_status(h, n);
+}
 
 int excfv_test_set_wait_limit(int64_t limit_ns, int32_t plant_stall) {
   if (limit_ns <= 0) limit_ns = 2000000000LL;

@@ -80,6 +80,7 @@ struct Workspace {
   size_t part_cap = 0;      // complex elements
   int* status = nullptr;    // ST_NWORDS
   unsigned int* bar = nullptr;  // grid barrier words
+  int* prog = nullptr;      // (n) per-sweep progress of the band -> tridiagonal chase
   // host staging
   cplx* h_pinned = nullptr;
   size_t h_pinned_bytes = 0;
@@ -90,7 +91,7 @@ struct Workspace {
 // EXCFV_PROF_* in include/excfv.h.
 enum {
   PROF_MATCH = 0, PROF_SETUP_GEMM, PROF_SETUP_OTHER, PROF_POTRF, PROF_HEGST, PROF_TRD_PANEL,
-  PROF_TRD_UPDATE, PROF_STEIG, PROF_BACKTR, PROF_NCLS
+  PROF_TRD_UPDATE, PROF_STEIG, PROF_BACKTR, PROF_TRD_CHASE, PROF_NCLS
 };
 
 struct Prof {
@@ -122,6 +123,7 @@ struct excfv_handle {
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
   int prec = EXCFV_PREC_FP64;
+  int reduction = 0;          // tridiagonal reduction: 0 auto, 1 one-stage, 2 two-stage
   bool have_static = false;
   DevStatic st;
   Workspace ws;
@@ -168,3 +170,13 @@ int tridiag_rows_per_cta(bool complex64);
 int status_to_info(const int* st, int n);
 // device status -> LAPACK-style info (synchronises the stream)
 int stage_status(excfv_handle* h, int n);
+// the tridiagonal reduction of the FP64 form: one-stage panels or two-stage
+bool use_two_stage(excfv_handle* h, int n);
+int band_bandwidth();
+bool two_stage_supported(excfv_handle* h, int n);
+size_t chase_reflector_elems(int n);
+int he2hb(excfv_handle* h, int n, cplx* C, long long ld);
+int two_stage_finish_band(excfv_handle* h, int n, cplx* C, long long ld, cplx* AB);
+int hb2st(excfv_handle* h, int n, cplx* AB, cplx* V2, cplx* ph);
+int two_stage_back(excfv_handle* h, int n, int k, const cplx* C, long long ld, const cplx* V2,
+                   const cplx* ph, cplx* Z, long long ldz);

@@ -344,23 +344,27 @@ __global__ void k_copy_eval(int k, const double* w, double* out) {
 
 }  // namespace
 
-// Z (n x k) <- Q Z with Q = H_0 ... H_{n-2} from tridiag_reduce.
-int apply_q(excfv_handle* h, int n, int k, const cplx* C, long long ld, cplx* Z, long long ldz) {
+// Z (n x k) <- Q Z with Q = H_0 ... H_{n-1-off}: reflector c stored in
+// column c of C from row c + off down, unit entry explicit (off = 1 for the
+// one-stage reduction, the bandwidth for stage 1 of the two-stage one).
+int apply_q(excfv_handle* h, int n, int k, const cplx* C, long long ld, cplx* Z, long long ldz,
+            int off) {
   Workspace& ws = h->ws;
   cudaStream_t s = h->stream;
-  if (n < 2) return EXCFV_OK;
-  const int nblk = (n - 1 + NBQ - 1) / NBQ;
+  const int nrefl = n - off;
+  if (nrefl < 1) return EXCFV_OK;
+  const int nblk = (nrefl + NBQ - 1) / NBQ;
   const cplx one = cmk(1.0, 0.0), mone = cmk(-1.0, 0.0), zero = cmk(0.0, 0.0);
   cplx* Gall = ws.Tf + (size_t)nblk * NBQ * NBQ;
   // Gram matrices G_b = V_b^H V_b: the full blocks in one batched GEMM
   // (K shrinks by NBQ from block to block), the last partial block alone.
-  const int nfull = (n - 1) / NBQ;
+  const int nfull = nrefl / NBQ;
   if (nfull > 0) {
     ZgemmArgs g;
-    g.m = NBQ; g.n = NBQ; g.k = n - 1; g.kdec = NBQ;
+    g.m = NBQ; g.n = NBQ; g.k = n - off; g.kdec = NBQ;
     g.alpha = one; g.beta = zero;
-    g.A = C + 1; g.lda = ld; g.strideA = (long long)NBQ * (ld + 1);
-    g.B = C + 1; g.ldb = ld; g.strideB = (long long)NBQ * (ld + 1);
+    g.A = C + off; g.lda = ld; g.strideA = (long long)NBQ * (ld + 1);
+    g.B = C + off; g.ldb = ld; g.strideB = (long long)NBQ * (ld + 1);
     g.C = Gall; g.ldc = NBQ; g.strideC = (long long)NBQ * NBQ;
     g.batch = nfull; g.uplo_c = TRI_UPPER; g.tri_a = TRI_UPPER; g.tri_b = TRI_LOWER;
     g.splitk = 1; g.part = nullptr;
@@ -369,24 +373,24 @@ int apply_q(excfv_handle* h, int n, int k, const cplx* C, long long ld, cplx* Z,
   }
   if (nfull < nblk) {
     const int p = nfull * NBQ;
-    const int nb = n - 1 - p, m = n - p - 1;
-    const cplx* V = C + (p + 1) + ld * p;
+    const int nb = nrefl - p, m = n - p - off;
+    const cplx* V = C + (p + off) + ld * p;
     int rc = zgemm1(s, OP_C, OP_N, nb, nb, m, one, V, ld, V, ld, zero, Gall + (size_t)nfull * NBQ * NBQ,
                     NBQ, TRI_UPPER, TRI_UPPER, TRI_LOWER);
     if (rc) return rc;
   }
   const int smem = (int)(2 * sizeof(cplx) * NBQ * (NBQ + 1));
   CUDA_TRY(cudaFuncSetAttribute(k_larft, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  k_larft<<<nblk, LT, smem, s>>>(n, Gall, ws.tau, ws.Tf); count_launch();
+  k_larft<<<nblk, LT, smem, s>>>(nrefl + 1, Gall, ws.tau, ws.Tf); count_launch();
   CUDA_TRY(cudaGetLastError());
   cplx* X1 = ws.Xs;
   cplx* X2 = ws.Xs + (size_t)NBQ * ws.kmax;
   for (int b = nblk - 1; b >= 0; --b) {
     const int p = b * NBQ;
-    const int nb = min(NBQ, n - 1 - p);
-    const int m = n - p - 1;
-    const cplx* V = C + (p + 1) + ld * p;
-    cplx* Zs = Z + (p + 1);
+    const int nb = min(NBQ, nrefl - p);
+    const int m = n - p - off;
+    const cplx* V = C + (p + off) + ld * p;
+    cplx* Zs = Z + (p + off);
     int rc = zgemm1(s, OP_C, OP_N, nb, k, m, one, V, ld, Zs, ldz, zero, X1, NBQ, TRI_NONE,
                     TRI_UPPER, TRI_NONE);
     if (rc) return rc;
@@ -416,6 +420,17 @@ int cholqr(excfv_handle* h, int n, int k, cplx*& Z, long long ldz) {
   Z = ws.Z2;
   ws.Z2 = t;
   return EXCFV_OK;
+}
+
+// The two-stage reduction when the handle asks for it and it supports n
+// (its chase reflectors must fit ws.O); the one-stage panels otherwise.  On
+// one B200 the one-stage panels are faster at the orders of the workloads
+// (n = 316..5028): the chase's ~3n dependent steps each pay a hand-off
+// between SMs, so EXCFV_REDUCTION_AUTO takes the one-stage reduction.
+bool use_two_stage(excfv_handle* h, int n) {
+  if (h->reduction != EXCFV_REDUCTION_TWO_STAGE) return false;
+  if (!two_stage_supported(h, n)) return false;
+  return chase_reflector_elems(n) <= (size_t)n * n;
 }
 
 // States carried through the complex64 reduction so that the Rayleigh-Ritz
@@ -453,8 +468,18 @@ int stage_solve(excfv_handle* h, int n, int k, double evaltol, double* d_eval, c
     return rc;
   if ((rc = mirror_upper(s, n, ws.H, ld))) return rc;
   prof_end(h, PROF_HEGST);
-  // tridiagonal reduction
-  if ((rc = tridiag_reduce(h, n, ws.H, ld))) return rc;
+  // tridiagonal reduction: C = Q T Q^H, Q's reflectors in C (and, two-stage,
+  // the chase reflectors in ws.O, the band in ws.T, the phase in ws.ybuf)
+  const bool two = use_two_stage(h, n);
+  if (two) {
+    if ((rc = he2hb(h, n, ws.H, ld))) return rc;
+    if ((rc = two_stage_finish_band(h, n, ws.H, ld, ws.T))) return rc;
+    prof_begin(h, PROF_TRD_CHASE);
+    if ((rc = hb2st(h, n, ws.T, ws.O, ws.ybuf))) return rc;
+    prof_end(h, PROF_TRD_CHASE);
+  } else {
+    if ((rc = tridiag_reduce(h, n, ws.H, ld))) return rc;
+  }
   // eigenpairs of T
   cplx* Z = ws.Z;
   prof_begin(h, PROF_STEIG);
@@ -464,7 +489,11 @@ int stage_solve(excfv_handle* h, int n, int k, double evaltol, double* d_eval, c
   prof_begin(h, PROF_BACKTR);
   if ((rc = cholqr(h, n, k, Z, ld))) return rc;
   // back-transforms
-  if ((rc = apply_q(h, n, k, ws.H, ld, Z, ld))) return rc;
+  if (two) {
+    if ((rc = two_stage_back(h, n, k, ws.H, ld, ws.O, ws.ybuf, Z, ld))) return rc;
+  } else {
+    if ((rc = apply_q(h, n, k, ws.H, ld, Z, ld, 1))) return rc;
+  }
   if ((rc = zgemm1(s, OP_N, OP_N, n, k, n, one, ws.Ui, ld, Z, ld, zero, d_evec, ldevec, TRI_NONE,
                    TRI_UPPER, TRI_NONE)))
     return rc;
@@ -527,7 +556,7 @@ static int stage_solve_mixed(excfv_handle* h, int n, int k, double evaltol, doub
     return rc;
   prof_end(h, PROF_STEIG);
   prof_begin(h, PROF_BACKTR);
-  if ((rc = apply_q(h, n, kx, ws.O, ld, Z, ld))) return rc;
+  if ((rc = apply_q(h, n, kx, ws.O, ld, Z, ld, 1))) return rc;
   // X0 = Z: orthonormal up to the complex64 rounding of the reflectors,
   // S = X0^H X0 = I + D with |D| ~ 1e-7.  Rayleigh-Ritz in FP64 on
   // S^-1/2 Hk S^-1/2 with S^-1/2 = I - D/2 (error O(D^2)):

@@ -81,6 +81,9 @@ SIGNATURES = {
     "excfv_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "excfv_launch_count": (C.c_longlong, []),
     "excfv_test_set_wait_limit": (C.c_int, [C.c_int64, C.c_int32]),
+    "excfv_set_reduction": (C.c_int, [C.c_void_p, C.c_int]),
+    "excfv_test_reduce_band": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.c_void_p]),
     "excfv_seceqn_batched_dev": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
@@ -101,7 +104,11 @@ SIGNATURES = {
 NOALLOC_SCRATCH_BYTES = 32 << 20
 
 PROF_CLASSES = ["match", "setup_gemm", "setup_other", "potrf", "hegst", "trd_panel",
-                "trd_update", "steig", "backtr"]
+                "trd_update", "steig", "backtr", "trd_chase"]
+
+EXCFV_REDUCTION_AUTO = 0
+EXCFV_REDUCTION_ONE_STAGE = 1
+EXCFV_REDUCTION_TWO_STAGE = 2
 
 _lib: Optional[C.CDLL] = None
 

@@ -121,6 +121,19 @@ int excfv_destroy(excfv_handle* h);
 const char* excfv_last_error(void);
 /* Precision form: EXCFV_PREC_FP64 (default) or EXCFV_PREC_MIXED. */
 int excfv_set_precision(excfv_handle* h, int prec);
+
+/* Tridiagonal reduction of the FP64 form (the ZHETRD step of ZHEGVX,
+ * external/LAPACK/zheevx.f:441).  EXCFV_REDUCTION_AUTO (default) and
+ * EXCFV_REDUCTION_ONE_STAGE: the one-stage Householder panels (the faster
+ * form on one B200 at the workloads' orders).  EXCFV_REDUCTION_TWO_STAGE:
+ * dense -> band of width 32 (cluster panel QRs, DMMA GEMMs), then band ->
+ * tridiagonal by bulge chasing, for orders 128..5664 (others fall back to
+ * the one-stage form); eigenvalues agree with the one-stage form to
+ * rounding. */
+#define EXCFV_REDUCTION_AUTO 0
+#define EXCFV_REDUCTION_ONE_STAGE 1
+#define EXCFV_REDUCTION_TWO_STAGE 2
+int excfv_set_reduction(excfv_handle* h, int reduction);
 /* Stream used by the _dev entry points (cudaStream_t as void*; NULL = own). */
 int excfv_set_stream(excfv_handle* h, void* stream);
 /* Sizes the device workspace for matrices up to nmatmax and G+k sets up to
@@ -239,11 +252,12 @@ int excfv_get_timings(excfv_handle* h, double* t4);
 #define EXCFV_PROF_SETUP_OTHER 2 /* LO band, interstitial, mirror            */
 #define EXCFV_PROF_POTRF 3       /* Cholesky + inverse factor                */
 #define EXCFV_PROF_HEGST 4       /* U^-H H U^-1                              */
-#define EXCFV_PROF_TRD_PANEL 5   /* tridiagonal panel kernels (launches)     */
+#define EXCFV_PROF_TRD_PANEL 5   /* tridiagonal / band panel kernels         */
 #define EXCFV_PROF_TRD_UPDATE 6  /* trailing rank-2k updates                 */
 #define EXCFV_PROF_STEIG 7       /* bisection + inverse iteration            */
 #define EXCFV_PROF_BACKTR 8      /* orthonormalisation + back-transforms     */
-#define EXCFV_PROF_NCLS 9
+#define EXCFV_PROF_TRD_CHASE 9   /* band -> tridiagonal bulge chase + phase  */
+#define EXCFV_PROF_NCLS 10
 int excfv_profile(excfv_handle* h, int enable);
 int excfv_profile_read(excfv_handle* h, double* ms, long long* count, int nclasses);
 
@@ -261,6 +275,18 @@ long long excfv_launch_count(void);
  * EXCFV_ERR_TIMEOUT with the handle still usable.  Not for production use.
  */
 int excfv_test_set_wait_limit(int64_t limit_ns, int32_t plant_stall);
+
+/*
+ * Test aid (no counterpart in the reference): the stages of the two-stage
+ * reduction on a Hermitian n x n matrix c (host, column-major, both
+ * triangles).  stages = 1: dense -> band only; band receives the lower band
+ * in compact storage, band[(r - c) + (bw + 1) c], bw = *bandwidth.
+ * stages = 2: the whole reduction; d (n) and e (n - 1) receive the real
+ * tridiagonal (band may be null).  For comparison with a restatement of
+ * LAPACK's he2hb / hb2st.
+ */
+int excfv_test_reduce_band(excfv_handle* h, int32_t n, const double* c, int32_t stages,
+                           double* band, double* d, double* e, int32_t* bandwidth);
 
 /* ---- matching coefficients without device allocation ------------------- */
 

@@ -38,13 +38,18 @@ def diamond():
     return st, kp, H, O, w_ref
 
 
-@pytest.mark.parametrize("prec,etol", [(EXCFV_PREC_FP64, 1e-10), (EXCFV_PREC_MIXED, 1e-8)],
-                         ids=["fp64", "mixed"])
-def test_bounded_wait_runs_out_then_handle_recovers(diamond, prec, etol):
+@pytest.mark.parametrize("prec,red,etol", [(EXCFV_PREC_FP64, L.EXCFV_REDUCTION_ONE_STAGE, 1e-10),
+                                          (EXCFV_PREC_FP64, L.EXCFV_REDUCTION_TWO_STAGE, 1e-10),
+                                          (EXCFV_PREC_MIXED, L.EXCFV_REDUCTION_AUTO, 1e-8)],
+                         ids=["fp64-panels", "fp64-chase", "mixed"])
+def test_bounded_wait_runs_out_then_handle_recovers(diamond, prec, red, etol):
+    """The planted stall hits the one-stage panel kernel's grid barrier, the
+    bulge chase's progress wait, or the complex64 panel kernel."""
     st, kp, H, O, w_ref = diamond
     lib = L.load()
     with FirstVariational(0, precision=prec) as fv:
         fv.set_static(st)
+        assert fv._L.excfv_set_reduction(fv._h, red) == 0
         w, _ = fv.seceqn(kp)                      # a normal solve first (warm handle)
         assert np.abs(w - w_ref).max() < etol
         try:
