@@ -55,18 +55,7 @@ void dfree(T*& p) {
   p = nullptr;
 }
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int cur;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
+
 
 double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -127,6 +116,8 @@ void free_static(DevStatic& st) {
   dfree(st.aa); dfree(st.loa); dfree(st.lolo); dfree(st.oalo); dfree(st.ololo); dfree(st.h1aa);
   dfree(st.ivg); dfree(st.ivgig); dfree(st.veffig); dfree(st.xig); dfree(st.cfunig);
   dfree(st.m2effig); dfree(st.zdinv);
+  dfree(st.vgc); dfree(st.atposc); dfree(st.gkcount);
+  st.have_lattice = false;
 }
 
 void free_workspace(Workspace& ws) {
@@ -136,6 +127,9 @@ void free_workspace(Workspace& ws) {
   dfree(ws.Wp); dfree(ws.red); dfree(ws.w); dfree(ws.stein_ws); dfree(ws.icl); dfree(ws.ybuf);
   dfree(ws.Z); dfree(ws.Z2); dfree(ws.Gk); dfree(ws.Gki); dfree(ws.Tf); dfree(ws.Xs);
   dfree(ws.status); dfree(ws.bar); dfree(ws.part); dfree(ws.prog);
+  if (ws.h_pinned) cudaFreeHost(ws.h_pinned);
+  ws.h_pinned = nullptr;
+  ws.h_pinned_bytes = 0;
   ws.part_cap = 0;
   ws.nmatmax = ws.ngkmax = ws.kmax = 0;
 }
@@ -520,7 +514,13 @@ int excfv_hamiltonandoverlapsetup(excfv_handle* h, int32_t nmatp, int32_t ngp, i
   const size_t nn = (size_t)nmatp * nmatp;
   CUDA_TRY(cudaMemcpyAsync(hmat, ws.H, sizeof(cplx) * nn, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaMemcpyAsync(omat, ws.O, sizeof(cplx) * nn, cudaMemcpyDeviceToHost, s));
+  int setup_flag = 0;
+  CUDA_TRY(cudaMemcpyAsync(&setup_flag, ws.status + ST_SETUP, sizeof(int), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
+  if (setup_flag) {
+    excfv_set_error("a bounded wait of the setup contraction timed out");
+    return EXCFV_ERR_TIMEOUT;
+  }
   return EXCFV_OK;
 }
 
@@ -698,6 +698,115 @@ int excfv_sync(excfv_handle* h) {
 }
 
 long long excfv_launch_count(void) { return g_launches.load(); }
+
+int excfv_set_lattice(excfv_handle* h, const double* vgc, const double* atposc) {
+  if (!h || !vgc || !atposc) return EXCFV_ERR_ARG;
+  if (!h->have_static) {
+    excfv_set_error("excfv_set_static must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  DeviceGuard g(h->device);
+  return stage_set_lattice(h, vgc, atposc);
+}
+
+int excfv_gengpvec_dev(excfv_handle* h, const double* vpl, const double* vpc, double gkmax, int32_t ngkmax,
+                       int32_t* d_ngp, int32_t* igpig, double* vgpl, double* vgpc, double* gpc, double* tpgpc) {
+  if (!h || !vpl || !vpc || !d_ngp || !igpig || !vgpl || !vgpc || !gpc || !tpgpc || ngkmax < 1 || gkmax <= 0.0)
+    return EXCFV_ERR_ARG;
+  if (!h->have_static || !h->st.have_lattice) {
+    excfv_set_error("excfv_set_static and excfv_set_lattice must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  DeviceGuard g(h->device);
+  return stage_gengpvec(h, vpl, vpc, gkmax, ngkmax, d_ngp, igpig, vgpl, vgpc, gpc, tpgpc);
+}
+
+int excfv_gengpvec(excfv_handle* h, const double* vpl, const double* vpc, double gkmax, int32_t ngkmax,
+                   int32_t* ngp, int32_t* igpig, double* vgpl, double* vgpc, double* gpc, double* tpgpc) {
+  if (!h || !ngp || !igpig || !vgpl || !vgpc || !gpc || !tpgpc || ngkmax < 1) return EXCFV_ERR_ARG;
+  if (!h->have_static || !h->st.have_lattice) {
+    excfv_set_error("excfv_set_static and excfv_set_lattice must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  DeviceGuard g(h->device);
+  cudaStream_t s = h->stream;
+  int* di = nullptr;
+  double* dd = nullptr;
+  int rc;
+  if ((rc = dalloc(&di, (size_t)ngkmax + 1))) return rc;
+  if ((rc = dalloc(&dd, (size_t)9 * ngkmax))) {
+    cudaFree(di);
+    return rc;
+  }
+  double* dvgpl = dd;
+  double* dvgpc = dd + 3 * (size_t)ngkmax;
+  double* dgpc = dd + 6 * (size_t)ngkmax;
+  double* dtp = dd + 7 * (size_t)ngkmax;
+  rc = stage_gengpvec(h, vpl, vpc, gkmax, ngkmax, di + ngkmax, di, dvgpl, dvgpc, dgpc, dtp);
+  int n = 0;
+  if (rc == EXCFV_OK && cudaMemcpyAsync(&n, di + ngkmax, sizeof(int), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+      cudaStreamSynchronize(s) == cudaSuccess) {
+    if (n < 0) {
+      excfv_set_error("gengpvec: %d G+k vectors exceed ngkmax = %d", -n, ngkmax);
+      rc = EXCFV_ERR_ARG;
+    } else if (n > 0) {
+      cudaMemcpyAsync(igpig, di, sizeof(int) * n, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(vgpl, dvgpl, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(vgpc, dvgpc, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(gpc, dgpc, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(tpgpc, dtp, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, s);
+      if (cudaStreamSynchronize(s) != cudaSuccess) rc = EXCFV_ERR_CUDA;
+    }
+    *ngp = n;
+  } else if (rc == EXCFV_OK) {
+    rc = EXCFV_ERR_CUDA;
+  }
+  cudaFree(di);
+  cudaFree(dd);
+  return rc;
+}
+
+int excfv_gensfacgp_dev(excfv_handle* h, int32_t ngp, const double* vgpc, int32_t ld, double* sfacgp) {
+  if (!h || !vgpc || !sfacgp || ngp < 0 || ld < ngp) return EXCFV_ERR_ARG;
+  if (!h->have_static || !h->st.have_lattice) {
+    excfv_set_error("excfv_set_static and excfv_set_lattice must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  if (ngp == 0) return EXCFV_OK;
+  DeviceGuard g(h->device);
+  return stage_gensfacgp(h, ngp, vgpc, ld, reinterpret_cast<cplx*>(sfacgp));
+}
+
+int excfv_gensfacgp(excfv_handle* h, int32_t ngp, const double* vgpc, int32_t ld, double* sfacgp) {
+  if (!h || !vgpc || !sfacgp || ngp < 0 || ld < ngp) return EXCFV_ERR_ARG;
+  if (!h->have_static || !h->st.have_lattice) {
+    excfv_set_error("excfv_set_static and excfv_set_lattice must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  if (ngp == 0) return EXCFV_OK;
+  DeviceGuard g(h->device);
+  cudaStream_t s = h->stream;
+  double* dv = nullptr;
+  cplx* ds = nullptr;
+  int rc;
+  if ((rc = dalloc(&dv, (size_t)3 * ngp))) return rc;
+  if ((rc = dalloc(&ds, (size_t)ld * h->st.natmtot))) {
+    cudaFree(dv);
+    return rc;
+  }
+  if (cudaMemcpyAsync(dv, vgpc, sizeof(double) * 3 * ngp, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemsetAsync(ds, 0, sizeof(cplx) * (size_t)ld * h->st.natmtot, s) != cudaSuccess)
+    rc = EXCFV_ERR_CUDA;
+  if (rc == EXCFV_OK) rc = stage_gensfacgp(h, ngp, dv, ld, ds);
+  if (rc == EXCFV_OK &&
+      (cudaMemcpyAsync(sfacgp, ds, sizeof(cplx) * (size_t)ld * h->st.natmtot, cudaMemcpyDeviceToHost, s) !=
+           cudaSuccess ||
+       cudaStreamSynchronize(s) != cudaSuccess))
+    rc = EXCFV_ERR_CUDA;
+  cudaFree(dv);
+  cudaFree(ds);
+  return rc;
+}
 
 int excfv_test_reduce_band(excfv_handle* h, int32_t n, const double* c, int32_t stages,
                            double* band, double* d, double* e, int32_t* bandwidth) {

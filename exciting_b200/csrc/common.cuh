@@ -39,7 +39,10 @@ EXCFV_HD double cabs2(cplx a) { return a.x * a.x + a.y * a.y; }
 //   [1] grid barrier timeout count
 //   [2] stein: number of eigenvectors that failed to converge
 //   [3] stebz: bisection did not converge for some eigenvalue
-enum { ST_POTRF = 0, ST_BARRIER = 1, ST_STEIN = 2, ST_STEBZ = 3, ST_REFINE = 4, ST_NWORDS = 8 };
+//   [4] refinement: cluster above the precision form's limit
+//   [5] setup: a bounded wait of the setup contraction gave up (cleared by the
+//       setup, not by the eigensolve)
+enum { ST_POTRF = 0, ST_BARRIER = 1, ST_STEIN = 2, ST_STEBZ = 3, ST_REFINE = 4, ST_SETUP = 5, ST_NWORDS = 8 };
 
 #define CUDA_TRY(expr)                                                          \
   do {                                                                          \

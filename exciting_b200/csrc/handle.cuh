@@ -40,6 +40,11 @@ struct DevStatic {
   cplx* cfunig = nullptr;
   cplx* m2effig = nullptr;
   double* zdinv = nullptr;  // (apwordmax, apwordmax, lmaxapw+1, natmtot) inverse of zd
+  // lattice for the device G+k set (excfv_set_lattice)
+  bool have_lattice = false;
+  double* vgc = nullptr;    // (3, ngvec) Cartesian G vectors
+  double* atposc = nullptr; // (3, natmtot) Cartesian atomic positions
+  int* gkcount = nullptr;   // per-block counts of the G+k compaction, then ngp and overflow
 };
 
 struct Workspace {
@@ -133,6 +138,20 @@ struct excfv_handle {
   bool her2k_smem_set = false;  // k_her2k_f32's shared-memory limit raised on this device
 };
 
+// makes the handle's device current for the scope of an entry point
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
 // makes the handle's split-K scratch current for this thread's GEMMs
 inline void bind_gemm_ctx(excfv_handle* h) {
   GemmCtx c;
@@ -170,6 +189,15 @@ int tridiag_rows_per_cta(bool complex64);
 int status_to_info(const int* st, int n);
 // device status -> LAPACK-style info (synchronises the stream)
 int stage_status(excfv_handle* h, int n);
+// device G+k set and structure factors (gkset.cu)
+int stage_set_lattice(excfv_handle* h, const double* vgc, const double* atposc);
+int stage_gengpvec(excfv_handle* h, const double* vpl, const double* vpc, double gkmax, int ngkmax,
+                   int* d_ngp, int* igpig, double* vgpl, double* vgpc, double* gpc, double* tpgpc);
+int stage_gensfacgp(excfv_handle* h, int ngp, const double* vgpc, long long ld, cplx* sfacgp);
+// C_z = alpha A_z^H B_z + beta C_z (z < batch <= 2) with TMA-fed tiles (zgemm_tma.cu)
+int zgemm_cn_tma(excfv_handle* h, int m, int n, int k, cplx alpha, const cplx* const* A, long long lda,
+                 const cplx* const* B, long long ldb, cplx beta, cplx* const* C, long long ldc, int batch,
+                 int uplo);
 // the tridiagonal reduction of the FP64 form: one-stage panels or two-stage
 bool use_two_stage(excfv_handle* h, int n);
 int band_bandwidth();

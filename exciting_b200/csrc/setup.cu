@@ -197,6 +197,7 @@ int stage_setup(excfv_handle* h, int nmatp, int ngp, bool mirror_o) {
   const cplx one = cmk(1.0, 0.0), zero = cmk(0.0, 0.0);
   int rc;
   bind_gemm_ctx(h);
+  CUDA_TRY(cudaMemsetAsync(ws.status + ST_SETUP, 0, sizeof(int), s));
 
   // Z_a = aa_a * A_a for every atom (hamiltonsetup.f90:75-88)
   ZgemmArgs z;
@@ -212,35 +213,30 @@ int stage_setup(excfv_handle* h, int nmatp, int ngp, bool mirror_o) {
   CUDA_TRY(cudaGetLastError());
   // H_GG = sum_a A_a^H Z_a (hamiltonsetup.f90:90-103), upper triangle
   // O_GG = sum_a A_a^H (I + H1) A_a (overlapsetup.f90:82-108), upper triangle
+  // A^H B contractions with TMA-fed operand tiles (zgemm_tma.cu)
+  const cplx* Aop[2] = {ws.Apk, ws.Apk};
   if (!st.have_h1aa) {
-    // both contractions share A^H: one launch of two batch entries
-    // (B = Z or A, C = H or O; the strides are the distances between the buffers)
-    ZgemmArgs g;
-    g.m = N; g.n = N; g.k = (int)AM; g.kdec = 0; g.alpha = one; g.beta = zero;
-    g.A = ws.Apk; g.lda = AM; g.strideA = 0;
-    g.B = ws.Zpk; g.ldb = AM; g.strideB = ws.Apk - ws.Zpk;
-    g.C = ws.H; g.ldc = ld; g.strideC = ws.O - ws.H;
-    g.batch = 2; g.uplo_c = TRI_UPPER; g.tri_a = TRI_NONE; g.tri_b = TRI_NONE;
-    g.splitk = 1; g.part = nullptr;
+    // both contractions share A^H: one grid over both outputs
+    const cplx* Bop[2] = {ws.Zpk, ws.Apk};
+    cplx* Cop[2] = {ws.H, ws.O};
     prof_begin(h, PROF_SETUP_GEMM);
-    if ((rc = zgemm(s, OP_C, OP_N, g))) return rc;
+    if ((rc = zgemm_cn_tma(h, N, N, (int)AM, one, Aop, AM, Bop, AM, zero, Cop, ld, 2, TRI_UPPER))) return rc;
     prof_end(h, PROF_SETUP_GEMM);
   } else {
     // IORA*: Z is overwritten by (I + H1) A after the H contraction
+    const cplx* Bop[1] = {ws.Zpk};
+    cplx* Cop[1] = {ws.H};
     prof_begin(h, PROF_SETUP_GEMM);
-    if ((rc = zgemm1(s, OP_C, OP_N, N, N, (int)AM, one, ws.Apk, AM, ws.Zpk, AM, zero, ws.H, ld,
-                     TRI_UPPER)))
-      return rc;
+    if ((rc = zgemm_cn_tma(h, N, N, (int)AM, one, Aop, AM, Bop, AM, zero, Cop, ld, 1, TRI_UPPER))) return rc;
     prof_end(h, PROF_SETUP_GEMM);
     const long long tot = AM * N;
     k_apply_h1<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(
         N, st.natmtot, st.maxaa, st.apwordmax, st.lmaxapw, st.idxis, st.flist, st.fofl,
         st.lmmaxapw, st.h1aa, ws.Apk, ws.Zpk); count_launch();
     CUDA_TRY(cudaGetLastError());
+    cplx* Cop2[1] = {ws.O};
     prof_begin(h, PROF_SETUP_GEMM);
-    if ((rc = zgemm1(s, OP_C, OP_N, N, N, (int)AM, one, ws.Apk, AM, ws.Zpk, AM, zero, ws.O, ld,
-                     TRI_UPPER)))
-      return rc;
+    if ((rc = zgemm_cn_tma(h, N, N, (int)AM, one, Aop, AM, Bop, AM, zero, Cop2, ld, 1, TRI_UPPER))) return rc;
     prof_end(h, PROF_SETUP_GEMM);
   }
   CUDA_TRY(cudaGetLastError());

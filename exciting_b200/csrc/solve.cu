@@ -452,7 +452,7 @@ int stage_solve(excfv_handle* h, int n, int k, double evaltol, double* d_eval, c
   if (k < 1 || k > n) return EXCFV_ERR_ARG;
   bind_gemm_ctx(h);
   if (k > ws.kmax) return EXCFV_ERR_ARG;
-  CUDA_TRY(cudaMemsetAsync(ws.status, 0, ST_NWORDS * sizeof(int), s));
+  CUDA_TRY(cudaMemsetAsync(ws.status, 0, ST_SETUP * sizeof(int), s));
   // O = U^H U, Ui = U^-1
   prof_begin(h, PROF_POTRF);
   if ((rc = potrf_upper(h, n, ws.O, ws.Ui, ld))) return rc;
@@ -524,7 +524,7 @@ static int stage_solve_mixed(excfv_handle* h, int n, int k, double evaltol, doub
     return EXCFV_ERR_ARG;
   }
   bind_gemm_ctx(h);
-  CUDA_TRY(cudaMemsetAsync(ws.status, 0, ST_NWORDS * sizeof(int), s));
+  CUDA_TRY(cudaMemsetAsync(ws.status, 0, ST_SETUP * sizeof(int), s));
   prof_begin(h, PROF_POTRF);
   if ((rc = potrf_upper(h, n, ws.O, ws.Ui, ld))) return rc;
   if ((rc = trtri_upper(h, n, ws.O, ws.Ui, ld, ws.T))) return rc;
@@ -641,6 +641,10 @@ int stage_status(excfv_handle* h, int n) {
 }
 
 int status_to_info(const int* st, int n) {
+  if (st[ST_SETUP]) {
+    excfv_set_error("a bounded wait of the setup contraction timed out");
+    return EXCFV_ERR_TIMEOUT;
+  }
   if (st[ST_BARRIER]) {
     excfv_set_error("grid barrier timed out in the tridiagonal reduction");
     return EXCFV_ERR_TIMEOUT;

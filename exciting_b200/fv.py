@@ -313,6 +313,35 @@ class FirstVariational:
             raise ExcfvError(rc, "excfv_seceqn_batched")
         return outs, info
 
+    # ------------------------------------------------------------------
+    # G+k set and structure factors on the device
+    def set_lattice(self, vgc: np.ndarray, atposc: np.ndarray) -> None:
+        """Cartesian G vectors (3, ngvec) in ivg order and atomic positions (3, natmtot)."""
+        v = _f(vgc[:, :self.static.ngvec], np.float64)
+        a = _f(atposc, np.float64)
+        self._check(self._L.excfv_set_lattice(self._h, _ptr(v), _ptr(a)), "excfv_set_lattice")
+
+    def gengpvec(self, vpl, vpc, gkmax: float, ngkmax: int) -> dict:
+        """``gengpvec`` on the device; host arrays out (reference layouts)."""
+        vpl = _f(vpl, np.float64)
+        vpc = _f(vpc, np.float64)
+        ngp = C.c_int32(0)
+        out = {"igpig": np.zeros(ngkmax, dtype=np.int32),
+               "vgpl": np.zeros((3, ngkmax), order="F"), "vgpc": np.zeros((3, ngkmax), order="F"),
+               "gpc": np.zeros(ngkmax), "tpgpc": np.zeros((2, ngkmax), order="F")}
+        rc = self._L.excfv_gengpvec(self._h, _ptr(vpl), _ptr(vpc), float(gkmax), int(ngkmax), C.byref(ngp),
+                                    _ptr(out["igpig"]), _ptr(out["vgpl"]), _ptr(out["vgpc"]),
+                                    _ptr(out["gpc"]), _ptr(out["tpgpc"]))
+        self._check(rc, "excfv_gengpvec")
+        out["ngp"] = int(ngp.value)
+        return out
+
+    def gensfacgp(self, ngp: int, vgpc: np.ndarray, ld: int) -> np.ndarray:
+        v = _f(vgpc, np.float64)
+        out = np.zeros((ld, self.static.natmtot), dtype=np.complex128, order="F")
+        self._check(self._L.excfv_gensfacgp(self._h, int(ngp), _ptr(v), int(ld), _ptr(out)), "excfv_gensfacgp")
+        return out
+
     def set_stream(self, stream_ptr: int) -> None:
         self._check(self._L.excfv_set_stream(self._h, C.c_void_p(stream_ptr)), "excfv_set_stream")
 

@@ -82,6 +82,19 @@ SIGNATURES = {
     "excfv_launch_count": (C.c_longlong, []),
     "excfv_test_set_wait_limit": (C.c_int, [C.c_int64, C.c_int32]),
     "excfv_set_reduction": (C.c_int, [C.c_void_p, C.c_int]),
+    "excfv_set_lattice": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "excfv_putevecfv": (C.c_int, [C.c_char_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                  C.c_void_p]),
+    "excfv_putevecfv_dev": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32,
+                                      C.c_int32, C.c_void_p]),
+    "excfv_getevecfv": (C.c_int, [C.c_char_p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_int32,
+                                  C.c_void_p]),
+    "excfv_gengpvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int32, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "excfv_gengpvec_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int32, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "excfv_gensfacgp": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p]),
+    "excfv_gensfacgp_dev": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p]),
     "excfv_test_reduce_band": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.c_void_p]),
     "excfv_seceqn_batched_dev": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
@@ -139,3 +152,29 @@ class ExcfvError(RuntimeError):
     def __init__(self, code: int, where: str):
         self.code = code
         super().__init__(f"{where} failed with status {code}: {last_error()}")
+
+
+def putevecfv(path: str, ik: int, vkl, evecfv) -> None:
+    """Write record ik (1-based) of an EVECFV file; evecfv is (nmatmax, nstfv[, nspnfv]) complex."""
+    import numpy as np
+    L = load()
+    e = np.asfortranarray(evecfv, dtype=np.complex128)
+    if e.ndim == 2:
+        e = e[:, :, None]
+    v = np.ascontiguousarray(vkl, dtype=np.float64)
+    rc = L.excfv_putevecfv(path.encode(), ik, v.ctypes.data, e.shape[0], e.shape[1], e.shape[2], e.ctypes.data)
+    if rc:
+        raise ExcfvError(rc, "excfv_putevecfv")
+
+
+def getevecfv(path: str, ik: int, vkl, nmatmax: int, nstfv: int, nspnfv: int = 1):
+    """Read record ik of an EVECFV file with the reference's consistency checks."""
+    import numpy as np
+    L = load()
+    e = np.zeros((nmatmax, nstfv, nspnfv), dtype=np.complex128, order="F")
+    v = None if vkl is None else np.ascontiguousarray(vkl, dtype=np.float64)
+    rc = L.excfv_getevecfv(path.encode(), ik, None if v is None else v.ctypes.data, nmatmax, nstfv, nspnfv,
+                           e.ctypes.data)
+    if rc:
+        raise ExcfvError(rc, "excfv_getevecfv")
+    return e

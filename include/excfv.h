@@ -122,6 +122,54 @@ const char* excfv_last_error(void);
 /* Precision form: EXCFV_PREC_FP64 (default) or EXCFV_PREC_MIXED. */
 int excfv_set_precision(excfv_handle* h, int prec);
 
+/* ---- G+k set and structure factors on the device ------------------------ */
+
+/* Lattice data of the device G+k set (module data that gengvec and mod_atoms
+ * hold in the reference): vgc(3, ngvec) the Cartesian G vectors in the order
+ * of excfv_static.ivg (sorted by length), atposc(3, natmtot) the Cartesian
+ * atomic positions.  Host pointers, copied.  excfv_set_static drops them, so
+ * call this after it. */
+int excfv_set_lattice(excfv_handle* h, const double* vgc, const double* atposc);
+
+/* gengpvec (src/gengpvec.f90:13): the G+k vectors of the k-point vpl
+ * (lattice coordinates; vpc its Cartesian form) with |G + k| < gkmax, in G
+ * order.  Host arrays out: *ngp, igpig(ngkmax) (1-based), vgpl(3, ngkmax),
+ * vgpc(3, ngkmax), gpc(ngkmax), tpgpc(2, ngkmax) (sphcrd: theta, phi in
+ * [0, 2 pi)); entries past ngp are untouched.  More than ngkmax vectors is
+ * EXCFV_ERR_ARG (the reference stops). */
+int excfv_gengpvec(excfv_handle* h, const double* vpl, const double* vpc, double gkmax, int32_t ngkmax,
+                   int32_t* ngp, int32_t* igpig, double* vgpl, double* vgpc, double* gpc, double* tpgpc);
+/* The same into device arrays, asynchronous on the handle's stream (vpl and
+ * vpc are host arrays of three): *d_ngp (device) receives the count,
+ * negated when it exceeds ngkmax. */
+int excfv_gengpvec_dev(excfv_handle* h, const double* vpl, const double* vpc, double gkmax, int32_t ngkmax,
+                       int32_t* d_ngp, int32_t* igpig, double* vgpl, double* vgpc, double* gpc, double* tpgpc);
+/* gensfacgp (src/gensfacgp.f90:10): sfacgp(ld, natmtot) complex,
+ * sfacgp(igp, ias) = exp(i (G+k) . r_ias) for igp < ngp; host arrays
+ * (rows past ngp are zeroed) or device arrays (_dev, asynchronous, rows past
+ * ngp untouched). */
+int excfv_gensfacgp(excfv_handle* h, int32_t ngp, const double* vgpc, int32_t ld, double* sfacgp);
+int excfv_gensfacgp_dev(excfv_handle* h, int32_t ngp, const double* vgpc, int32_t ld, double* sfacgp);
+
+/* ---- EVECFV records (src/writers/putevecfv.f90, src/read/getevecfv.f90) --- */
+
+/* The reference's EVECFV file: Fortran unformatted direct access, one record
+ * per k-point (ik 1-based) at byte offset (ik - 1) * recl, recl = 36 + 16
+ * nmatmax nstfv nspnfv, no record markers, native byte order:
+ * vkl(3) real(8), nmatmax, nstfv, nspnfv int(4), evecfv(nmatmax, nstfv,
+ * nspnfv) complex(8).  path is the file (EVECFV.OUT in the reference);
+ * excfv_putevecfv creates it when missing.  evecfv is a host array; the _dev
+ * form takes a device array (staged through the handle's pinned buffer).
+ * excfv_getevecfv returns EXCFV_ERR_ARG, with a message, where the reference
+ * stops: a missing record, differing nmatmax / nstfv / nspnfv, or a k-point
+ * whose |dvkl|_1 exceeds 1e-6 (vkl may be null to skip that check). */
+int excfv_putevecfv(const char* path, int32_t ik, const double* vkl, int32_t nmatmax, int32_t nstfv,
+                    int32_t nspnfv, const double* evecfv);
+int excfv_putevecfv_dev(excfv_handle* h, const char* path, int32_t ik, const double* vkl, int32_t nmatmax,
+                        int32_t nstfv, int32_t nspnfv, const double* d_evecfv);
+int excfv_getevecfv(const char* path, int32_t ik, const double* vkl, int32_t nmatmax, int32_t nstfv,
+                    int32_t nspnfv, double* evecfv);
+
 /* Tridiagonal reduction of the FP64 form (the ZHETRD step of ZHEGVX,
  * external/LAPACK/zheevx.f:441).  EXCFV_REDUCTION_AUTO (default) and
  * EXCFV_REDUCTION_ONE_STAGE: the one-stage Householder panels (the faster

@@ -12,6 +12,8 @@ Each function follows one reference routine:
 ``solvewithlapack``    ``src/src_eigensystem/modfvsystem.f90:668-711`` (ZHEGVX)
 ``seceqnfv``           ``src/seceqnfv.f90:69-90``
 ``seceqn``             ``src/seceqn.f90:57-64`` (match + seceqnfv, one spin)
+``gengpvec``           ``src/gengpvec.f90:43-68`` (G+k set; ``sphcrd``)
+``gensfacgp``          ``src/gensfacgp.f90:40-53`` (structure factors)
 =====================  ======================================================
 
 Matrices use 0-based indices; the reference's 1-based ``idxlo`` values are
@@ -36,6 +38,61 @@ FOURPI = 4.0 * math.pi
 def idxlm(l: int, m: int) -> int:
     """0-based packed (l, m) index: l(l+1)+m."""
     return l * (l + 1) + m
+
+
+# ---------------------------------------------------------------------------
+# G+k set and structure factors
+# ---------------------------------------------------------------------------
+
+def sphcrd(v: np.ndarray) -> Tuple[float, np.ndarray]:
+    """Length and (theta, phi) of a Cartesian vector (``src/src_lib/sphcrd.f90``):
+    phi in [0, 2 pi), both angles 0 below |v| = 1e-14, phi 0 on the z axis."""
+    eps = 1e-14
+    r = math.sqrt(float(v[0]) ** 2 + float(v[1]) ** 2 + float(v[2]) ** 2)
+    tp = np.zeros(2)
+    if r > eps:
+        t1 = float(v[2]) / r
+        t1 = min(t1, 1.0) if t1 > 0.0 else max(t1, -1.0)
+        tp[0] = math.acos(t1)
+        if abs(float(v[0])) > eps or abs(float(v[1])) > eps:
+            tp[1] = math.atan2(float(v[1]), float(v[0]))
+            if tp[1] < 0.0:
+                tp[1] += 2.0 * math.pi
+    return r, tp
+
+
+def gengpvec(vgc: np.ndarray, ivg: np.ndarray, ngvec: int, vpl: np.ndarray, vpc: np.ndarray,
+             gkmax: float, ngkmax: int):
+    """G+k vectors with |G+k| < gkmax, in G order (``src/gengpvec.f90:43-68``).
+
+    Returns ngp and igpig (1-based), vgpl, vgpc (3, ngkmax), gpc, tpgpc (2, ngkmax)."""
+    t1 = gkmax ** 2
+    igpig = np.zeros(ngkmax, dtype=np.int32)
+    vgpl = np.zeros((3, ngkmax), order="F")
+    vgpc = np.zeros((3, ngkmax), order="F")
+    gpc = np.zeros(ngkmax)
+    tpgpc = np.zeros((2, ngkmax), order="F")
+    igp = 0
+    for ig in range(ngvec):
+        v = vgc[:, ig] + vpc
+        t2 = v[0] ** 2 + v[1] ** 2 + v[2] ** 2
+        if t2 < t1:
+            if igp >= ngkmax:
+                raise ValueError("number of G+p-vectors exceeds ngkmax")
+            igpig[igp] = ig + 1
+            vgpl[:, igp] = ivg[:, ig].astype(np.float64) + vpl
+            vgpc[:, igp] = v
+            gpc[igp], tpgpc[:, igp] = sphcrd(v)
+            igp += 1
+    return igp, igpig, vgpl, vgpc, gpc, tpgpc
+
+
+def gensfacgp(ngp: int, vgpc: np.ndarray, atposc: np.ndarray, ld: int) -> np.ndarray:
+    """Structure factors exp(i (G+k).r_a) (``src/gensfacgp.f90:40-53``), (ld, natmtot)."""
+    out = np.zeros((ld, atposc.shape[1]), dtype=np.complex128, order="F")
+    t1 = vgpc[:, :ngp].T @ atposc
+    out[:ngp] = np.cos(t1) + 1j * np.sin(t1)
+    return out
 
 
 # ---------------------------------------------------------------------------
