@@ -7,8 +7,9 @@
 One step = one k-point through ``seceqn`` (match, hamiltonsetup, overlapsetup,
 ZHEGVX-equivalent eigensolve for the lowest nstfv states).  Prints one JSON
 line (rank 0).  N > 1: one process per GPU (torchrun), every rank solves its
-own k-point (weak scaling, no data-path collective); the timing is the
-maximum over ranks.
+own k-point (weak scaling) and the eigenvalues are all-gathered on the
+device inside the step, as the reference's exchange after the k-loop; the
+timing is the maximum over ranks.
 
 ``value``: k-points/s with the k-point inputs resident in HBM, CUDA events on
 the library's stream, L2 flushed (512 MB write) between steps outside the
@@ -179,6 +180,7 @@ def load_traffic():
 # ---------------------------------------------------------------------------
 
 def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn, prec):
+    from exciting_b200 import kpar
     from exciting_b200.fv import FirstVariational
     from exciting_b200.lib import EXCFV_PREC_MIXED
     import torch.distributed as dist
@@ -221,6 +223,8 @@ def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn, prec)
                 s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 s.record(stream)
                 fvb.seceqn_batched_dev(*bargs)
+                if world > 1:   # every rank's batch eigenvalues to every rank
+                    kpar.gather_evals_device(torch.stack(ev), [nk] * world)
                 e.record(stream)
                 e.synchronize()
                 t_ += s.elapsed_time(e)
@@ -420,8 +424,14 @@ def main():
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     torch.cuda.synchronize()
 
+    from exciting_b200 import kpar
+
     def step_dev():
         fv.seceqn_dev(n, kp.ngp, kp.ngkmax, ptrs, nmatmax, d_eval.data_ptr(), d_evec.data_ptr())
+        if world > 1:
+            # the eigenvalue exchange after the k-loop (scf_cycle.f90:298), on
+            # the device and inside the timed step
+            kpar.gather_evals_device(d_eval.view(1, k), [1] * world)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -632,7 +642,9 @@ def main():
         "mixed_single_k": mixed_single,
         "config": {"workload": workload_desc(args.workload, p), "form": "plain FP64",
                    "l2": "flushed between steps (512 MB write, outside the timed events)",
-                   "parallelism": f"k-points over {world} GPU(s), no data-path collective",
+                   "parallelism": (f"k-points over {world} GPU(s): one k-point per rank per step, "
+                                   "eigenvalues all-gathered on the device inside the step"
+                                   if world > 1 else "one GPU"),
                    "stage_ms_per_step": stages, "fp64_tensor_peak_tflops": zpeak,
                    "setup_gemm_tflops": g_ach, "trd_panel_gbs": p_ach,
                    "lowest_eigenvalues": [float(x) for x in ev_host[:3]]},

@@ -89,3 +89,57 @@ def gather_evals(local: np.ndarray, counts: Sequence[int], nstfv: int, group=Non
     dist.all_gather(parts, buf, group=group)
     rows = [parts[r][:counts[r]].cpu().numpy() for r in range(world)]
     return np.concatenate(rows, axis=0) if rows else np.zeros((0, nstfv))
+
+
+def gather_evals_device(local, counts: Sequence[int], group=None):
+    """``gather_evals`` without leaving the device: ``local`` is a (nk_local,
+    nstfv) float64 tensor on this rank's device (NCCL) or the CPU (gloo); the
+    result is (sum(counts), nstfv) on the same device.  Stream-ordered, so it
+    can sit inside a CUDA-event timed region."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    nstfv = local.shape[1]
+    mx = max(counts)
+    buf = torch.zeros((mx, nstfv), dtype=torch.float64, device=local.device)
+    if counts[rank]:
+        buf[:counts[rank]] = local[:counts[rank]]
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf, group=group)
+    return torch.cat([parts[r][:counts[r]] for r in range(world)], dim=0)
+
+
+class KpointRankLost(RuntimeError):
+    """A rank of the k-point loop did not reach the eigenvalue exchange."""
+
+
+def run_kloop(solve_block, costs: Sequence[float], nstfv: int, group=None, balanced: bool = True):
+    """The k-point loop of one SCF iteration over ranks (``src/scf_cycle.f90:255-299``).
+
+    Rank r solves its contiguous block of k-points (``balanced_split`` by
+    ``costs``, e.g. nmat^3 for uneven basis sizes, or the reference's
+    ``block_split``) with ``solve_block(lo, hi) -> (hi - lo, nstfv)`` array of
+    eigenvalues (on GPUs the batched entry of libexcfv over that block), then
+    the eigenvalues of all k-points are all-gathered, as the reference's
+    mpi_allgatherv after the loop.  Eigenvectors stay where they were computed.
+    A rank that leaves before the exchange makes the others raise
+    ``KpointRankLost`` once the process group's timeout runs out, instead of
+    waiting for good.  Returns (all eigenvalues, this rank's (lo, hi)).
+    """
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    nk = len(costs)
+    split = balanced_split(costs, world) if balanced else block_split(nk, world)
+    lo, hi = split[rank]
+    local = np.asarray(solve_block(lo, hi), dtype=np.float64).reshape(hi - lo, nstfv)
+    counts = [b - a for a, b in split]
+    try:
+        allw = gather_evals(local, counts, nstfv, group=group)
+    except Exception as e:  # a lost peer surfaces as a timed-out or broken collective
+        raise KpointRankLost(f"rank {rank}: eigenvalue exchange of the k-point loop failed "
+                             f"({type(e).__name__}: {e})") from e
+    return allw, (lo, hi)

@@ -107,3 +107,67 @@ def test_lost_rank_is_reported_not_hung():
     for p in procs:
         p.join(timeout=60)
     assert msg != "no error"
+
+
+def _driver_worker(rank, world, port, q, die_before_exchange):
+    import torch.distributed as dist
+    from datetime import timedelta
+    from exciting_b200 import synthetic as syn
+    from oracle import fvref
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=8))
+    p = syn.make_problem("diamond2", nk=5, ngk_range=(40, 70), nstfv=4)
+    costs = [float(k.nmat) ** 3 for k in p.kpts]
+
+    def solve_block(lo, hi):
+        if die_before_exchange and rank == 1:
+            os._exit(3)              # leaves between steps, nothing in flight
+        return [fvref.seceqn(p.static, p.kpts[i])[0] for i in range(lo, hi)]
+
+    try:
+        allw, (lo, hi) = kpar.run_kloop(solve_block, costs, 4)
+        q.put((rank, "ok", allw, (lo, hi)))
+        dist.barrier()
+        dist.destroy_process_group()
+    except kpar.KpointRankLost as e:
+        q.put((rank, "lost", str(e), None))
+
+
+def _run_driver(die):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_driver_worker, args=(r, 2, port, q, die)) for r in range(2)]
+    for p in procs:
+        p.start()
+    n_expect = 1 if die else 2
+    res = [q.get(timeout=180) for _ in range(n_expect)]
+    for p in procs:
+        p.join(timeout=60)
+    return res, procs
+
+
+def test_kloop_driver_balanced_split_and_exchange():
+    """Uneven k-points split by nmat^3 over two ranks; every rank ends with all
+    eigenvalues in k order, equal to a sequential oracle loop."""
+    res, procs = _run_driver(False)
+    assert all(p.exitcode == 0 for p in procs)
+    from exciting_b200 import synthetic as syn
+    from oracle import fvref
+    prob = syn.make_problem("diamond2", nk=5, ngk_range=(40, 70), nstfv=4)
+    ref = np.array([fvref.seceqn(prob.static, k)[0] for k in prob.kpts])
+    spans = sorted(r[3] for r in res)
+    assert spans[0][0] == 0 and spans[-1][1] == 5 and spans[0][1] == spans[1][0]
+    for rank, status, allw, _ in res:
+        assert status == "ok"
+        assert np.allclose(allw, ref, atol=1e-12)
+
+
+def test_kloop_driver_reports_a_lost_rank():
+    """Rank 1 exits after its block, before the exchange: rank 0 raises
+    KpointRankLost once the group's timeout runs out, instead of hanging."""
+    res, procs = _run_driver(True)
+    assert res[0][0] == 0 and res[0][1] == "lost"
+    assert "eigenvalue exchange" in res[0][2]
+    assert procs[1].exitcode == 3
