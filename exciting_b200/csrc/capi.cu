@@ -141,7 +141,7 @@ int stage_set_static(excfv_handle* h, const excfv_static* s) {
   h->have_static = false;
   if (!s || s->natmtot <= 0 || s->nspecies <= 0 || s->lmaxapw < 0 || s->apwordmax <= 0 ||
       s->maxaa <= 0 || s->ngvec <= 0 || s->ngrtot < s->ngvec || s->nstfv <= 0 || !s->idxis ||
-      !s->rmt || !s->apword || !s->aa || !s->ivg || !s->ivgig || !s->veffig || !s->cfunig ||
+      !s->rmt || !s->apword || !s->ivg || !s->ivgig || !s->veffig || !s->cfunig ||
       !s->sprwin || !s->apwfrwin || s->npmatch <= 0) {
     excfv_set_error("excfv_set_static: missing or inconsistent arguments");
     return EXCFV_ERR_ARG;
@@ -196,8 +196,7 @@ int stage_set_static(excfv_handle* h, const excfv_static* s) {
   std::vector<int> lo_atom(std::max(1, st.nlotot), -1), lo_local(std::max(1, st.nlotot), -1);
   std::vector<int> lo_lm((size_t)std::max(1, st.maxnlo) * na, -1), lo_ilo((size_t)std::max(1, st.maxnlo) * na, -1);
   if (st.nlotot > 0) {
-    if (!s->nlorb || !s->lorbl || !s->idxlo || !s->losize || !s->loa || !s->lolo || !s->oalo ||
-        !s->ololo) {
+    if (!s->nlorb || !s->lorbl || !s->idxlo || !s->losize) {
       excfv_set_error("excfv_set_static: local-orbital arrays missing");
       return EXCFV_ERR_ARG;
     }
@@ -244,8 +243,9 @@ int stage_set_static(excfv_handle* h, const excfv_static* s) {
   const size_t nololo = (size_t)std::max(1, st.nlomax) * std::max(1, st.nlomax) * na;
   std::vector<double> oalo(noalo, 0.0), ololo(nololo, 0.0);
   if (st.nlotot > 0) {
-    for (size_t i = 0; i < noalo; ++i) oalo[i] = s->oalo[i] + (s->h1loa ? s->h1loa[i] : 0.0);
-    for (size_t i = 0; i < nololo; ++i) ololo[i] = s->ololo[i] + (s->h1lolo ? s->h1lolo[i] : 0.0);
+    for (size_t i = 0; i < noalo; ++i) oalo[i] = (s->oalo ? s->oalo[i] : 0.0) + (s->h1loa ? s->h1loa[i] : 0.0);
+    for (size_t i = 0; i < nololo; ++i)
+      ololo[i] = (s->ololo ? s->ololo[i] : 0.0) + (s->h1lolo ? s->h1lolo[i] : 0.0);
   }
   st.have_h1aa = false;
   const size_t nh1 = (size_t)st.apwordmax * st.apwordmax * L1 * na;
@@ -260,6 +260,16 @@ int stage_set_static(excfv_handle* h, const excfv_static* s) {
   }
   const size_t nbox = (size_t)e1 * e2 * e3;
   const size_t maxnlo1 = std::max(1, st.maxnlo);
+  st.h_idxis = idxis;
+  st.h_apword.assign(s->apword, s->apword + (size_t)L1 * ns);
+  st.h_nlorb.assign(ns, 0);
+  st.h_lorbl.assign((size_t)std::max(1, st.nlomax) * ns, 0);
+  if (s->nlorb && s->lorbl)
+    for (int is = 0; is < ns; ++is) {
+      st.h_nlorb[is] = s->nlorb[is];
+      for (int ilo = 0; ilo < s->nlorb[is] && ilo < st.nlomax; ++ilo)
+        st.h_lorbl[ilo + (size_t)std::max(1, st.nlomax) * is] = s->lorbl[ilo + (size_t)st.nlomax * is];
+    }
   if ((rc = upload(&st.idxis, idxis.data(), na))) return rc;
   if ((rc = upload(&st.rmt, s->rmt, ns))) return rc;
   if ((rc = upload(&st.apword, s->apword, (size_t)L1 * ns))) return rc;
@@ -272,6 +282,7 @@ int stage_set_static(excfv_handle* h, const excfv_static* s) {
   if ((rc = upload(&st.aa, s->aa, (size_t)st.maxaa * st.maxaa * na))) return rc;
   if ((rc = upload(&st.loa, st.nlotot ? s->loa : nullptr, maxnlo1 * st.maxaa * na))) return rc;
   if ((rc = upload(&st.lolo, st.nlotot ? s->lolo : nullptr, maxnlo1 * maxnlo1 * na))) return rc;
+  // upload(nullptr) zero-fills: a NULL aa / loa / lolo waits for excfv_hmlint
   if ((rc = upload(&st.oalo, oalo.data(), noalo))) return rc;
   if ((rc = upload(&st.ololo, ololo.data(), nololo))) return rc;
   if (st.have_h1aa && (rc = upload(&st.h1aa, s->h1aa, nh1))) return rc;
@@ -443,6 +454,17 @@ int excfv_set_static(excfv_handle* h, const excfv_static* s) {
   if (!h) return EXCFV_ERR_ARG;
   DeviceGuard g(h->device);
   return stage_set_static(h, s);
+}
+
+int excfv_hmlint(excfv_handle* h, const excfv_mtrad* r, double* aa, double* loa, double* lolo, double* oalo,
+                 double* ololo) {
+  if (!h || !r) return EXCFV_ERR_ARG;
+  if (!h->have_static) {
+    excfv_set_error("excfv_set_static must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  DeviceGuard g(h->device);
+  return stage_hmlint(h, r, aa, loa, lolo, oalo, ololo);
 }
 
 static int check_k(excfv_handle* h, int nmatp, int ngp, int ngkmax) {

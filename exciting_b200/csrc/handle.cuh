@@ -17,6 +17,9 @@ struct DevStatic {
   int nstfv = 0;
   double evaltol = 0.0;
   bool have_h1aa = false;
+  // host copies for the muffin-tin build: 0-based species, nlorb, lorbl
+  // (stride max(1, nlomax)), apword
+  std::vector<int> h_idxis, h_nlorb, h_lorbl, h_apword;
   // device arrays
   int* idxis = nullptr;     // (natmtot) 0-based species
   double* rmt = nullptr;    // (nspecies)
@@ -168,6 +171,9 @@ void prof_collect(excfv_handle* h);
 // ---- stages (each enqueues work on h->stream) ------------------------------
 int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax);
 int stage_set_static(excfv_handle* h, const excfv_static* s);
+// olprad + hmlint on the device (mtbuild.cu)
+int stage_hmlint(excfv_handle* h, const excfv_mtrad* r, double* aa_out, double* loa_out, double* lolo_out,
+                 double* oalo_out, double* ololo_out);
 void free_static(DevStatic& st);
 void free_workspace(Workspace& ws);
 

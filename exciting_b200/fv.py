@@ -19,7 +19,7 @@ there is no CPU path.
 from __future__ import annotations
 
 import ctypes as C
-from typing import Tuple
+from typing import Optional, Tuple
 
 import numpy as np
 
@@ -158,6 +158,45 @@ class FirstVariational:
         s.evaltol = float(st.evaltol)
         self._check(self._L.excfv_set_static(self._h, C.byref(s)), "excfv_set_static")
         self.static = st
+
+    def hmlint(self, rad, outputs: bool = True) -> Optional[dict]:
+        """``olprad`` + ``hmlint(mt_hscf)`` on the device (``src/scf_cycle.f90:212-222``):
+        rebuilds the handle's aa / loa / lolo / oalo / ololo (and the IORA* h1
+        terms) from the radial data ``rad`` (lmaxvr, nrmt, spr, apwfr, lofr,
+        veffmt in the reference layouts).  With ``outputs`` returns the host
+        copies {aa, loa, lolo, oalo, ololo}."""
+        st = self.static
+        keep = []
+
+        def f64(a):
+            if a is None:
+                return None
+            x = _f(a, np.float64)
+            keep.append(x)
+            return x.ctypes.data_as(_lib._f64p)
+
+        nrmt = _f(rad.nrmt, np.int32)
+        r = _lib.ExcfvMtrad()
+        r.lmaxvr = int(rad.lmaxvr)
+        r.nrmtmax = int(np.asarray(rad.spr).shape[0])
+        r.nrmt = nrmt.ctypes.data_as(_lib._i32p)
+        r.spr = f64(rad.spr)
+        r.apwfr = f64(rad.apwfr)
+        r.lofr = f64(rad.lofr) if st.nlotot > 0 else None
+        r.veffmt = f64(rad.veffmt)
+        out = None
+        ptrs = [None] * 5
+        if outputs:
+            nlo1 = max(st.maxnlo, 1)
+            nlm = max(st.nlomax, 1)
+            out = {"aa": np.zeros((st.maxaa, st.maxaa, st.natmtot), dtype=np.complex128, order="F"),
+                   "loa": np.zeros((nlo1, st.maxaa, st.natmtot), dtype=np.complex128, order="F"),
+                   "lolo": np.zeros((nlo1, nlo1, st.natmtot), dtype=np.complex128, order="F"),
+                   "oalo": np.zeros((st.apwordmax, nlm, st.natmtot), order="F"),
+                   "ololo": np.zeros((nlm, nlm, st.natmtot), order="F")}
+            ptrs = [_ptr(out[k]) for k in ("aa", "loa", "lolo", "oalo", "ololo")]
+        self._check(self._L.excfv_hmlint(self._h, C.byref(r), *ptrs), "excfv_hmlint")
+        return out
 
     def reserve(self, nmatmax: int, ngkmax: int) -> None:
         self._check(self._L.excfv_reserve(self._h, nmatmax, ngkmax), "excfv_reserve")

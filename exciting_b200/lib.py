@@ -49,6 +49,14 @@ class ExcfvStatic(C.Structure):
     ]
 
 
+class ExcfvMtrad(C.Structure):
+    """Mirror of ``struct excfv_mtrad`` (field order and types must match)."""
+    _fields_ = [
+        ("lmaxvr", C.c_int32), ("nrmtmax", C.c_int32), ("nrmt", _i32p), ("spr", _f64p),
+        ("apwfr", _f64p), ("lofr", _f64p), ("veffmt", _f64p),
+    ]
+
+
 #: name -> (restype, argtypes); every symbol declared in include/excfv.h
 SIGNATURES = {
     "excfv_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -59,6 +67,8 @@ SIGNATURES = {
     "excfv_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "excfv_reserve": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "excfv_set_static": (C.c_int, [C.c_void_p, C.POINTER(ExcfvStatic)]),
+    "excfv_hmlint": (C.c_int, [C.c_void_p, C.POINTER(ExcfvMtrad), C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.c_void_p, C.c_void_p]),
     "excfv_match": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                               C.c_void_p, C.c_void_p]),
     "excfv_hamiltonandoverlapsetup": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32,

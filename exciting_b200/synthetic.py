@@ -530,3 +530,81 @@ def make_problem(name: str, *, seed: Optional[int] = None, nk: int = 1,
         k.nmat = k.ngp + st.nlotot
     nmatmax = max(k.nmat for k in kpts)
     return Problem(name=name, static=st, kpts=kpts, nmatmax=nmatmax, ngkmax=ngkmax)
+
+
+# ---------------------------------------------------------------------------
+# radial data of the muffin-tin Hamiltonian build
+# ---------------------------------------------------------------------------
+
+def make_radial(st: "Static", *, seed: int = 4242, nrmt: int = 200, lmaxvr: int = 6, sprmin: float = 1e-5):
+    """Seeded radial data for the per-SCF-iteration MT build (hmlint / olprad).
+
+    A logarithmic mesh from ``sprmin`` to R_MT per species; APW and LO radial
+    functions u(r) = r^l exp(-a r) (1 + b r) and their exact derivatives
+    (smooth and regular at the origin), the APW functions of each (atom, l)
+    orthonormalised and the local orbitals normalised; an effective potential
+    with V_00 y00 = -Z/r + c (Z = 6) and small smooth higher-lm terms.
+    Returns an ``oracle.mtham.Radial``-compatible object, and updates the
+    static's match window (sprwin, apwfrwin) to the same radial functions.
+    """
+    import types
+    rng = np.random.default_rng(seed)
+    nsp = st.nspecies
+    lmmaxvr = (lmaxvr + 1) ** 2
+    spr = np.zeros((nrmt, nsp), order="F")
+    for is_ in range(nsp):
+        spr[:, is_] = sprmin * np.exp(np.arange(nrmt) * math.log(st.rmt[is_] / sprmin) / (nrmt - 1))
+    apwfr = np.zeros((nrmt, 2, st.apwordmax, st.lmaxapw + 1, st.natmtot), order="F")
+    lofr = np.zeros((nrmt, 2, max(st.nlomax, 1), st.natmtot), order="F")
+    veffmt = np.zeros((lmmaxvr, nrmt, st.natmtot), order="F")
+
+    def radf(r, l, a, b):
+        # u = r^l exp(-a r)(1 + b r), u' = (l/r - a) u + r^l exp(-a r) b
+        e = np.exp(-a * r) * r ** l
+        u = e * (1.0 + b * r)
+        du = (l / r - a) * u + e * b if l > 0 else -a * u + e * b
+        return u, du
+
+    Y00 = 0.28209479177387814347
+    for ias in range(st.natmtot):
+        is_ = int(st.idxis[ias])
+        r = spr[:, is_]
+        for l in range(st.lmaxapw + 1):
+            for io in range(int(st.apword[l, is_])):
+                a = 0.6 + 0.15 * io + 0.02 * l + 0.05 * rng.uniform()
+                b = 0.3 * rng.uniform() - 0.1 * io
+                apwfr[:, 0, io, l, ias], apwfr[:, 1, io, l, ias] = radf(r, l, a, b)
+        for ilo in range(int(st.nlorb[is_])):
+            l = int(st.lorbl[ilo, is_])
+            a = 1.1 + 0.2 * ilo + 0.05 * rng.uniform()
+            b = 0.5 * rng.uniform() - 0.25
+            lofr[:, 0, ilo, ias], lofr[:, 1, ilo, ias] = radf(r, l, a, b)
+        veffmt[0, :, ias] = (-6.0 / r + 0.3 + 0.1 * rng.uniform()) / Y00
+        for lm in range(1, lmmaxvr):
+            l = int(math.isqrt(lm))
+            veffmt[lm, :, ias] = 0.2 * rng.standard_normal() * r ** l * np.exp(-1.5 * r)
+    # orthonormal APW functions per (atom, l) and normalised local orbitals,
+    # as genapwfr / genlofr leave them (inner product: trapezoid in r with r^2)
+    for ias in range(st.natmtot):
+        r = spr[:, int(st.idxis[ias])]
+        wr = np.zeros(nrmt)
+        dr = np.diff(r)
+        wr[:-1] += 0.5 * dr
+        wr[1:] += 0.5 * dr
+        wr *= r * r
+        for l in range(st.lmaxapw + 1):
+            for io in range(int(st.apword[l, int(st.idxis[ias])])):
+                for jo in range(io):
+                    c = np.dot(wr, apwfr[:, 0, io, l, ias] * apwfr[:, 0, jo, l, ias])
+                    apwfr[:, :, io, l, ias] -= c * apwfr[:, :, jo, l, ias]
+                nrm = math.sqrt(np.dot(wr, apwfr[:, 0, io, l, ias] ** 2))
+                apwfr[:, :, io, l, ias] /= nrm
+        for ilo in range(int(st.nlorb[int(st.idxis[ias])])):
+            nrm = math.sqrt(np.dot(wr, lofr[:, 0, ilo, ias] ** 2))
+            lofr[:, :, ilo, ias] /= nrm
+    # the match window follows the same radial functions
+    npm = st.npmatch
+    st.sprwin = np.asfortranarray(spr[nrmt - npm:, :])
+    st.apwfrwin = np.asfortranarray(apwfr[nrmt - npm:, 0, :, :, :])
+    return types.SimpleNamespace(lmaxvr=lmaxvr, nrmt=np.full(nsp, nrmt, dtype=np.int32), spr=spr,
+                                 apwfr=apwfr, lofr=lofr, veffmt=veffmt, nrmtmax=nrmt)

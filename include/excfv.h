@@ -189,8 +189,38 @@ int excfv_set_stream(excfv_handle* h, void* stream);
  * newsystem, src/seceqnfv.f90:74).  Called implicitly when needed. */
 int excfv_reserve(excfv_handle* h, int32_t nmatmax, int32_t ngkmax);
 
-/* Uploads the per-SCF-iteration data (replaces module globals). */
+/* Uploads the per-SCF-iteration data (replaces module globals).  aa, loa,
+ * lolo, oalo and ololo may be NULL (zero) when excfv_hmlint builds them. */
 int excfv_set_static(excfv_handle* h, const excfv_static* s);
+
+/* ---- the muffin-tin Hamiltonian build (once per SCF iteration) ---------- */
+
+/* Radial data of olprad and hmlint (module data in the reference: spr and
+ * nrmt of mod_muffin_tin, apwfr and lofr of mod_APW_LO, veffmt of
+ * mod_potential_and_density).  Host pointers, read during the call. */
+typedef struct excfv_mtrad {
+  int32_t lmaxvr;          /* input%groundstate%lmaxvr (<= 20); lmmaxvr = (lmaxvr+1)^2 */
+  int32_t nrmtmax;
+  const int32_t* nrmt;     /* (nspecies) radial points of each species (3..nrmtmax) */
+  const double* spr;       /* (nrmtmax, nspecies) radial mesh */
+  const double* apwfr;     /* (nrmtmax, 2, apwordmax, 0:lmaxapw, natmtot): u and du/dr */
+  const double* lofr;      /* (nrmtmax, 2, nlomax, natmtot), NULL without local orbitals */
+  const double* veffmt;    /* (lmmaxvr, nrmtmax, natmtot) real-harmonic coefficients */
+} excfv_mtrad;
+
+/* olprad (src/src_eigensystem/olprad.f90:13) and hmlint(mt_hscf)
+ * (src/src_eigensystem/hmlint.f90:14: mt_kin + mt_pot), in the order
+ * src/scf_cycle.f90:212-222 calls them, on the device: every radial integral
+ * (spline integral of fderiv(-1) over the species mesh), the Gaunt
+ * contraction over the lm of veffmt, into the handle's aa, loa, lolo, oalo,
+ * ololo (and, when h1on, h1aa with h1loa and h1lolo folded into oalo and
+ * ololo), replacing what excfv_set_static uploaded.  Optional host copies
+ * (NULL skips): aa complex (maxaa, maxaa, natmtot), loa complex (maxnlo,
+ * maxaa, natmtot), lolo complex (maxnlo, maxnlo, natmtot), oalo (apwordmax,
+ * nlomax, natmtot), ololo (nlomax, nlomax, natmtot), the last two without
+ * the IORA* terms, as olprad leaves them.  Synchronous. */
+int excfv_hmlint(excfv_handle* h, const excfv_mtrad* r, double* aa, double* loa, double* lolo, double* oalo,
+                 double* ololo);
 
 /* ---- the hot path ------------------------------------------------------ */
 
