@@ -467,6 +467,43 @@ int excfv_hmlint(excfv_handle* h, const excfv_mtrad* r, double* aa, double* loa,
   return stage_hmlint(h, r, aa, loa, lolo, oalo, ololo);
 }
 
+int excfv_genveffig(excfv_handle* h, const int32_t* ngrid, const double* veffir, const double* cfunir,
+                    double* veffig) {
+  if (!h || !ngrid || !veffir || !cfunir) return EXCFV_ERR_ARG;
+  if (!h->have_static) {
+    excfv_set_error("excfv_set_static must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  DeviceGuard g(h->device);
+  const int kinds[1] = {0};
+  cplx* dst[1] = {h->st.veffig};
+  cplx* out[1] = {reinterpret_cast<cplx*>(veffig)};
+  return stage_genfig(h, ngrid, veffir, cfunir, 1, kinds, dst, out);
+}
+
+int excfv_genmeffig(excfv_handle* h, const int32_t* ngrid, const double* veffir, const double* cfunir,
+                    double* meffig, double* m2effig) {
+  if (!h || !ngrid || !veffir || !cfunir) return EXCFV_ERR_ARG;
+  if (!h->have_static) {
+    excfv_set_error("excfv_set_static must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  DeviceGuard g(h->device);
+  // meffig only with valence relativity, m2effig only for IORA* (genmeffig.f90:34,45)
+  int kinds[2];
+  cplx* dst[2];
+  cplx* out[2];
+  int nk = 0;
+  if (h->st.vrel != 0) {
+    kinds[nk] = 1; dst[nk] = h->st.xig; out[nk] = reinterpret_cast<cplx*>(meffig); ++nk;
+  }
+  if (h->st.h1on) {
+    kinds[nk] = 2; dst[nk] = h->st.m2effig; out[nk] = reinterpret_cast<cplx*>(m2effig); ++nk;
+  }
+  if (nk == 0) return EXCFV_OK;
+  return stage_genfig(h, ngrid, veffir, cfunir, nk, kinds, dst, out);
+}
+
 static int check_k(excfv_handle* h, int nmatp, int ngp, int ngkmax) {
   if (!h) return EXCFV_ERR_ARG;
   if (!h->have_static) {

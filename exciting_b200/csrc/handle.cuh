@@ -171,6 +171,10 @@ void prof_collect(excfv_handle* h);
 // ---- stages (each enqueues work on h->stream) ------------------------------
 int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax);
 int stage_set_static(excfv_handle* h, const excfv_static* s);
+// genveffig / genmeffig on the device (interstitial.cu): kinds 0 veffig,
+// 1 meffig, 2 m2effig into dst[q] (device, ngvec), optional host copies
+int stage_genfig(excfv_handle* h, const int* ngrid, const double* veffir, const double* cfunir, int nkinds,
+                 const int* kinds, cplx* const* dst, cplx* const* host_out);
 // olprad + hmlint on the device (mtbuild.cu)
 int stage_hmlint(excfv_handle* h, const excfv_mtrad* r, double* aa_out, double* loa_out, double* lolo_out,
                  double* oalo_out, double* ololo_out);

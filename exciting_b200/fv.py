@@ -159,6 +159,29 @@ class FirstVariational:
         self._check(self._L.excfv_set_static(self._h, C.byref(s)), "excfv_set_static")
         self.static = st
 
+    def genveffig(self, ngrid, veffir, cfunir) -> np.ndarray:
+        """``genveffig`` on the device (``src/genveffig.f90``): replaces the
+        handle's veffig and returns it (complex (ngvec))."""
+        ng = _f(ngrid, np.int32)
+        v = _f(veffir, np.float64)
+        c = _f(cfunir, np.float64)
+        out = np.zeros(self.static.ngvec, dtype=np.complex128)
+        self._check(self._L.excfv_genveffig(self._h, _ptr(ng), _ptr(v), _ptr(c), _ptr(out)), "excfv_genveffig")
+        return out
+
+    def genmeffig(self, ngrid, veffir, cfunir) -> Tuple[np.ndarray, np.ndarray]:
+        """``genmeffig`` on the device (``src/genmeffig.f90``): replaces the
+        handle's meffig (valence relativity) and m2effig (IORA*) and returns
+        them (zeros where the reference computes nothing)."""
+        ng = _f(ngrid, np.int32)
+        v = _f(veffir, np.float64)
+        c = _f(cfunir, np.float64)
+        m1 = np.zeros(self.static.ngvec, dtype=np.complex128)
+        m2 = np.zeros(self.static.ngvec, dtype=np.complex128)
+        self._check(self._L.excfv_genmeffig(self._h, _ptr(ng), _ptr(v), _ptr(c), _ptr(m1), _ptr(m2)),
+                    "excfv_genmeffig")
+        return m1, m2
+
     def hmlint(self, rad, outputs: bool = True) -> Optional[dict]:
         """``olprad`` + ``hmlint(mt_hscf)`` on the device (``src/scf_cycle.f90:212-222``):
         rebuilds the handle's aa / loa / lolo / oalo / ololo (and the IORA* h1

@@ -67,6 +67,9 @@ SIGNATURES = {
     "excfv_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
     "excfv_reserve": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "excfv_set_static": (C.c_int, [C.c_void_p, C.POINTER(ExcfvStatic)]),
+    "excfv_genveffig": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "excfv_genmeffig": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p]),
     "excfv_hmlint": (C.c_int, [C.c_void_p, C.POINTER(ExcfvMtrad), C.c_void_p, C.c_void_p, C.c_void_p,
                                C.c_void_p, C.c_void_p]),
     "excfv_match": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,

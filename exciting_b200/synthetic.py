@@ -608,3 +608,35 @@ def make_radial(st: "Static", *, seed: int = 4242, nrmt: int = 200, lmaxvr: int 
     st.apwfrwin = np.asfortranarray(apwfr[nrmt - npm:, 0, :, :, :])
     return types.SimpleNamespace(lmaxvr=lmaxvr, nrmt=np.full(nsp, nrmt, dtype=np.int32), spr=spr,
                                  apwfr=apwfr, lofr=lofr, veffmt=veffmt, nrmtmax=nrmt)
+
+
+# ---------------------------------------------------------------------------
+# real-space interstitial functions (inputs of genveffig / genmeffig)
+# ---------------------------------------------------------------------------
+
+def make_interstitial_real(st: "Static", *, seed: int = 99):
+    """ngrid(3) and real veffir, cfunir (ngrtot, column-major) on the grid of
+    the static's G-vector box: cfunir is the real-space form of the static's
+    cfunig (so the overlap is unchanged), veffir that of its veffig plus a
+    seeded smooth term.  Returns (ngrid, veffir, cfunir)."""
+    rng = np.random.default_rng(seed)
+    iv = np.asarray(st.intgv)
+    ngrid = np.array([int(iv[d, 1] - iv[d, 0] + 1) for d in range(3)], dtype=np.int32)
+    n1, n2, n3 = (int(x) for x in ngrid)
+    N = n1 * n2 * n3
+    ivg = np.asarray(st.ivg)[:, :st.ngvec]
+    idx = np.where(ivg >= 0, ivg, ngrid[:, None] + ivg)
+    flat = idx[0] + n1 * (idx[1] + n2 * idx[2])
+
+    def real_space(coef):
+        z = np.zeros(N, dtype=np.complex128)
+        z[flat] = coef
+        r = np.fft.ifftn(z.reshape((n1, n2, n3), order="F")) * N
+        return np.ascontiguousarray(r.real.reshape(-1, order="F"))
+
+    cfunir = real_space(np.asarray(st.cfunig))
+    extra = np.zeros(st.ngvec, dtype=np.complex128)
+    g = np.sqrt((np.asarray(st.vgc)[:, :st.ngvec] ** 2).sum(axis=0))
+    extra += 0.05 * rng.standard_normal() * np.exp(-0.5 * g * g)
+    veffir = real_space(np.asarray(st.veffig) + extra)
+    return ngrid, veffir, cfunir

@@ -193,6 +193,24 @@ int excfv_reserve(excfv_handle* h, int32_t nmatmax, int32_t ngkmax);
  * lolo, oalo and ololo may be NULL (zero) when excfv_hmlint builds them. */
 int excfv_set_static(excfv_handle* h, const excfv_static* s);
 
+/* ---- interstitial Fourier coefficients (once per SCF iteration) -------- */
+
+/* genveffig (src/genveffig.f90:13) and genmeffig (src/genmeffig.f90:13) on
+ * the device: the forward transform, divided by the grid size, of
+ * veffir * cfunir, cfunir / (1 - a2 veffir) and cfunir / (1 - a2 veffir)^2
+ * (a2 = alpha^2 / 2) over the real-space grid ngrid(3) (veffir, cfunir:
+ * real (ngrtot), column-major ngrid(1) x ngrid(2) x ngrid(3), host
+ * arrays), read at the G vectors of excfv_static.ivg (negative components
+ * wrapped by + ngrid, as gengvec's igfft).  The results replace the
+ * handle's veffig, meffig (only when valence_relativity != 0) and m2effig
+ * (only when h1on), which the next setup uses; optional host copies
+ * complex (ngvec) (NULL skips).  ngrid must hold the G-vector box intgv.
+ * Synchronous. */
+int excfv_genveffig(excfv_handle* h, const int32_t* ngrid, const double* veffir, const double* cfunir,
+                    double* veffig);
+int excfv_genmeffig(excfv_handle* h, const int32_t* ngrid, const double* veffir, const double* cfunir,
+                    double* meffig, double* m2effig);
+
 /* ---- the muffin-tin Hamiltonian build (once per SCF iteration) ---------- */
 
 /* Radial data of olprad and hmlint (module data in the reference: spr and
