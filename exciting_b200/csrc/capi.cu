@@ -126,7 +126,8 @@ void free_workspace(Workspace& ws) {
   dfree(ws.tpgpc); dfree(ws.sfacgp); dfree(ws.gk_iv); dfree(ws.d); dfree(ws.e); dfree(ws.tau);
   dfree(ws.Wp); dfree(ws.red); dfree(ws.w); dfree(ws.stein_ws); dfree(ws.icl); dfree(ws.ybuf);
   dfree(ws.Z); dfree(ws.Z2); dfree(ws.Gk); dfree(ws.Gki); dfree(ws.Tf); dfree(ws.Xs);
-  dfree(ws.status); dfree(ws.bar); dfree(ws.part); dfree(ws.prog);
+  dfree(ws.status); dfree(ws.bar); dfree(ws.part); dfree(ws.prog); dfree(ws.slices); dfree(ws.slice_sc);
+  ws.slices_elems = ws.slice_sc_n = 0;
   if (ws.h_pinned) cudaFreeHost(ws.h_pinned);
   ws.h_pinned = nullptr;
   ws.h_pinned_bytes = 0;
@@ -322,7 +323,9 @@ int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax) {
   }
   // the precision form carries extra states through the eigensolver
   if (h->prec == EXCFV_PREC_MIXED) kmax = mixed_states(nmatmax, kmax);
-  if (nmatmax <= ws.nmatmax && ngkmax <= ws.ngkmax && kmax <= ws.kmax && ws.H) return EXCFV_OK;
+  const bool want_slices = (h->prec == EXCFV_PREC_MIXED);
+  if (nmatmax <= ws.nmatmax && ngkmax <= ws.ngkmax && kmax <= ws.kmax && ws.H && (!want_slices || ws.slices))
+    return EXCFV_OK;
   nmatmax = std::max(nmatmax, ws.nmatmax);
   ngkmax = std::max(ngkmax, ws.ngkmax);
   kmax = std::max(kmax, ws.kmax);
@@ -355,6 +358,17 @@ int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax) {
     return rc;
   }
   ws.part_cap = std::max((size_t)(8u << 20), n * 64 * 4);
+  if (want_slices) {
+    // A and aa A as BF16 slice planes (setup_bf16.cu)
+    const size_t pe = bf16x_plane_elems((int)AM, (int)ngkmax);
+    const size_t nsc = 2 * (size_t)bf16x_rpad((int)ngkmax);
+    if ((rc = dalloc(&ws.slices, 2 * pe)) || (rc = dalloc(&ws.slice_sc, nsc))) {
+      free_workspace(ws);
+      return rc;
+    }
+    ws.slices_elems = 2 * pe;
+    ws.slice_sc_n = nsc;
+  }
   // zeroed in the handle's stream order (lane streams do not wait for the legacy stream)
   CUDA_TRY(cudaMemsetAsync(ws.status, 0, ST_NWORDS * sizeof(int), h->stream));
   CUDA_TRY(cudaMemsetAsync(ws.bar, 0, 4 * sizeof(unsigned), h->stream));

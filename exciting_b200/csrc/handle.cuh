@@ -1,6 +1,8 @@
 // Internal state of an excfv handle and the stage entry points.
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include <vector>
 
 #include "common.cuh"
@@ -89,6 +91,11 @@ struct Workspace {
   int* status = nullptr;    // ST_NWORDS
   unsigned int* bar = nullptr;  // grid barrier words
   int* prog = nullptr;      // (n) per-sweep progress of the band -> tridiagonal chase
+  // split-BF16 setup of the precision form: slice planes of A and of aa A, row scales
+  __nv_bfloat16* slices = nullptr;
+  size_t slices_elems = 0;
+  double* slice_sc = nullptr;
+  size_t slice_sc_n = 0;
   // host staging
   cplx* h_pinned = nullptr;
   size_t h_pinned_bytes = 0;
@@ -208,6 +215,13 @@ int stage_gensfacgp(excfv_handle* h, int ngp, const double* vgpc, long long ld, 
 int zgemm_cn_tma(excfv_handle* h, int m, int n, int k, cplx alpha, const cplx* const* A, long long lda,
                  const cplx* const* B, long long ldb, cplx beta, cplx* const* C, long long ldc, int batch,
                  int uplo);
+// H = A^H Z and O = A^H A (upper triangles) as split-BF16 tcgen05 products
+// recombined to FP64 (setup_bf16.cu); the slice buffers come from the workspace
+int zgemm_cn_bf16x(excfv_handle* h, int n, int K, const cplx* A, const cplx* Z, long long ld, cplx* H, cplx* O,
+                   long long ldc);
+int bf16x_kpad(int K);
+int bf16x_rpad(int R);
+size_t bf16x_plane_elems(int K, int R);
 // the tridiagonal reduction of the FP64 form: one-stage panels or two-stage
 bool use_two_stage(excfv_handle* h, int n);
 int band_bandwidth();

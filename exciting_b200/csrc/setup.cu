@@ -215,7 +215,12 @@ int stage_setup(excfv_handle* h, int nmatp, int ngp, bool mirror_o) {
   // O_GG = sum_a A_a^H (I + H1) A_a (overlapsetup.f90:82-108), upper triangle
   // A^H B contractions with TMA-fed operand tiles (zgemm_tma.cu)
   const cplx* Aop[2] = {ws.Apk, ws.Apk};
-  if (!st.have_h1aa) {
+  if (h->prec == EXCFV_PREC_MIXED && !st.have_h1aa) {
+    // precision form: split-BF16 tensor-core products recombined to FP64 (setup_bf16.cu)
+    prof_begin(h, PROF_SETUP_GEMM);
+    if ((rc = zgemm_cn_bf16x(h, N, (int)AM, ws.Apk, ws.Zpk, AM, ws.H, ws.O, ld))) return rc;
+    prof_end(h, PROF_SETUP_GEMM);
+  } else if (!st.have_h1aa) {
     // both contractions share A^H: one grid over both outputs
     const cplx* Bop[2] = {ws.Zpk, ws.Apk};
     cplx* Cop[2] = {ws.H, ws.O};

@@ -42,7 +42,8 @@ def test_cell16_both_forms_against_oracle():
     wm, Xm = _solve(EXCFV_PREC_MIXED, st, kp)
     assert np.abs(wm - w_ref).max() < 1e-8
     assert fvref.residuals(H, O, wm, Xm[:n]).max() < 1e-7
-    assert fvref.o_orthonormality(O, Xm[:n]) < 1e-11
+    # orthonormal in the split-BF16 overlap the precision form sets up (~1e-10 of FP64's)
+    assert fvref.o_orthonormality(O, Xm[:n]) < 1e-9
 
 
 def test_super64_properties():
@@ -67,7 +68,7 @@ def test_super64_properties():
     Hd = torch.from_numpy(H).to(dev)
     Od = torch.from_numpy(O).to(dev)
     del H, O
-    for w, X, res_tol in ((w64, X64, 1e-13), (wm, Xm, 1e-7)):
+    for w, X, res_tol, orth_tol in ((w64, X64, 1e-13, 1e-11), (wm, Xm, 1e-7, 1e-9)):
         Xd = torch.from_numpy(np.ascontiguousarray(X[:n])).to(dev)
         wd = torch.from_numpy(w).to(dev)
         R = Hd @ Xd - (Od @ Xd) * wd[None, :]
@@ -75,4 +76,4 @@ def test_super64_properties():
         G = Xd.conj().T @ (Od @ Xd)
         orth = (G - torch.eye(G.shape[0], dtype=G.dtype, device=dev)).abs().max()
         assert res.item() < res_tol
-        assert orth.item() < 1e-11
+        assert orth.item() < orth_tol

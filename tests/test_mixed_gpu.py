@@ -1,13 +1,17 @@
 """GPU parity of the precision form (EXCFV_PREC_MIXED) against the oracle.
 
-The precision form reduces C = U^-H H U^-1 to tridiagonal form in complex64
+The precision form sets H and O up as split-BF16 tensor-core products
+recombined to FP64 (setup_bf16.cu; relative error ~1e-10 of the setup), then
+reduces C = U^-H H U^-1 to tridiagonal form in complex64
 storage, carries k' = k + max(16, k/8) states through the eigensolver and
 restores FP64 accuracy with a Rayleigh-Ritz step in FP64: the k' x k' matrix
 X0^H C X0 is diagonalised exactly within clusters of near-degenerate states
 and by perturbation theory between them.  Its bar is the
-metric's: eigenvalues within 1e-8 Ha of ZHEGVX.  Eigenvectors are O-orthonormal
-to FP64 rounding (both the Ritz basis and the Ritz vectors are orthonormalised
-in FP64); their residuals are those of Ritz vectors from a complex64 basis,
+metric's: eigenvalues within 1e-8 Ha of ZHEGVX.  Eigenvectors are orthonormal
+to FP64 rounding in the overlap the form set up (both the Ritz basis and the
+Ritz vectors are orthonormalised in FP64); against the oracle's FP64 O that is
+the setup's accuracy, bounded here at ORTH_TOL = 1e-9 (measured 2e-11 on
+cubic8).  Their residuals are those of Ritz vectors from a complex64 basis,
 first order in the FP32 perturbation (2e-8 relative to ||H||_F measured on the
 diamond cell), and are bounded here at RES_TOL = 1e-7.  The Ritz values are
 second order: measured within 2e-12 Ha of ZHEGVX.
@@ -23,7 +27,7 @@ pytestmark = pytest.mark.gpu
 
 EIG_TOL = 1e-8
 RES_TOL = 1e-7
-ORTH_TOL = 1e-11
+ORTH_TOL = 1e-9
 
 
 @pytest.fixture(scope="module")
