@@ -201,6 +201,7 @@ int stage_set_static(excfv_handle* h, const excfv_static* s) {
       excfv_set_error("excfv_set_static: local-orbital arrays missing");
       return EXCFV_ERR_ARG;
     }
+    st.h_lo_first.assign(na, -1);
     for (int a = 0; a < na; ++a) {
       const int is = idxis[a];
       int first = -1;
@@ -226,6 +227,7 @@ int stage_set_static(excfv_handle* h, const excfv_static* s) {
             excfv_set_error("excfv_set_static: LO block larger than maxnlo");
             return EXCFV_ERR_ARG;
           }
+          st.h_lo_first[a] = first;
           lo_atom[g] = a;
           lo_local[g] = jj;
           lo_lm[jj + (size_t)st.maxnlo * a] = lm;
@@ -430,6 +432,7 @@ int excfv_destroy(excfv_handle* h) {
   }
   h->lanes.clear();
   drop_graph(h);
+  free_rho(h->rho);
   if (h->kinfo) cudaFree(h->kinfo);
   free_workspace(h->ws);
   if (h->owns_static) free_static(h->st);
@@ -516,6 +519,91 @@ int excfv_genmeffig(excfv_handle* h, const int32_t* ngrid, const double* veffir,
   }
   if (nk == 0) return EXCFV_OK;
   return stage_genfig(h, ngrid, veffir, cfunir, nk, kinds, dst, out);
+}
+
+int excfv_set_rho(excfv_handle* h, const excfv_rhoset* r) {
+  if (!h || !r) return EXCFV_ERR_ARG;
+  if (!h->have_static) {
+    excfv_set_error("excfv_set_static must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  DeviceGuard g(h->device);
+  cudaStreamSynchronize(h->stream);
+  return stage_set_rho(h, r);
+}
+
+// G+k inputs of one k-point into the workspace; device or host pointers
+static int rho_stage_k(excfv_handle* h, int ngp, int ngkmax, int nmatmax, const double* gpc,
+                       const double* tpgpc, const double* sfacgp, cudaMemcpyKind kind) {
+  int rc;
+  if ((rc = stage_reserve(h, nmatmax, ngkmax, std::max(1, h->st.nstfv)))) return rc;
+  Workspace& ws = h->ws;
+  if (ngkmax != ws.ngkmax) {
+    // staged G+k arrays use the workspace leading dimension; re-reserve exactly
+    cudaStreamSynchronize(h->stream);
+    free_workspace(ws);
+    if ((rc = stage_reserve(h, nmatmax, ngkmax, std::max(1, h->st.nstfv)))) return rc;
+  }
+  cudaStream_t s = h->stream;
+  CUDA_TRY(cudaMemcpyAsync(ws.gpc, gpc, sizeof(double) * ngp, kind, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.tpgpc, tpgpc, sizeof(double) * 2 * ngp, kind, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.sfacgp, sfacgp, sizeof(cplx) * (size_t)ngkmax * h->st.natmtot, kind, s));
+  return stage_match(h, ngp, ngkmax, ws.apwalm);
+}
+
+static int check_rho(excfv_handle* h, int ngp, int ngkmax, int nmatmax) {
+  if (!h) return EXCFV_ERR_ARG;
+  if (!h->have_static || !h->rho.ready) {
+    excfv_set_error("excfv_set_static and excfv_set_rho must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  if (ngp <= 0 || ngp > ngkmax || nmatmax < ngp + h->st.nlotot) {
+    excfv_set_error("excfv_rhovalk: inconsistent sizes ngp=%d ngkmax=%d nmatmax=%d", ngp, ngkmax, nmatmax);
+    return EXCFV_ERR_ARG;
+  }
+  return EXCFV_OK;
+}
+
+int excfv_rhovalk(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
+                  const double* sfacgp, int32_t nmatmax, const double* evecfv, const double* wocc, double epsocc) {
+  int rc = check_rho(h, ngp, ngkmax, nmatmax);
+  if (rc) return rc;
+  if (!gpc || !tpgpc || !sfacgp || !evecfv || !wocc) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  if ((rc = rho_stage_k(h, ngp, ngkmax, nmatmax, gpc, tpgpc, sfacgp, cudaMemcpyHostToDevice))) return rc;
+  Workspace& ws = h->ws;
+  // evecfv(nmatmax, nstfv) into the eigenvector scratch (nmatmax x kmax, kmax >= nstfv)
+  const size_t need = (size_t)nmatmax * h->st.nstfv;
+  CUDA_TRY(cudaMemcpyAsync(ws.Z, evecfv, sizeof(cplx) * need, cudaMemcpyHostToDevice, h->stream));
+  if ((rc = stage_rhovalk(h, ngp, ngkmax, ws.apwalm, ws.Z, nmatmax, wocc, epsocc))) return rc;
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return EXCFV_OK;
+}
+
+int excfv_rhovalk_dev(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
+                      const double* sfacgp, int32_t nmatmax, const double* evecfv, const double* wocc,
+                      double epsocc) {
+  int rc = check_rho(h, ngp, ngkmax, nmatmax);
+  if (rc) return rc;
+  if (!gpc || !tpgpc || !sfacgp || !evecfv || !wocc) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  if ((rc = rho_stage_k(h, ngp, ngkmax, nmatmax, gpc, tpgpc, sfacgp, cudaMemcpyDeviceToDevice))) return rc;
+  return stage_rhovalk(h, ngp, ngkmax, h->ws.apwalm, reinterpret_cast<const cplx*>(evecfv), nmatmax, wocc,
+                       epsocc);
+}
+
+int excfv_get_rhomt(excfv_handle* h, double* rhomt, int32_t reset) {
+  if (!h) return EXCFV_ERR_ARG;
+  if (!h->rho.ready) {
+    excfv_set_error("excfv_set_rho must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  DeviceGuard g(h->device);
+  const size_t n = (size_t)h->rho.lmmaxvr * h->rho.nrmtmax * h->st.natmtot;
+  if (rhomt) CUDA_TRY(cudaMemcpyAsync(rhomt, h->rho.rhomt, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+  if (reset) CUDA_TRY(cudaMemsetAsync(h->rho.rhomt, 0, sizeof(double) * n, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return EXCFV_OK;
 }
 
 static int check_k(excfv_handle* h, int nmatp, int ngp, int ngkmax) {

@@ -22,6 +22,8 @@ struct DevStatic {
   // host copies for the muffin-tin build: 0-based species, nlorb, lorbl
   // (stride max(1, nlomax)), apword
   std::vector<int> h_idxis, h_nlorb, h_lorbl, h_apword;
+  // first global local-orbital index of each atom (-1: none)
+  std::vector<int> h_lo_first;
   // device arrays
   int* idxis = nullptr;     // (natmtot) 0-based species
   double* rmt = nullptr;    // (nspecies)
@@ -101,6 +103,24 @@ struct Workspace {
   size_t h_pinned_bytes = 0;
 };
 
+// Muffin-tin density state (rhoval.cu): radial functions on the coarse
+// radial mesh, the SHT matrices, the rhomt accumulator, coefficient scratch.
+struct DevRho {
+  bool ready = false;
+  int lmaxvr = 0, lmmaxvr = 0, lradstep = 1, nrmtmax = 0, nrcmax = 0;
+  size_t ncoef = 0;
+  int* nrmt = nullptr;
+  double* ucoarse = nullptr;
+  double* vcoarse = nullptr;
+  cplx* zb = nullptr;
+  double* rf = nullptr;
+  double* rhomt = nullptr;
+  cplx* coef = nullptr;
+  double* w = nullptr;
+  int* lo_first = nullptr;
+  int* lorbl = nullptr;
+};
+
 // Stage profiler: CUDA events around stages (or single launches) on the
 // handle's stream, enabled by excfv_profile().  Class ids match
 // EXCFV_PROF_* in include/excfv.h.
@@ -142,6 +162,7 @@ struct excfv_handle {
   bool have_static = false;
   DevStatic st;
   Workspace ws;
+  DevRho rho;
   double timings[4] = {0, 0, 0, 0};
   int nsm = 148;
   Prof prof;
@@ -182,6 +203,11 @@ int stage_set_static(excfv_handle* h, const excfv_static* s);
 // 1 meffig, 2 m2effig into dst[q] (device, ngvec), optional host copies
 int stage_genfig(excfv_handle* h, const int* ngrid, const double* veffir, const double* cfunir, int nkinds,
                  const int* kinds, cplx* const* dst, cplx* const* host_out);
+// muffin-tin valence density (rhoval.cu)
+int stage_set_rho(excfv_handle* h, const excfv_rhoset* r);
+int stage_rhovalk(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, const cplx* evec, long long ldev,
+                  const double* wocc, double epsocc);
+void free_rho(DevRho& r);
 // olprad + hmlint on the device (mtbuild.cu)
 int stage_hmlint(excfv_handle* h, const excfv_mtrad* r, double* aa_out, double* loa_out, double* lolo_out,
                  double* oalo_out, double* ololo_out);

@@ -182,6 +182,39 @@ class FirstVariational:
                     "excfv_genmeffig")
         return m1, m2
 
+    def set_rho(self, rad, lmaxvr: int, lradstep: int, zbshtvr: np.ndarray, rfshtvr: np.ndarray) -> None:
+        """rhovalk's per-SCF-iteration data (radial functions of ``rad``, the
+        SHT matrices); zeroes the rhomt accumulator."""
+        st = self.static
+        keep = [_f(rad.nrmt, np.int32), _f(rad.apwfr, np.float64),
+                _f(rad.lofr, np.float64) if st.nlotot > 0 else None,
+                _f(zbshtvr, np.complex128), _f(rfshtvr, np.float64)]
+        self._rho_keep = keep
+        r = _lib.ExcfvRhoset()
+        r.lmaxvr = int(lmaxvr)
+        r.lradstep = int(lradstep)
+        r.nrmtmax = int(np.asarray(rad.spr).shape[0])
+        r.nrmt = keep[0].ctypes.data_as(_lib._i32p)
+        r.apwfr = keep[1].ctypes.data_as(_lib._f64p)
+        r.lofr = keep[2].ctypes.data_as(_lib._f64p) if keep[2] is not None else None
+        r.zbshtvr = keep[3].ctypes.data_as(_lib._f64p)
+        r.rfshtvr = keep[4].ctypes.data_as(_lib._f64p)
+        self._rho_shape = ((lmaxvr + 1) ** 2, r.nrmtmax, st.natmtot)
+        self._check(self._L.excfv_set_rho(self._h, C.byref(r)), "excfv_set_rho")
+
+    def rhovalk(self, kp, evecfv: np.ndarray, wocc, epsocc: float = 1e-8) -> None:
+        """Adds the k-point's muffin-tin valence density to the handle's rhomt."""
+        ev = _f(evecfv, np.complex128)
+        w = _f(wocc, np.float64)
+        rc = self._L.excfv_rhovalk(self._h, kp.ngp, kp.ngkmax, _ptr(kp.gpc), _ptr(kp.tpgpc), _ptr(kp.sfacgp),
+                                   int(ev.shape[0]), _ptr(ev), _ptr(w), float(epsocc))
+        self._check(rc, "excfv_rhovalk")
+
+    def rhomt(self, reset: bool = False) -> np.ndarray:
+        out = np.zeros(self._rho_shape, order="F")
+        self._check(self._L.excfv_get_rhomt(self._h, _ptr(out), int(reset)), "excfv_get_rhomt")
+        return out
+
     def hmlint(self, rad, outputs: bool = True) -> Optional[dict]:
         """``olprad`` + ``hmlint(mt_hscf)`` on the device (``src/scf_cycle.f90:212-222``):
         rebuilds the handle's aa / loa / lolo / oalo / ololo (and the IORA* h1

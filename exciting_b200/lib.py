@@ -57,6 +57,14 @@ class ExcfvMtrad(C.Structure):
     ]
 
 
+class ExcfvRhoset(C.Structure):
+    """Mirror of ``struct excfv_rhoset`` (field order and types must match)."""
+    _fields_ = [
+        ("lmaxvr", C.c_int32), ("lradstep", C.c_int32), ("nrmtmax", C.c_int32), ("nrmt", _i32p),
+        ("apwfr", _f64p), ("lofr", _f64p), ("zbshtvr", _f64p), ("rfshtvr", _f64p),
+    ]
+
+
 #: name -> (restype, argtypes); every symbol declared in include/excfv.h
 SIGNATURES = {
     "excfv_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -70,6 +78,12 @@ SIGNATURES = {
     "excfv_genveffig": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "excfv_genmeffig": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_void_p]),
+    "excfv_set_rho": (C.c_int, [C.c_void_p, C.POINTER(ExcfvRhoset)]),
+    "excfv_rhovalk": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.c_int32, C.c_void_p, C.c_void_p, C.c_double]),
+    "excfv_rhovalk_dev": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_int32, C.c_void_p, C.c_void_p, C.c_double]),
+    "excfv_get_rhomt": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
     "excfv_hmlint": (C.c_int, [C.c_void_p, C.POINTER(ExcfvMtrad), C.c_void_p, C.c_void_p, C.c_void_p,
                                C.c_void_p, C.c_void_p]),
     "excfv_match": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,

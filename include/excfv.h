@@ -211,6 +211,47 @@ int excfv_genveffig(excfv_handle* h, const int32_t* ngrid, const double* veffir,
 int excfv_genmeffig(excfv_handle* h, const int32_t* ngrid, const double* veffir, const double* cfunir,
                     double* meffig, double* m2effig);
 
+/* ---- muffin-tin valence density ----------------------------------------- */
+
+/* Data of rhovalk (src/rhovalk.f90:13) that is fixed over an SCF iteration:
+ * the radial functions (mod_APW_LO apwfr, lofr; only the function values at
+ * every lradstep-th radial point are used), nrmt, and the spherical harmonic
+ * transform matrices of mod_SHT (gen_zshtmat / gen_rshtmat): zbshtvr complex
+ * (lmmaxvr, lmmaxvr), Y_lm at the covering points (point, lm), and rfshtvr
+ * (lmmaxvr, lmmaxvr), the forward real transform (lm, point).  Host
+ * pointers, copied. */
+typedef struct excfv_rhoset {
+  int32_t lmaxvr;          /* input%groundstate%lmaxvr (0..8, <= lmaxapw) */
+  int32_t lradstep;        /* input%groundstate%lradstep (>= 1) */
+  int32_t nrmtmax;
+  const int32_t* nrmt;     /* (nspecies) */
+  const double* apwfr;     /* (nrmtmax, 2, apwordmax, 0:lmaxapw, natmtot) */
+  const double* lofr;      /* (nrmtmax, 2, nlomax, natmtot), NULL without local orbitals */
+  const double* zbshtvr;   /* complex (lmmaxvr, lmmaxvr) */
+  const double* rfshtvr;   /* (lmmaxvr, lmmaxvr) */
+} excfv_rhoset;
+
+/* Uploads the rhovalk data and zeroes the handle's rhomt accumulator. */
+int excfv_set_rho(excfv_handle* h, const excfv_rhoset* r);
+/* rhovalk (src/rhovalk.f90:13) for the spin-unpolarised ground state without
+ * second-variational vectors: the k-point's muffin-tin valence density is
+ * added to the handle's rhomt(lmmaxvr, nrmtmax, natmtot) (real harmonics,
+ * on the radial points 1, 1 + lradstep, ...; the others stay untouched), from
+ * its G+k data (as excfv_match: gpc, tpgpc, sfacgp(ngkmax, natmtot)), its
+ * first-variational vectors evecfv complex (nmatmax, nstfv) and the weights
+ * wocc(nstfv) = wkpt(ik) occsv(j, ik) (host array in both forms); states
+ * with |wocc| <= epsocc are skipped.  The host form is synchronous; the _dev
+ * form takes device gpc, tpgpc, sfacgp and evecfv and is asynchronous on the
+ * handle's stream. */
+int excfv_rhovalk(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
+                  const double* sfacgp, int32_t nmatmax, const double* evecfv, const double* wocc, double epsocc);
+int excfv_rhovalk_dev(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
+                      const double* sfacgp, int32_t nmatmax, const double* evecfv, const double* wocc,
+                      double epsocc);
+/* Copies rhomt (lmmaxvr, nrmtmax, natmtot) to the host (rhomt may be NULL)
+ * and, when reset != 0, zeroes the accumulator. */
+int excfv_get_rhomt(excfv_handle* h, double* rhomt, int32_t reset);
+
 /* ---- the muffin-tin Hamiltonian build (once per SCF iteration) ---------- */
 
 /* Radial data of olprad and hmlint (module data in the reference: spr and
