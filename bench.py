@@ -286,7 +286,7 @@ def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn, prec)
                  "execution": "single-k-point entry, k-points one after another",
                  "eig_diff_vs_batched": float(np.abs(wp - evals).max())}
     nm = [k.nmat for k in kpts]
-    form = "mixed (complex64 tridiagonal reduction + FP64 Rayleigh-Ritz)" if prec == EXCFV_PREC_MIXED \
+    form = "mixed (split-BF16 tcgen05 setup recombined to FP64, complex64 tridiagonal reduction + FP64 Rayleigh-Ritz)" if prec == EXCFV_PREC_MIXED \
         else "plain FP64"
     return {"workload": f"{nk} k-points per GPU of the 8-atom cell, nmat {min(nm)}..{max(nm)} "
                         f"(uniform, seeded), lowest {st.nstfv} states, {form}",
@@ -579,6 +579,15 @@ def main():
             mevs.append((s, e))
         fvm.sync(n)
         torch.cuda.synchronize()
+        # stage breakdown of the precision form, outside its timed steps
+        fvm.profile(True)
+        for _ in range(args.steps):
+            flush.zero_()
+            fvm.seceqn_dev(n, kp.ngp, kp.ngkmax, ptrs, nmatmax, dm_eval.data_ptr(), dm_evec.data_ptr())
+        fvm.sync(n)
+        torch.cuda.synchronize()
+        mprof = fvm.profile_read()
+        fvm.profile(False)
     m_ms = sum(s.elapsed_time(e) for s, e in mevs)
     tm = torch.tensor([m_ms], dtype=torch.float64, device=dev)
     if world > 1:
@@ -586,9 +595,26 @@ def main():
     m_ms = float(tm.item())
     wm_host = dm_eval.cpu().numpy()
     fvm.close()
+    # split-BF16 setup on tcgen05 (slicing + the tensor-core kernel): 2 outputs
+    # x 15 slice pairs x 4 real products x 2 flops x K x N(N+1)/2 of BF16
+    # tensor work, against the measured BF16 peak; and the FP64 work it
+    # replaces (2 x 8 x K x N(N+1)/2) per second
+    ms_sg, cnt_sg = mprof["setup_gemm"]
+    sg_s = ms_sg / args.steps / 1e3
+    bf16_flops = 2 * 15 * 4 * 2.0 * AM * (N * (N + 1) / 2)
+    bf16_peak = peaks.get("bf16_tflops")
     mixed_single = {"value": world * args.steps / (m_ms / 1e3), "unit": UNIT,
                     "ms_per_step": m_ms / args.steps,
-                    "eig_err_vs_fp64_gpu": float(np.abs(wm_host - ev_host).max())}
+                    "eig_err_vs_fp64_gpu": float(np.abs(wm_host - ev_host).max()),
+                    "stage_ms_per_step": {kk: round(v[0] / args.steps, 4) for kk, v in mprof.items()},
+                    "setup_split_bf16": {
+                        "kernel": "k_zgemm_bf16x (tcgen05 kind::f16, 128x48 tiles) + k_slice",
+                        "ms_per_k": sg_s * 1e3,
+                        "bf16_tflops": bf16_flops / sg_s / 1e12 if cnt_sg else None,
+                        "bf16_peak_tflops": bf16_peak,
+                        "frac_of_bf16_peak": (bf16_flops / sg_s / 1e12 / bf16_peak) if (cnt_sg and bf16_peak) else None,
+                        "fp64_equivalent_tflops": g_flops / sg_s / 1e12 if cnt_sg else None,
+                        "peak_source": "bf16: MEASURED_PEAKS.json (cuBLAS BF16 burst)"}}
 
     # ---- batching form: 64 k-points of the 8-atom cell, nmat 1800..2300 ------
     batched = None

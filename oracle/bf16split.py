@@ -44,3 +44,11 @@ def product(A: np.ndarray, B: np.ndarray, nsl: int = 5) -> np.ndarray:
             im += a[s][0].T @ b[t][1] - a[s][1].T @ b[t][0]
         C += np.ldexp(1.0, -7 * (d + 2)) * (re + 1j * im)
     return C * sa[:, None] * sb[None, :]
+
+
+def hermitian_product(A: np.ndarray, B: np.ndarray, nsl: int = 5) -> np.ndarray:
+    """``product`` of a Hermitian result (H = A^H aa A, O = A^H A): the device
+    form writes its diagonal real."""
+    C = product(A, B, nsl)
+    C[np.diag_indices(min(C.shape))] = C.diagonal().real
+    return C

@@ -92,4 +92,5 @@ def test_batch_as_benchmarked(batch, prec, etol, rtol):
         Xi = X[i].view(st.nstfv, p.nmatmax).T.cpu().numpy()[:n]
         assert np.all(X[i].view(st.nstfv, p.nmatmax).T[n:].abs().cpu().numpy() == 0)
         assert fvref.residuals(H, O, w, Xi).max() < rtol
-        assert fvref.o_orthonormality(O, Xi) < 1e-11
+        # orthonormal in the overlap each form set up: FP64, or split-BF16 (~1e-10 of FP64's)
+        assert fvref.o_orthonormality(O, Xi) < (1e-11 if prec == EXCFV_PREC_FP64 else 1e-9)

@@ -5,7 +5,7 @@ against the FP64 setup.
 
 - H and O through excfv_hamiltonandoverlapsetup in the precision form equal
   the oracle's H and O with the APW-APW block replaced by the exact
-  split-BF16 product to 1e-13 of their largest entry (the device sums
+  split-BF16 product (diagonal real) to 1e-13 of their largest entry (the device sums
   are exact integer sums in FP32, so only FP64 rounding differs), on cubic8
   at full size and on a small diamond cell (tile edges: n < 128, n not a
   multiple of 48);
@@ -38,8 +38,8 @@ def test_split_bf16_setup_matches_exact_splitting(name, kw):
     Z = np.concatenate([st.aa[:, :, ias] @ fvref._apwi(st, apwalm, ias, ngp) for ias in range(st.natmtot)],
                        axis=0)
     H_ref, O_ref = fvref.hamiltonandoverlapsetup(st, kp, apwalm)
-    dH = bf16split.product(A, Z) - A.conj().T @ Z
-    dO = bf16split.product(A, A) - A.conj().T @ A
+    dH = bf16split.hermitian_product(A, Z) - A.conj().T @ Z
+    dO = bf16split.hermitian_product(A, A) - A.conj().T @ A
     # the setup keeps the upper triangle and mirrors it
     dH = np.triu(dH) + np.triu(dH, 1).conj().T
     dO = np.triu(dO) + np.triu(dO, 1).conj().T
