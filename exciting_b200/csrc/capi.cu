@@ -433,6 +433,7 @@ int excfv_destroy(excfv_handle* h) {
   h->lanes.clear();
   drop_graph(h);
   free_rho(h->rho);
+  free_sv(h->sv);
   if (h->kinfo) cudaFree(h->kinfo);
   free_workspace(h->ws);
   if (h->owns_static) free_static(h->st);
@@ -590,6 +591,93 @@ int excfv_rhovalk_dev(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double
   if ((rc = rho_stage_k(h, ngp, ngkmax, nmatmax, gpc, tpgpc, sfacgp, cudaMemcpyDeviceToDevice))) return rc;
   return stage_rhovalk(h, ngp, ngkmax, h->ws.apwalm, reinterpret_cast<const cplx*>(evecfv), nmatmax, wocc,
                        epsocc);
+}
+
+int excfv_set_bfield(excfv_handle* h, const excfv_bfield* b) {
+  if (!h || !b) return EXCFV_ERR_ARG;
+  if (!h->have_static) {
+    excfv_set_error("excfv_set_static must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  DeviceGuard g(h->device);
+  cudaStreamSynchronize(h->stream);
+  return stage_set_bfield(h, b);
+}
+
+// the k-point's G+k data into the workspace and its packed matching coefficients
+static int sv_stage_k(excfv_handle* h, int ngp, int ngkmax, int nmatmax, const double* gpc, const double* tpgpc,
+                      const double* sfacgp, const int32_t* igpig, cudaMemcpyKind kind) {
+  int rc;
+  if ((rc = stage_reserve(h, nmatmax, ngkmax, std::max(1, h->st.nstfv)))) return rc;
+  Workspace& ws = h->ws;
+  if (ngkmax != ws.ngkmax) {
+    cudaStreamSynchronize(h->stream);
+    free_workspace(ws);
+    if ((rc = stage_reserve(h, nmatmax, ngkmax, std::max(1, h->st.nstfv)))) return rc;
+  }
+  cudaStream_t s = h->stream;
+  CUDA_TRY(cudaMemcpyAsync(ws.gpc, gpc, sizeof(double) * ngp, kind, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.tpgpc, tpgpc, sizeof(double) * 2 * ngp, kind, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.sfacgp, sfacgp, sizeof(cplx) * (size_t)ngkmax * h->st.natmtot, kind, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.igpig, igpig, sizeof(int) * ngp, kind, s));
+  return stage_match(h, ngp, ngkmax, nullptr);
+}
+
+static int check_sv(excfv_handle* h, int ngp, int ngkmax, int nmatmax) {
+  if (!h) return EXCFV_ERR_ARG;
+  if (!h->have_static || !h->sv.ready) {
+    excfv_set_error("excfv_set_static and excfv_set_bfield must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  if (ngp <= 0 || ngp > ngkmax || nmatmax < ngp + h->st.nlotot || h->st.nstfv > ngp) {
+    excfv_set_error("excfv_seceqnsv: inconsistent sizes ngp=%d ngkmax=%d nmatmax=%d nstfv=%d", ngp, ngkmax,
+                    nmatmax, h->st.nstfv);
+    return EXCFV_ERR_ARG;
+  }
+  return EXCFV_OK;
+}
+
+int excfv_seceqnsv(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
+                   const double* sfacgp, const int32_t* igpig, int32_t nmatmax, const double* evalfv,
+                   const double* evecfv, double* evalsv, double* evecsv) {
+  int rc = check_sv(h, ngp, ngkmax, nmatmax);
+  if (rc) return rc;
+  if (!gpc || !tpgpc || !sfacgp || !igpig || !evalfv || !evecfv || !evalsv || !evecsv) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  if ((rc = sv_stage_k(h, ngp, ngkmax, nmatmax, gpc, tpgpc, sfacgp, igpig, cudaMemcpyHostToDevice))) return rc;
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  const int n = h->st.nstfv;
+  CUDA_TRY(cudaMemcpyAsync(ws.Z2, evecfv, sizeof(cplx) * (size_t)nmatmax * n, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(h->sv.evalfv, evalfv, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  double* dw = nullptr;
+  cplx* dv = nullptr;
+  if ((rc = dalloc(&dw, (size_t)2 * n)) || (rc = dalloc(&dv, (size_t)4 * n * n))) {
+    if (dw) cudaFree(dw);
+    return rc;
+  }
+  rc = stage_seceqnsv(h, ngp, ws.Z2, nmatmax, h->sv.evalfv, dw, dv);
+  if (rc == EXCFV_OK) rc = stage_status(h, n);
+  if (rc == EXCFV_OK) {
+    cudaMemcpyAsync(evalsv, dw, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(evecsv, dv, sizeof(cplx) * 4 * (size_t)n * n, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) rc = EXCFV_ERR_CUDA;
+  }
+  cudaFree(dw);
+  cudaFree(dv);
+  return rc;
+}
+
+int excfv_seceqnsv_dev(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
+                       const double* sfacgp, const int32_t* igpig, int32_t nmatmax, const double* evalfv,
+                       const double* evecfv, double* evalsv, double* evecsv) {
+  int rc = check_sv(h, ngp, ngkmax, nmatmax);
+  if (rc) return rc;
+  if (!gpc || !tpgpc || !sfacgp || !igpig || !evalfv || !evecfv || !evalsv || !evecsv) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  if ((rc = sv_stage_k(h, ngp, ngkmax, nmatmax, gpc, tpgpc, sfacgp, igpig, cudaMemcpyDeviceToDevice))) return rc;
+  return stage_seceqnsv(h, ngp, reinterpret_cast<const cplx*>(evecfv), nmatmax, evalfv, evalsv,
+                        reinterpret_cast<cplx*>(evecsv));
 }
 
 int excfv_get_rhomt(excfv_handle* h, double* rhomt, int32_t reset) {

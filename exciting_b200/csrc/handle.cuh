@@ -121,6 +121,24 @@ struct DevRho {
   int* lorbl = nullptr;
 };
 
+// Second-variational state (secvar.cu): the collinear field's muffin-tin
+// blocks (mt_hscf%alpha; beta = -alpha), the Fourier coefficients of the
+// interstitial field over the whole grid, scratch.
+struct DevSV {
+  bool ready = false;
+  int ngrid[3] = {0, 0, 0};
+  cplx* aa = nullptr;     // (maxaa, maxaa, natmtot)
+  cplx* loa = nullptr;    // (maxnlo, maxaa, natmtot)
+  cplx* lolo = nullptr;   // (maxnlo, maxnlo, natmtot)
+  cplx* birhat = nullptr; // (ngrtot) forward transform of bir / ngrtot
+  cplx* evlo = nullptr;   // (maxnlo * natmtot, nstfv) LO rows of evecfv per atom
+  cplx* zhlo = nullptr;   // (maxnlo * natmtot, nstfv)
+  cplx* S = nullptr;      // (nstfv, nstfv) field matrix of the up block
+  double* evalfv = nullptr;  // (nstfv)
+  int* lo_first = nullptr;   // (natmtot) first global LO index, -1 none
+  int* status_save = nullptr;  // (ST_NWORDS) the up block's solver status
+};
+
 // Stage profiler: CUDA events around stages (or single launches) on the
 // handle's stream, enabled by excfv_profile().  Class ids match
 // EXCFV_PROF_* in include/excfv.h.
@@ -163,6 +181,7 @@ struct excfv_handle {
   DevStatic st;
   Workspace ws;
   DevRho rho;
+  DevSV sv;
   double timings[4] = {0, 0, 0, 0};
   int nsm = 148;
   Prof prof;
@@ -208,6 +227,15 @@ int stage_set_rho(excfv_handle* h, const excfv_rhoset* r);
 int stage_rhovalk(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, const cplx* evec, long long ldev,
                   const double* wocc, double epsocc);
 void free_rho(DevRho& r);
+// second variation, collinear field (secvar.cu)
+int stage_set_bfield(excfv_handle* h, const excfv_bfield* b);
+int stage_seceqnsv(excfv_handle* h, int ngp, const cplx* evec, long long ldev, const double* d_evalfv,
+                   double* d_evalsv, cplx* d_evecsv);
+void free_sv(DevSV& v);
+int stage_mt_field(excfv_handle* h, const excfv_mtrad* r, const double* field, cplx* aa, cplx* loa, cplx* lolo,
+                   double* aa_out, double* loa_out, double* lolo_out);
+int stage_grid_field(excfv_handle* h, const int* ngrid, const double* f, const double* cfunir, double c0,
+                     cplx* dst);
 // olprad + hmlint on the device (mtbuild.cu)
 int stage_hmlint(excfv_handle* h, const excfv_mtrad* r, double* aa_out, double* loa_out, double* lolo_out,
                  double* oalo_out, double* ololo_out);

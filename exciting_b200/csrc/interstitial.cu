@@ -23,19 +23,26 @@ namespace {
 constexpr double A2 = 0.5 / (137.03599911 * 137.03599911);
 constexpr int DFT_NMAX = 1024;
 
-// zfft = f(veffir, cfunir) on the whole grid
-__global__ void k_ir_prepare(long long n, int kind, const double* veffir, const double* cfunir, cplx* z) {
+// zfft = f(veffir, cfunir) on the whole grid; kind 3: (v + c0) cfunir (the
+// interstitial magnetic field of seceqnsv.f90:660-668)
+__global__ void k_ir_prepare(long long n, int kind, const double* veffir, const double* cfunir, double c0,
+                             cplx* z) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double v = veffir[i], c = cfunir[i];
   double r;
   if (kind == 0) r = v * c;
   else if (kind == 1) r = c / (1.0 - v * A2);
-  else {
+  else if (kind == 2) {
     const double t = 1.0 - v * A2;
     r = c / (t * t);
-  }
+  } else r = (v + c0) * c;
   z[i] = cmk(r, 0.0);
+}
+
+__global__ void k_ir_scale(long long n, double scale, const cplx* z, cplx* out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = cmk(z[i].x * scale, z[i].y * scale);
 }
 
 // forward DFT along one axis of the column-major grid: lines of length n with
@@ -120,7 +127,7 @@ int stage_genfig(excfv_handle* h, const int* ngrid, const double* veffir, const 
   } else {
     const unsigned gb = (unsigned)((N + 255) / 256);
     for (int q = 0; q < nkinds && rc == EXCFV_OK; ++q) {
-      k_ir_prepare<<<gb, 256, 0, s>>>(N, kinds[q], d_v, d_c, z0);
+      k_ir_prepare<<<gb, 256, 0, s>>>(N, kinds[q], d_v, d_c, 0.0, z0);
       count_launch();
       const long long nl1 = N / n1, nl2 = N / n2, nl3 = N / n3;
       auto grid = [](long long nl) { return (unsigned)std::min<long long>(nl, 148LL * 16); };
@@ -145,6 +152,58 @@ int stage_genfig(excfv_handle* h, const int* ngrid, const double* veffir, const 
   }
   cudaError_t serr = cudaStreamSynchronize(s);
   if (rc == EXCFV_OK && serr != cudaSuccess) fail(serr);
+  cudaFree(d_v);
+  cudaFree(d_c);
+  cudaFree(z0);
+  cudaFree(z1);
+  return rc;
+}
+
+// the forward transform (divided by the grid size) of (f + c0) cfunir over
+// the whole grid into dst (ngrtot complex, device): the Fourier coefficients
+// of the interstitial field whose product with a wavefunction seceqnsv forms
+// by zfftifc(+1), a multiplication and zfftifc(-1)
+int stage_grid_field(excfv_handle* h, const int* ngrid, const double* f, const double* cfunir, double c0,
+                     cplx* dst) {
+  cudaStream_t s = h->stream;
+  const int n1 = ngrid[0], n2 = ngrid[1], n3 = ngrid[2];
+  if (n1 < 1 || n2 < 1 || n3 < 1 || n1 > DFT_NMAX || n2 > DFT_NMAX || n3 > DFT_NMAX) {
+    excfv_set_error("interstitial field: ngrid (%d %d %d) outside 1..%d", n1, n2, n3, DFT_NMAX);
+    return EXCFV_ERR_ARG;
+  }
+  const long long N = (long long)n1 * n2 * n3;
+  double *d_v = nullptr, *d_c = nullptr;
+  cplx *z0 = nullptr, *z1 = nullptr;
+  int rc = EXCFV_OK;
+  cudaError_t err;
+  if ((err = cudaMalloc(&d_v, sizeof(double) * N)) != cudaSuccess ||
+      (err = cudaMalloc(&d_c, sizeof(double) * N)) != cudaSuccess ||
+      (err = cudaMalloc(&z0, sizeof(cplx) * N)) != cudaSuccess ||
+      (err = cudaMalloc(&z1, sizeof(cplx) * N)) != cudaSuccess ||
+      (err = cudaMemcpyAsync(d_v, f, sizeof(double) * N, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+      (err = cudaMemcpyAsync(d_c, cfunir, sizeof(double) * N, cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+    excfv_set_error("interstitial field: %s", cudaGetErrorString(err));
+    rc = EXCFV_ERR_CUDA;
+  } else {
+    const unsigned gb = (unsigned)((N + 255) / 256);
+    k_ir_prepare<<<gb, 256, 0, s>>>(N, 3, d_v, d_c, c0, z0);
+    count_launch();
+    const long long nl1 = N / n1, nl2 = N / n2, nl3 = N / n3;
+    auto grid = [](long long nl) { return (unsigned)std::min<long long>(nl, 148LL * 16); };
+    k_dft_axis<<<grid(nl1), 64, 0, s>>>(n1, 1, nl1, z0, z1);
+    count_launch();
+    k_dft_axis<<<grid(nl2), 64, 0, s>>>(n2, n1, nl2, z1, z0);
+    count_launch();
+    k_dft_axis<<<grid(nl3), 64, 0, s>>>(n3, (long long)n1 * n2, nl3, z0, z1);
+    count_launch();
+    k_ir_scale<<<gb, 256, 0, s>>>(N, 1.0 / (double)N, z1, dst);
+    count_launch();
+    if ((err = cudaGetLastError()) != cudaSuccess) {
+      excfv_set_error("interstitial field: %s", cudaGetErrorString(err));
+      rc = EXCFV_ERR_CUDA;
+    }
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess && rc == EXCFV_OK) rc = EXCFV_ERR_CUDA;
   cudaFree(d_v);
   cudaFree(d_c);
   cudaFree(z0);

@@ -299,7 +299,7 @@ __global__ void k_mt_aa(MtArgs m, const int* flist, const cplx* gnt, const doubl
   int l3 = 0; while ((l3 + 1) * (l3 + 1) <= lm3) ++l3;
   const int L1 = m.lmaxmat + 1, lmmat = L1 * L1;
   cplx s = cmk(0.0, 0.0);
-  if (lm1 == lm3) s.x = kaa[((size_t)ias * L1 + l1) * m.apwordmax * m.apwordmax + io1 * m.apwordmax + io2];
+  if (lm1 == lm3 && kaa) s.x = kaa[((size_t)ias * L1 + l1) * m.apwordmax * m.apwordmax + io1 * m.apwordmax + io2];
   const double* h = haa + ((((size_t)ias * L1 + l1) * m.apwordmax + io1) * L1 + l3) * m.apwordmax * m.lmvr +
                     (size_t)io2 * m.lmvr;
   const cplx* g = gnt + ((size_t)lm1 * lmmat + lm3) * m.lmvr;
@@ -323,7 +323,7 @@ __global__ void k_mt_loa(MtArgs m, const int* flist, const int* lo_lm, const int
   int l3 = 0; while ((l3 + 1) * (l3 + 1) <= lm3) ++l3;
   const int L1 = m.lmaxmat + 1, lmmat = L1 * L1;
   cplx s = cmk(0.0, 0.0);
-  if (lm1 == lm3) s.x = kalo[((size_t)ias * m.nlomax + ilo) * m.apwordmax + io];
+  if (lm1 == lm3 && kalo) s.x = kalo[((size_t)ias * m.nlomax + ilo) * m.apwordmax + io];
   const double* h = halo + ((((size_t)ias * m.nlomax + ilo) * L1 + l3) * m.apwordmax + io) * m.lmvr;
   const cplx* g = gnt + ((size_t)lm1 * lmmat + lm3) * m.lmvr;
   for (int lm2 = 0; lm2 < m.lmvr; ++lm2) s = cadd(s, cscale(g[lm2], h[lm2]));
@@ -343,7 +343,7 @@ __global__ void k_mt_lolo(MtArgs m, const int* lo_lm, const int* lo_ilo, const c
   if (lm1 < 0 || ilo1 < 0 || lm3 < 0 || ilo2 < 0) { lolo[t] = cmk(0.0, 0.0); return; }
   const int lmmat = (m.lmaxmat + 1) * (m.lmaxmat + 1);
   cplx s = cmk(0.0, 0.0);
-  if (lm1 == lm3) s.x = klolo[((size_t)ias * m.nlomax + ilo1) * m.nlomax + ilo2];
+  if (lm1 == lm3 && klolo) s.x = klolo[((size_t)ias * m.nlomax + ilo1) * m.nlomax + ilo2];
   const double* h = hlolo + (((size_t)ias * m.nlomax + ilo1) * m.nlomax + ilo2) * m.lmvr;
   const cplx* g = gnt + ((size_t)lm1 * lmmat + lm3) * m.lmvr;
   for (int lm2 = 0; lm2 < m.lmvr; ++lm2) s = cadd(s, cscale(g[lm2], h[lm2]));
@@ -385,21 +385,25 @@ int upload(T** d, const void* h, size_t n) {
 
 }  // namespace
 
-// hmlint + olprad into the handle's static blocks; the host copies (nullable)
-// receive aa, loa, lolo (complex) and oalo, ololo (real, without the IORA*
-// terms) in the reference layouts.
-int stage_hmlint(excfv_handle* h, const excfv_mtrad* r, double* aa_out, double* loa_out, double* lolo_out,
-                 double* oalo_out, double* ololo_out) {
+// mt_kin (kinetic) + mt_pot of the field `pot` (host, veffmt's layout; NULL:
+// veffmt) into dst_aa / dst_loa / dst_lolo (device, the handle's block
+// layouts), and with `olp` olprad into the handle's oalo / ololo / h1 terms;
+// the host copies (nullable) receive aa, loa, lolo (complex) and oalo, ololo
+// (real, without the IORA* terms) in the reference layouts.
+static int mt_build(excfv_handle* h, const excfv_mtrad* r, const double* pot, bool kinetic, bool olp,
+                    cplx* dst_aa, cplx* dst_loa, cplx* dst_lolo, double* aa_out, double* loa_out,
+                    double* lolo_out, double* oalo_out, double* ololo_out) {
   DevStatic& st = h->st;
   const int* nlorb_h = st.h_nlorb.data();
   const int* lorbl_h = st.h_lorbl.data();
   const int* apword_h = st.h_apword.data();
   if (r->lmaxvr < 0 || r->lmaxvr > SPECFUN_LMAX || r->nrmtmax < 3 || !r->nrmt || !r->spr || !r->apwfr ||
-      !r->veffmt || (st.nlotot > 0 && !r->lofr)) {
-    excfv_set_error("excfv_hmlint: missing or inconsistent radial data");
+      (!pot && !r->veffmt) || (kinetic && !r->veffmt) || (st.nlotot > 0 && !r->lofr)) {
+    excfv_set_error("muffin-tin build: missing or inconsistent radial data");
     return EXCFV_ERR_ARG;
   }
-  if (st.h1on && !st.h1aa) {
+  if (!pot) pot = r->veffmt;
+  if (olp && st.h1on && !st.h1aa) {
     CUDA_TRY(cudaMalloc(&st.h1aa, sizeof(double) * st.apwordmax * st.apwordmax * (st.lmaxapw + 1) * st.natmtot));
     CUDA_TRY(cudaMemset(st.h1aa, 0, sizeof(double) * st.apwordmax * st.apwordmax * (st.lmaxapw + 1) * st.natmtot));
   }
@@ -441,7 +445,7 @@ int stage_hmlint(excfv_handle* h, const excfv_mtrad* r, double* aa_out, double* 
       (rc = upload(&d_spr, r->spr, nr2 * st.nspecies)) ||
       (rc = upload(&d_apwfr, r->apwfr, nr2 * 2 * st.apwordmax * (st.lmaxapw + 1) * st.natmtot)) ||
       (rc = upload(&d_lofr, r->lofr, nr2 * 2 * nlomax * st.natmtot)) ||
-      (rc = upload(&d_veff, r->veffmt, (size_t)lmvr * nr2 * st.natmtot)) ||
+      (rc = upload(&d_veff, pot, (size_t)lmvr * nr2 * st.natmtot)) ||
       (rc = upload(&d_gnt, gnt.data(), gnt.size()))) {
     cudaFree(d_idxis); cudaFree(d_nrmt); cudaFree(d_apword); cudaFree(d_nlorb); cudaFree(d_lorbl);
     cudaFree(d_wts); cudaFree(d_spr); cudaFree(d_apwfr); cudaFree(d_lofr); cudaFree(d_veff); cudaFree(d_gnt);
@@ -469,41 +473,48 @@ int stage_hmlint(excfv_handle* h, const excfv_mtrad* r, double* aa_out, double* 
     k_mt_potint<<<grid(per_aa * N), 128, 0, s>>>(m, 0, per_aa, haa); count_launch();
     k_mt_potint<<<grid(per_loa * N), 128, 0, s>>>(m, 1, per_loa, halo); count_launch();
     k_mt_potint<<<grid(per_lolo * N), 128, 0, s>>>(m, 2, per_lolo, hlolo); count_launch();
-    k_mt_radint<<<grid(per_kaa * N), 128, 0, s>>>(m, 0, 0, per_kaa, kaa); count_launch();
-    k_mt_radint<<<grid(per_kalo * N), 128, 0, s>>>(m, 1, 0, per_kalo, kalo); count_launch();
-    k_mt_radint<<<grid(per_klolo * N), 128, 0, s>>>(m, 2, 0, per_klolo, klolo); count_launch();
-    k_mt_radint<<<grid(per_kalo * N), 128, 0, s>>>(m, 1, 2, per_kalo, oalo_r); count_launch();
-    k_mt_radint<<<grid(per_klolo * N), 128, 0, s>>>(m, 2, 2, per_klolo, ololo_r); count_launch();
-    if (st.h1on) {
+    if (kinetic) {
+      k_mt_radint<<<grid(per_kaa * N), 128, 0, s>>>(m, 0, 0, per_kaa, kaa); count_launch();
+      k_mt_radint<<<grid(per_kalo * N), 128, 0, s>>>(m, 1, 0, per_kalo, kalo); count_launch();
+      k_mt_radint<<<grid(per_klolo * N), 128, 0, s>>>(m, 2, 0, per_klolo, klolo); count_launch();
+    }
+    if (olp) {
+      k_mt_radint<<<grid(per_kalo * N), 128, 0, s>>>(m, 1, 2, per_kalo, oalo_r); count_launch();
+      k_mt_radint<<<grid(per_klolo * N), 128, 0, s>>>(m, 2, 2, per_klolo, ololo_r); count_launch();
+    }
+    if (olp && st.h1on) {
       k_mt_radint<<<grid(per_kaa * N), 128, 0, s>>>(m, 0, 1, per_kaa, h1aa_r); count_launch();
       k_mt_radint<<<grid(per_kalo * N), 128, 0, s>>>(m, 1, 1, per_kalo, h1loa_r); count_launch();
       k_mt_radint<<<grid(per_klolo * N), 128, 0, s>>>(m, 2, 1, per_klolo, h1lolo_r); count_launch();
     }
     // assembly into the static blocks
-    k_mt_aa<<<grid((long long)st.maxaa * st.maxaa * N), 128, 0, s>>>(m, st.flist, d_gnt, haa, kaa, st.aa);
+    const double* ka = kinetic ? kaa : nullptr;
+    const double* kl = kinetic ? kalo : nullptr;
+    const double* kll = kinetic ? klolo : nullptr;
+    k_mt_aa<<<grid((long long)st.maxaa * st.maxaa * N), 128, 0, s>>>(m, st.flist, d_gnt, haa, ka, dst_aa);
     count_launch();
     if (st.maxnlo > 0) {
       k_mt_loa<<<grid((long long)st.maxnlo * st.maxaa * N), 128, 0, s>>>(m, st.flist, st.lo_lm, st.lo_ilo, d_gnt,
-                                                                          halo, kalo, st.loa);
+                                                                          halo, kl, dst_loa);
       count_launch();
       k_mt_lolo<<<grid((long long)st.maxnlo * st.maxnlo * N), 128, 0, s>>>(m, st.lo_lm, st.lo_ilo, d_gnt, hlolo,
-                                                                            klolo, st.lolo);
+                                                                            kll, dst_lolo);
       count_launch();
     }
-    if (st.nlomax > 0 || st.h1on) {
+    if (olp && (st.nlomax > 0 || st.h1on)) {
       k_mt_olp<<<st.natmtot, 128, 0, s>>>(m, oalo_r, h1loa_r, ololo_r, h1lolo_r, h1aa_r, st.oalo, st.ololo,
                                           st.h1aa, st.h1on);
       count_launch();
     }
     if (cudaGetLastError() != cudaSuccess) { rc = EXCFV_ERR_CUDA; goto done; }
     // optional host copies (reference layouts)
-    if (aa_out) cudaMemcpyAsync(aa_out, st.aa, sizeof(cplx) * st.maxaa * st.maxaa * N, cudaMemcpyDeviceToHost, s);
+    if (aa_out) cudaMemcpyAsync(aa_out, dst_aa, sizeof(cplx) * st.maxaa * st.maxaa * N, cudaMemcpyDeviceToHost, s);
     if (loa_out && st.maxnlo > 0)
-      cudaMemcpyAsync(loa_out, st.loa, sizeof(cplx) * st.maxnlo * st.maxaa * N, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(loa_out, dst_loa, sizeof(cplx) * st.maxnlo * st.maxaa * N, cudaMemcpyDeviceToHost, s);
     if (lolo_out && st.maxnlo > 0)
-      cudaMemcpyAsync(lolo_out, st.lolo, sizeof(cplx) * st.maxnlo * st.maxnlo * N, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(lolo_out, dst_lolo, sizeof(cplx) * st.maxnlo * st.maxnlo * N, cudaMemcpyDeviceToHost, s);
     std::vector<double> tmp;
-    if ((oalo_out || ololo_out) && st.nlomax > 0) {
+    if (olp && (oalo_out || ololo_out) && st.nlomax > 0) {
       tmp.resize((size_t)(per_kalo + per_klolo) * N);
       cudaMemcpyAsync(tmp.data(), oalo_r, sizeof(double) * per_kalo * N, cudaMemcpyDeviceToHost, s);
       cudaMemcpyAsync(tmp.data() + per_kalo * N, ololo_r, sizeof(double) * per_klolo * N, cudaMemcpyDeviceToHost, s);
@@ -530,6 +541,20 @@ done:
                   (void*)hlolo, (void*)kaa, (void*)kalo, (void*)klolo, (void*)oalo_r, (void*)ololo_r, (void*)h1aa_r,
                   (void*)h1loa_r, (void*)h1lolo_r})
     cudaFree(p);
-  if (rc == EXCFV_OK && st.h1on) st.have_h1aa = true;
+  if (rc == EXCFV_OK && olp && st.h1on) st.have_h1aa = true;
   return rc;
+}
+
+int stage_hmlint(excfv_handle* h, const excfv_mtrad* r, double* aa_out, double* loa_out, double* lolo_out,
+                 double* oalo_out, double* ololo_out) {
+  DevStatic& st = h->st;
+  return mt_build(h, r, nullptr, true, true, st.aa, st.loa, st.lolo, aa_out, loa_out, lolo_out, oalo_out,
+                  ololo_out);
+}
+
+// mt_pot of a field without the kinetic term and without olprad (the spin
+// blocks of hmlint.f90:88-108) into the given device blocks
+int stage_mt_field(excfv_handle* h, const excfv_mtrad* r, const double* field, cplx* aa, cplx* loa, cplx* lolo,
+                   double* aa_out, double* loa_out, double* lolo_out) {
+  return mt_build(h, r, field, false, false, aa, loa, lolo, aa_out, loa_out, lolo_out, nullptr, nullptr);
 }

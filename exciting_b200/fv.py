@@ -182,6 +182,59 @@ class FirstVariational:
                     "excfv_genmeffig")
         return m1, m2
 
+    def _mtrad(self, rad, keep):
+        st = self.static
+
+        def f64(a):
+            if a is None:
+                return None
+            x = _f(a, np.float64)
+            keep.append(x)
+            return x.ctypes.data_as(_lib._f64p)
+
+        nrmt = _f(rad.nrmt, np.int32)
+        keep.append(nrmt)
+        r = _lib.ExcfvMtrad()
+        r.lmaxvr = int(rad.lmaxvr)
+        r.nrmtmax = int(np.asarray(rad.spr).shape[0])
+        r.nrmt = nrmt.ctypes.data_as(_lib._i32p)
+        r.spr = f64(rad.spr)
+        r.apwfr = f64(rad.apwfr)
+        r.lofr = f64(rad.lofr) if st.nlotot > 0 else None
+        r.veffmt = f64(getattr(rad, "veffmt", None))
+        keep.append(r)
+        return r
+
+    def set_bfield(self, rad, bxcmt, bmtconst, ngrid, bxcir, cfunir, birconst: float) -> None:
+        """The collinear field of the second variation (mt_hscf%alpha and the
+        interstitial field), built on the device."""
+        keep = []
+        r = self._mtrad(rad, keep)
+        arrs = [_f(bxcmt, np.float64), _f(bmtconst, np.float64), _f(ngrid, np.int32), _f(bxcir, np.float64),
+                _f(cfunir, np.float64)]
+        b = _lib.ExcfvBfield()
+        b.rad = C.pointer(r)
+        b.bxcmt = arrs[0].ctypes.data_as(_lib._f64p)
+        b.bmtconst = arrs[1].ctypes.data_as(_lib._f64p)
+        b.ngrid = arrs[2].ctypes.data_as(_lib._i32p)
+        b.bxcir = arrs[3].ctypes.data_as(_lib._f64p)
+        b.cfunir = arrs[4].ctypes.data_as(_lib._f64p)
+        b.birconst = float(birconst)
+        self._check(self._L.excfv_set_bfield(self._h, C.byref(b)), "excfv_set_bfield")
+
+    def seceqnsv(self, kp, evalfv, evecfv) -> Tuple[np.ndarray, np.ndarray]:
+        """``seceqnsv`` for the collinear field: (evalsv (2 nstfv), evecsv (2 nstfv, 2 nstfv))."""
+        n = self.static.nstfv
+        w = _f(evalfv, np.float64)
+        ev = _f(evecfv, np.complex128)
+        ig = _f(kp.igpig, np.int32)
+        ws = np.zeros(2 * n)
+        vs = np.zeros((2 * n, 2 * n), dtype=np.complex128, order="F")
+        rc = self._L.excfv_seceqnsv(self._h, kp.ngp, kp.ngkmax, _ptr(kp.gpc), _ptr(kp.tpgpc), _ptr(kp.sfacgp),
+                                    _ptr(ig), int(ev.shape[0]), _ptr(w), _ptr(ev), _ptr(ws), _ptr(vs))
+        self._check(rc, "excfv_seceqnsv", n)
+        return ws, vs
+
     def set_rho(self, rad, lmaxvr: int, lradstep: int, zbshtvr: np.ndarray, rfshtvr: np.ndarray) -> None:
         """rhovalk's per-SCF-iteration data (radial functions of ``rad``, the
         SHT matrices); zeroes the rhomt accumulator."""

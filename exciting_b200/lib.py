@@ -65,6 +65,14 @@ class ExcfvRhoset(C.Structure):
     ]
 
 
+class ExcfvBfield(C.Structure):
+    """Mirror of ``struct excfv_bfield`` (field order and types must match)."""
+    _fields_ = [
+        ("rad", C.POINTER(ExcfvMtrad)), ("bxcmt", _f64p), ("bmtconst", _f64p), ("ngrid", _i32p),
+        ("bxcir", _f64p), ("cfunir", _f64p), ("birconst", C.c_double),
+    ]
+
+
 #: name -> (restype, argtypes); every symbol declared in include/excfv.h
 SIGNATURES = {
     "excfv_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -84,6 +92,11 @@ SIGNATURES = {
     "excfv_rhovalk_dev": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_int32, C.c_void_p, C.c_void_p, C.c_double]),
     "excfv_get_rhomt": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "excfv_set_bfield": (C.c_int, [C.c_void_p, C.POINTER(ExcfvBfield)]),
+    "excfv_seceqnsv": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "excfv_seceqnsv_dev": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "excfv_hmlint": (C.c_int, [C.c_void_p, C.POINTER(ExcfvMtrad), C.c_void_p, C.c_void_p, C.c_void_p,
                                C.c_void_p, C.c_void_p]),
     "excfv_match": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,

@@ -281,6 +281,43 @@ typedef struct excfv_mtrad {
 int excfv_hmlint(excfv_handle* h, const excfv_mtrad* r, double* aa, double* loa, double* lolo, double* oalo,
                  double* ololo);
 
+/* ---- second variation, collinear spin ------------------------------------ */
+
+/* The collinear exchange-correlation field of seceqnsv (src/seceqnsv.f90:10)
+ * on its default path (groundstate/spin realspace = false), fixed over an
+ * SCF iteration.  Host pointers, read during excfv_set_bfield. */
+typedef struct excfv_bfield {
+  const excfv_mtrad* rad;   /* radial data (lmaxvr, nrmt, spr, apwfr, lofr; veffmt unused) */
+  const double* bxcmt;      /* (lmmaxvr, nrmtmax, natmtot): bxcmt(:,:,:,1), the z field */
+  const double* bmtconst;   /* (natmtot): ga4 (bfcmt(3) + bfieldc(3)) of each atom, added to the
+                               spherical part (hmlint.f90:94) */
+  const int32_t* ngrid;     /* (3) the real-space grid */
+  const double* bxcir;      /* (ngrtot) bxcir(:,1) */
+  const double* cfunir;     /* (ngrtot) */
+  double birconst;          /* ga4 bfieldc(3) (seceqnsv.f90:668) */
+} excfv_bfield;
+
+/* Builds mt_hscf%alpha (mt_pot of the field, hmlint.f90:88-108; beta = -alpha)
+ * and the interstitial field bir = (bxcir + birconst) cfunir in Fourier space
+ * on the device. */
+int excfv_set_bfield(excfv_handle* h, const excfv_bfield* b);
+/* seceqnsv (src/seceqnsv.f90:10) for a collinear field without spin-orbit
+ * coupling and LDA+U: the first-variational states' matrix of the field (the
+ * muffin-tin contractions with alpha, the interstitial product of each
+ * wavefunction with bir), evalfv on the diagonal, and one Hermitian
+ * eigensolve per spin block (ZHEEV('V','U'), ndmag = 1).  Inputs: the
+ * k-point's G+k data as excfv_seceqn (gpc, tpgpc, sfacgp, igpig), evalfv
+ * (nstfv) and evecfv complex (nmatmax, nstfv); outputs evalsv (2 nstfv: the
+ * up block's eigenvalues, then the down block's) and evecsv complex
+ * (2 nstfv, 2 nstfv), block diagonal.  The host form is synchronous; the
+ * _dev form takes device arrays (all of them) and is asynchronous. */
+int excfv_seceqnsv(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
+                   const double* sfacgp, const int32_t* igpig, int32_t nmatmax, const double* evalfv,
+                   const double* evecfv, double* evalsv, double* evecsv);
+int excfv_seceqnsv_dev(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
+                       const double* sfacgp, const int32_t* igpig, int32_t nmatmax, const double* evalfv,
+                       const double* evecfv, double* evalsv, double* evecsv);
+
 /* ---- the hot path ------------------------------------------------------ */
 
 /* match (src/match.f90:13): APW matching coefficients.

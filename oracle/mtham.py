@@ -195,9 +195,11 @@ def _zora(st, rad, ias, nr):
     return a, 1.0 / (1.0 - a * rad.veffmt[0, :nr, ias] * Y00)
 
 
-def hmlint(st, rad: Radial, gnt=None):
+def hmlint(st, rad: Radial, gnt=None, pot=None, kinetic: bool = True):
     """aa (maxaa, maxaa, natmtot), loa (maxnlo, maxaa, natmtot), lolo (maxnlo,
-    maxnlo, natmtot): mt_kin + mt_pot into zeroed blocks.
+    maxnlo, natmtot): mt_kin + mt_pot into zeroed blocks.  ``pot`` replaces
+    veffmt in mt_pot (hmlint.f90 runs mt_pot on the magnetic field for the
+    spin blocks, without mt_kin: ``kinetic=False``).
 
     The radial integrals of every pair of radial functions (and every lm of
     the potential) are taken together, one spline per integrand as the
@@ -217,7 +219,7 @@ def hmlint(st, rad: Radial, gnt=None):
         a, rm = _zora(st, rad, ias, nr)
         u = rad.apwfr[:nr, :, :, :, ias]        # (nr, 2, io, l)
         lo = rad.lofr[:nr, :, :, ias]           # (nr, 2, ilo)
-        V = rad.veffmt[:lmmaxvr, :nr, ias]      # (lm2, nr)
+        V = (rad.veffmt if pot is None else pot)[:lmmaxvr, :nr, ias]      # (lm2, nr)
         fs = _packed(st, is_)
         los = _lo_funcs(st, is_)
         # radial functions of the atom: APW (l, io) for l <= lmaxmat, then LOs
@@ -250,9 +252,11 @@ def hmlint(st, rad: Radial, gnt=None):
 
         def block(b1, lm1, b3, lm3):
             G = gnt[lm1][:, :, lm3]                       # (n1, lm2, n3)
-            pot = np.einsum("akb,abk->ab", G, R[np.ix_(b1, b3)])
+            pot_ = np.einsum("akb,abk->ab", G, R[np.ix_(b1, b3)])
+            if not kinetic:
+                return pot_
             kin = np.where(lm1[:, None] == lm3[None, :], K[np.ix_(b1, b3)], 0.0)
-            return kin + pot
+            return kin + pot_
 
         aa[:nf, :nf, ias] = block(fb, flm, fb, flm)
         if nl:

@@ -177,3 +177,24 @@ def test_chase_back_transform_in_blocks(n, b, m):
     _, _, _, refl = ts.hb2st(B, b)
     Z = rng.standard_normal((n, 11)) + 1j * rng.standard_normal((n, 11))
     assert np.abs(ts.apply_q2_blocked(refl, Z, m) - ts.apply_q2(refl, Z)).max() < 1e-13
+
+
+def test_chase_task_compiles_for_the_device(tmp_path):
+    """chase.cuh's task is __host__ __device__: its sm_100a device build
+    compiles (a one-thread wrapper; compile only, nothing runs)."""
+    import os
+    import shutil
+    import subprocess
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not found")
+    here = os.path.dirname(os.path.abspath(__file__))
+    src = tmp_path / "chase_device.cu"
+    src.write_text('#include "chase.cuh"\n'
+                   "__global__ void k_chase_one(BandView B, int col, int lo, int hi, cplx* v, cplx* tau,\n"
+                   "                            cplx* work) {\n"
+                   "  if (threadIdx.x == 0 && blockIdx.x == 0) chase_task(B, col, lo, hi, v, tau, work);\n"
+                   "}\n")
+    subprocess.run([nvcc, "-std=c++17", "-O2", "-gencode", "arch=compute_100a,code=sm_100a", "-c",
+                    "-I", os.path.join(here, "..", "exciting_b200", "csrc"), str(src),
+                    "-o", str(tmp_path / "chase_device.o")], check=True)
