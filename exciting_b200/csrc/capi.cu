@@ -364,11 +364,11 @@ int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax) {
     // A and aa A as BF16 slice planes (setup_bf16.cu)
     const size_t pe = bf16x_plane_elems((int)AM, (int)ngkmax);
     const size_t nsc = 2 * (size_t)bf16x_rpad((int)ngkmax);
-    if ((rc = dalloc(&ws.slices, 2 * pe)) || (rc = dalloc(&ws.slice_sc, nsc))) {
+    if ((rc = dalloc(&ws.slices, pe)) || (rc = dalloc(&ws.slice_sc, nsc))) {
       free_workspace(ws);
       return rc;
     }
-    ws.slices_elems = 2 * pe;
+    ws.slices_elems = pe;
     ws.slice_sc_n = nsc;
   }
   // zeroed in the handle's stream order (lane streams do not wait for the legacy stream)

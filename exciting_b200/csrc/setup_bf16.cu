@@ -20,11 +20,14 @@
 //
 // Kernel.  One CTA per 128 x 48 output tile (upper triangle of H and of O,
 // both in one grid), 10 warps: warp 0 issues the TMA copies (one 3-D box of
-// all 2 NSL planes of A's 128 rows and one of B's 48 rows per 16 of K, into
-// a 3-stage ring, 32-byte swizzle), warp 1 allocates the 512 TMEM columns
-// and one of its threads issues tcgen05.mma (kind::f16, BF16 x BF16 -> F32,
-// M 128, N 48, K 16; both operands K-major) into one Re and one Im
-// accumulator per level (NSL x 96 columns), warps 2..9 read the
+// the 2 NSL planes (Re, Im per slice) of A's 128 rows and one of the 3 NSL
+// planes (Re, Im, -Re per slice) of B's 48 rows per 16 of K, into a 3-stage
+// ring, 32-byte swizzle), warp 1 allocates the 512 TMEM columns and one of
+// its threads issues tcgen05.mma (kind::f16, BF16 x BF16 -> F32, M 128,
+// N 96, K 16; both operands K-major): with B's planes in that order [Br; Bi]
+// and [Bi; -Br] are contiguous 96-row operands, so Ar [Br; Bi]^T + Ai [Bi;
+// -Br]^T = [Re | Im] is two MMAs per slice pair into one accumulator of 96
+// columns per level (NSL x 96 columns), warps 2..9 read the
 // accumulators back with tcgen05.ld after each 256 of K (tcgen05.commit on
 // an mbarrier) and keep the FP64 sums.  Every wait is bounded in time; a
 // wait that gives up sets the status word, the CTA waits for its copies and
@@ -39,7 +42,8 @@
 namespace {
 
 constexpr int NSL = 5;                 // slices per part
-constexpr int NPL = 2 * NSL;           // planes: (slice, re/im)
+constexpr int NPL = 2 * NSL;           // planes of the row (A) side: (slice, re/im)
+constexpr int NPB = 3 * NSL;           // planes of the column (B) side: (slice, re/im/-re)
 constexpr int BM = 128, BN = 48, KS = 16;
 constexpr int CHUNK = 16;              // K steps (of 16) per exact FP32 chunk = 256 of K
 constexpr int STAGES = 3;
@@ -47,7 +51,7 @@ constexpr int NEPI = 8;                // epilogue warps
 constexpr int NWARP = 2 + NEPI;
 constexpr unsigned A_PLANE = BM * KS * 2;            // 4096 B
 constexpr unsigned B_PLANE = BN * KS * 2;            // 1536 B
-constexpr unsigned STAGE_BYTES = NPL * (A_PLANE + B_PLANE);
+constexpr unsigned STAGE_BYTES = NPL * A_PLANE + NPB * B_PLANE;
 constexpr unsigned TMEM_COLS = 512;
 constexpr int COLS_PER_LEVEL = 2 * BN; // Re then Im
 constexpr int EPI_COLS = BN / 2;       // output columns per epilogue thread
@@ -131,10 +135,10 @@ __device__ __forceinline__ uint64_t sdesc(unsigned addr) {
   return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(256u >> 4) << 32) |
          ((uint64_t)1u << 46) | ((uint64_t)6u << 61);
 }
-// instruction descriptor: F32 accumulator, BF16 A and B, both K-major, N = BN, M = BM
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+// instruction descriptor: F32 accumulator, BF16 A and B, both K-major,
+// N = 2 BN (Re and Im side by side), M = BM
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)((2 * BN) >> 3) << 17) |
                            ((uint32_t)(BM >> 4) << 24);
-constexpr uint32_t IDESC_NEGB = IDESC | (1u << 14);
 
 __device__ __forceinline__ void umma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
   asm volatile(
@@ -255,18 +259,17 @@ __global__ void __launch_bounds__(32 * NWARP, 1)
         const unsigned baseB = baseA + NPL * A_PLANE;
 #pragma unroll
         for (int d = 0; d < NSL; ++d) {
-          const uint32_t dre = tmem + d * COLS_PER_LEVEL, dim = dre + BN;
+          const uint32_t dacc = tmem + d * COLS_PER_LEVEL;   // [Re | Im] of level d
 #pragma unroll
           for (int sa = 0; sa <= d; ++sa) {
             const int tb = d - sa;
             const uint64_t aRe = sdesc(baseA + (2 * sa) * A_PLANE), aIm = sdesc(baseA + (2 * sa + 1) * A_PLANE);
-            const uint64_t bRe = sdesc(baseB + (2 * tb) * B_PLANE), bIm = sdesc(baseB + (2 * tb + 1) * B_PLANE);
+            // [Br; Bi] and [Bi; -Br]: planes 3 tb, 3 tb + 1 and 3 tb + 1, 3 tb + 2
+            const uint64_t bP = sdesc(baseB + (3 * tb) * B_PLANE), bQ = sdesc(baseB + (3 * tb + 1) * B_PLANE);
             const uint32_t acc = (first && sa == 0) ? 0u : 1u;
-            // Re += Ar Br + Ai Bi ; Im += Ar Bi - Ai Br
-            umma(dre, aRe, bRe, IDESC, acc);
-            umma(dre, aIm, bIm, IDESC, 1u);
-            umma(dim, aRe, bIm, IDESC, acc);
-            umma(dim, aIm, bRe, IDESC_NEGB, 1u);
+            // [Re | Im] += Ar [Br | Bi] + Ai [Bi | -Br]
+            umma(dacc, aRe, bP, IDESC, acc);
+            umma(dacc, aIm, bQ, IDESC, 1u);
           }
         }
         umma_commit(&empty[s]);
@@ -339,10 +342,12 @@ __global__ void __launch_bounds__(32 * NWARP, 1)
 }
 
 // slices of one operand: X is K x R complex, column-major (leading dimension
-// ld), contiguous along K; out is [NPL][rpad][kpad] BF16 (plane 2s + part),
+// ld), contiguous along K.  outA (nullable) receives the row-side layout
+// [NPL][rpad][kpad] BF16 (plane 2s + part), outB (nullable) the column-side
+// layout [NPB][rpad][kpad] (planes 3s: Re, 3s + 1: Im, 3s + 2: -Re);
 // sc[r] = 2^e_r.  Rows past R and k past K are zero.
-__global__ void k_slice(const cplx* X, long long ld, int K, int R, int kpad, int rpad, __nv_bfloat16* out,
-                        double* sc) {
+__global__ void k_slice(const cplx* X, long long ld, int K, int R, int kpad, int rpad, __nv_bfloat16* outA,
+                        __nv_bfloat16* outB, double* sc) {
   const int r = blockIdx.x;
   __shared__ double red[32];
   double m = 0.0;
@@ -366,18 +371,26 @@ __global__ void k_slice(const cplx* X, long long ld, int K, int R, int kpad, int
   if (threadIdx.x == 0 && r < rpad) sc[r] = ldexp(1.0, e);
   const double inv = ldexp(1.0, 7 - e);   // scale, then the first slice's 2^7
   const size_t plane = (size_t)rpad * kpad;
+  const size_t at = (size_t)r * kpad;
   for (int k = threadIdx.x; k < kpad; k += blockDim.x) {
     cplx x = cmk(0.0, 0.0);
     if (r < R && k < K) x = X[k + ld * r];
+    double vr = x.x * inv, vi = x.y * inv;
 #pragma unroll
-    for (int part = 0; part < 2; ++part) {
-      double v = (part == 0 ? x.x : x.y) * inv;
-#pragma unroll
-      for (int s = 0; s < NSL; ++s) {
-        const double q = rint(v);
-        out[(size_t)(2 * s + part) * plane + (size_t)r * kpad + k] = __float2bfloat16_rn((float)q);
-        v = (v - q) * 128.0;
+    for (int s = 0; s < NSL; ++s) {
+      const double qr = rint(vr), qi = rint(vi);
+      const __nv_bfloat16 br = __float2bfloat16_rn((float)qr), bi = __float2bfloat16_rn((float)qi);
+      if (outA) {
+        outA[(size_t)(2 * s) * plane + at + k] = br;
+        outA[(size_t)(2 * s + 1) * plane + at + k] = bi;
       }
+      if (outB) {
+        outB[(size_t)(3 * s) * plane + at + k] = br;
+        outB[(size_t)(3 * s + 1) * plane + at + k] = bi;
+        outB[(size_t)(3 * s + 2) * plane + at + k] = __float2bfloat16_rn((float)-qr);
+      }
+      vr = (vr - qr) * 128.0;
+      vi = (vi - qi) * 128.0;
     }
   }
 }
@@ -394,16 +407,16 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// [NPL][rpad][kpad] BF16 planes as a 3-D map, boxes of 16 k x rows x NPL planes
-int plane_map(CUtensorMap* tm, const __nv_bfloat16* P, int kpad, int rpad, int rows) {
+// [np][rpad][kpad] BF16 planes as a 3-D map, boxes of 16 k x rows x np planes
+int plane_map(CUtensorMap* tm, const __nv_bfloat16* P, int kpad, int rpad, int rows, int np) {
   auto fn = encode_fn();
   if (!fn) {
     excfv_set_error("cuTensorMapEncodeTiled is not available from the driver");
     return EXCFV_ERR_CUDA;
   }
-  const cuuint64_t dims[3] = {(cuuint64_t)kpad, (cuuint64_t)rpad, (cuuint64_t)NPL};
+  const cuuint64_t dims[3] = {(cuuint64_t)kpad, (cuuint64_t)rpad, (cuuint64_t)np};
   const cuuint64_t strides[2] = {(cuuint64_t)kpad * 2, (cuuint64_t)kpad * rpad * 2};
-  const cuuint32_t box[3] = {(cuuint32_t)KS, (cuuint32_t)rows, (cuuint32_t)NPL};
+  const cuuint32_t box[3] = {(cuuint32_t)KS, (cuuint32_t)rows, (cuuint32_t)np};
   const cuuint32_t estr[3] = {1u, 1u, 1u};
   const CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(P), dims, strides,
                         box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
@@ -419,8 +432,9 @@ int plane_map(CUtensorMap* tm, const __nv_bfloat16* P, int kpad, int rpad, int r
 
 int bf16x_kpad(int K) { return (K + KS - 1) / KS * KS; }
 int bf16x_rpad(int R) { return (R + BM - 1) / BM * BM; }
-// BF16 elements of one operand's slice planes
-size_t bf16x_plane_elems(int K, int R) { return (size_t)NPL * bf16x_kpad(K) * bf16x_rpad(R); }
+// BF16 elements of the slice planes of one k-point: A in both layouts, aa A
+// in the column-side layout
+size_t bf16x_plane_elems(int K, int R) { return (size_t)(NPL + 2 * NPB) * bf16x_kpad(K) * bf16x_rpad(R); }
 
 // H = A^H Z and O = A^H A (upper triangles, n x n, leading dimension ldc)
 // from the packed K x n operands A and Z (leading dimension ld) through the
@@ -431,24 +445,25 @@ int zgemm_cn_bf16x(excfv_handle* h, int n, int K, const cplx* A, const cplx* Z, 
   cudaStream_t s = h->stream;
   if (n <= 0 || K <= 0) return EXCFV_ERR_ARG;
   const int kpad = bf16x_kpad(K), rpad = bf16x_rpad(n);
-  const size_t pe = (size_t)NPL * kpad * rpad;
-  if (!ws.slices || ws.slices_elems < 2 * pe || ws.slice_sc_n < 2 * (size_t)rpad) {
+  const size_t plane = (size_t)kpad * rpad;
+  if (!ws.slices || ws.slices_elems < bf16x_plane_elems(K, n) || ws.slice_sc_n < 2 * (size_t)rpad) {
     excfv_set_error("split-BF16 setup: slice workspace not reserved for K = %d, n = %d", K, n);
     return EXCFV_ERR_STATE;
   }
-  __nv_bfloat16* PA = ws.slices;
-  __nv_bfloat16* PZ = ws.slices + pe;
+  __nv_bfloat16* PA = ws.slices;                    // A, row side
+  __nv_bfloat16* PAB = PA + (size_t)NPL * plane;    // A, column side
+  __nv_bfloat16* PZB = PAB + (size_t)NPB * plane;   // aa A, column side
   double* scA = ws.slice_sc;
   double* scZ = ws.slice_sc + rpad;
-  k_slice<<<rpad, 256, 0, s>>>(A, ld, K, n, kpad, rpad, PA, scA);
+  k_slice<<<rpad, 256, 0, s>>>(A, ld, K, n, kpad, rpad, PA, PAB, scA);
   count_launch();
-  k_slice<<<rpad, 256, 0, s>>>(Z, ld, K, n, kpad, rpad, PZ, scZ);
+  k_slice<<<rpad, 256, 0, s>>>(Z, ld, K, n, kpad, rpad, nullptr, PZB, scZ);
   count_launch();
   CUDA_TRY(cudaGetLastError());
   CUtensorMap mA, mZ, mAb;
   int rc;
-  if ((rc = plane_map(&mA, PA, kpad, rpad, BM)) || (rc = plane_map(&mZ, PZ, kpad, rpad, BN)) ||
-      (rc = plane_map(&mAb, PA, kpad, rpad, BN)))
+  if ((rc = plane_map(&mA, PA, kpad, rpad, BM, NPL)) || (rc = plane_map(&mZ, PZB, kpad, rpad, BN, NPB)) ||
+      (rc = plane_map(&mAb, PAB, kpad, rpad, BN, NPB)))
     return rc;
   Bf16xArgs a;
   a.n = n;
