@@ -680,6 +680,43 @@ int excfv_seceqnsv_dev(excfv_handle* h, int32_t ngp, int32_t ngkmax, const doubl
                         reinterpret_cast<cplx*>(evecsv));
 }
 
+int excfv_rhovalk_sv(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
+                     const double* sfacgp, int32_t nmatmax, const double* evecfv, const double* evecsv,
+                     const double* wocc, double epsocc) {
+  int rc = check_rho(h, ngp, ngkmax, nmatmax);
+  if (rc) return rc;
+  if (!gpc || !tpgpc || !sfacgp || !evecfv || !evecsv || !wocc) return EXCFV_ERR_ARG;
+  DeviceGuard g(h->device);
+  if ((rc = rho_stage_k(h, ngp, ngkmax, nmatmax, gpc, tpgpc, sfacgp, cudaMemcpyHostToDevice))) return rc;
+  Workspace& ws = h->ws;
+  const int n = h->st.nstfv;
+  CUDA_TRY(cudaMemcpyAsync(ws.Z, evecfv, sizeof(cplx) * (size_t)nmatmax * n, cudaMemcpyHostToDevice, h->stream));
+  cplx* dsv = nullptr;
+  if ((rc = dalloc(&dsv, (size_t)4 * n * n))) return rc;
+  rc = EXCFV_OK;
+  if (cudaMemcpyAsync(dsv, evecsv, sizeof(cplx) * (size_t)4 * n * n, cudaMemcpyHostToDevice, h->stream) !=
+      cudaSuccess)
+    rc = EXCFV_ERR_CUDA;
+  if (rc == EXCFV_OK) rc = stage_rhovalk_sv(h, ngp, ngkmax, ws.apwalm, ws.Z, nmatmax, dsv, wocc, epsocc);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess && rc == EXCFV_OK) rc = EXCFV_ERR_CUDA;
+  cudaFree(dsv);
+  return rc;
+}
+
+int excfv_get_magmt(excfv_handle* h, double* magmt, int32_t reset) {
+  if (!h) return EXCFV_ERR_ARG;
+  if (!h->rho.ready) {
+    excfv_set_error("excfv_set_rho must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  DeviceGuard g(h->device);
+  const size_t n = (size_t)h->rho.lmmaxvr * h->rho.nrmtmax * h->st.natmtot;
+  if (magmt) CUDA_TRY(cudaMemcpyAsync(magmt, h->rho.magmt, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+  if (reset) CUDA_TRY(cudaMemsetAsync(h->rho.magmt, 0, sizeof(double) * n, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return EXCFV_OK;
+}
+
 int excfv_get_rhomt(excfv_handle* h, double* rhomt, int32_t reset) {
   if (!h) return EXCFV_ERR_ARG;
   if (!h->rho.ready) {

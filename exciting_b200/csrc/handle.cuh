@@ -119,6 +119,13 @@ struct DevRho {
   double* w = nullptr;
   int* lo_first = nullptr;
   int* lorbl = nullptr;
+  // the spin-polarised branch (second-variational vectors): magnetisation
+  // accumulator and the spinor components' coefficient scratch
+  double* magmt = nullptr;   // (lmmaxvr, nrmtmax, natmtot)
+  cplx* coef2 = nullptr;     // (apwordmax * lmmaxvr, 2 nstfv, natmtot)
+  cplx* lo1 = nullptr;       // (maxnlo * natmtot, nstfv) LO rows of evecfv
+  cplx* lo2 = nullptr;       // (maxnlo * natmtot, 2 nstfv)
+  cplx* esv = nullptr;       // (nstfv, 2 nstfv) one spin's rows of evecsv
 };
 
 // Second-variational state (secvar.cu): the collinear field's muffin-tin
@@ -226,6 +233,8 @@ int stage_genfig(excfv_handle* h, const int* ngrid, const double* veffir, const 
 int stage_set_rho(excfv_handle* h, const excfv_rhoset* r);
 int stage_rhovalk(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, const cplx* evec, long long ldev,
                   const double* wocc, double epsocc);
+int stage_rhovalk_sv(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, const cplx* evec, long long ldev,
+                     const cplx* evecsv, const double* wocc, double epsocc);
 void free_rho(DevRho& r);
 // second variation, collinear field (secvar.cu)
 int stage_set_bfield(excfv_handle* h, const excfv_bfield* b);

@@ -9,7 +9,13 @@
 //   rfmt(tp, r)    = sum_j w_j |sum_lm zbshtvr(tp, lm) wf(lm, r, j)|^2
 //   rhomt(lm, r)  += sum_tp rfshtvr(lm, tp) rfmt(tp, r)
 // on the coarse radial mesh (every lradstep-th point), w_j = wkpt occsv
-// (states with |w_j| <= epsocc skipped).  One CTA per (coarse radial point,
+// (states with |w_j| <= epsocc skipped).  With second-variational vectors
+// (collinear spin, rhovalk.f90:74-160) each spinor component of state j is
+// sum_ist evecsv((ispn-1) nstfv + ist, j) wfmt(ist), which is linear in the
+// coefficients: the first-variational coefficients (their parts below 1e-14
+// dropped first, as wavefmt_add drops them) times the spin's rows of evecsv
+// (entries with |Re| + |Im| <= epsocc dropped) by one GEMM, then the same
+// kernel per spin, rhomt += up + dn and magmt += up - dn.  One CTA per (coarse radial point,
 // atom): the backward transform of a chunk of states from shared memory,
 // |.|^2 summed per angular point in registers, the forward real transform at
 // the end; each CTA owns its rhomt entries, so k-points accumulate in stream
@@ -41,8 +47,13 @@ struct RhoArgs {
   const cplx* coef;      // (apwordmax * lmmaxvr, nst, natmtot): row io + apwordmax * lm
   const cplx* evec;      // (nmatmax, nst)
   long long ldev;
+  const cplx* locoef;    // nullable: LO coefficients (q + maxnlo ias, j) in place of evec's rows
+  long long ldlo;
+  int cut;               // apply wavefmt_add's cut-off to the coefficients
   const double* w;       // (nst) weights, 0 for skipped states
   double* rhomt;         // (lmmaxvr, nrmtmax, natmtot)
+  double* magmt;         // nullable: += msign * the same density
+  double msign;
 };
 
 __device__ __forceinline__ void wf_add(double a, double b, double f, cplx& acc) {
@@ -85,15 +96,18 @@ __global__ void k_rho_mt(RhoArgs a) {
         for (int io = 0; io < nap; ++io) {
           const cplx c = cf[(size_t)(io + a.apwordmax * lm) + (size_t)a.apwordmax * L * j];
           const double u = a.ucoarse[irc + (size_t)a.nrcmax * (io + (size_t)a.apwordmax * (l + (size_t)(a.lmaxvr + 1) * ias))];
-          wf_add(c.x, c.y, u, v);
+          if (a.cut) wf_add(c.x, c.y, u, v);
+          else { v.x += c.x * u; v.y += c.y * u; }
         }
         if (a.lo_first[ias] >= 0)
           for (int q = 0; q < a.maxnlo; ++q) {
             if (a.lo_lm[q + a.maxnlo * ias] != lm) continue;
             const int ilo = a.lo_ilo[q + a.maxnlo * ias];
-            const cplx c = a.evec[(size_t)(a.ngp + a.lo_first[ias] + q) + (size_t)a.ldev * j];
+            const cplx c = a.locoef ? a.locoef[(size_t)(q + a.maxnlo * ias) + (size_t)a.ldlo * j]
+                                    : a.evec[(size_t)(a.ngp + a.lo_first[ias] + q) + (size_t)a.ldev * j];
             const double f = a.vcoarse[irc + (size_t)a.nrcmax * (ilo + (size_t)a.nlomax * ias)];
-            wf_add(c.x, c.y, f, v);
+            if (a.cut) wf_add(c.x, c.y, f, v);
+            else { v.x += c.x * f; v.y += c.y * f; }
           }
       }
       wf[lm + L * jj] = v;
@@ -120,8 +134,47 @@ __global__ void k_rho_mt(RhoArgs a) {
     const int lm = threadIdx.x;
     double s = 0.0;
     for (int tp = 0; tp < L; ++tp) s += a.rf[lm + (size_t)L * tp] * rfmt[tp];
-    a.rhomt[lm + (size_t)L * (irc * a.lradstep + (size_t)a.nrmtmax * ias)] += s;
+    const size_t at = lm + (size_t)L * (irc * a.lradstep + (size_t)a.nrmtmax * ias);
+    a.rhomt[at] += s;
+    if (a.magmt) a.magmt[at] += a.msign * s;
   }
+}
+
+// drop real and imaginary parts below the cut-off (wavefmt_add)
+__global__ void k_rho_cut(long long n, cplx* c) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  cplx v = c[t];
+  if (fabs(v.x) < WF_EPS) v.x = 0.0;
+  if (fabs(v.y) < WF_EPS) v.y = 0.0;
+  c[t] = v;
+}
+
+// LO rows of evecfv per atom, cut: lo(q + maxnlo ias, j)
+__global__ void k_rho_gather_lo(int natmtot, int maxnlo, int nst, int ngp, const int* lo_lm, const int* lo_first,
+                                const cplx* evec, long long ldev, cplx* lo) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long rows = (long long)maxnlo * natmtot;
+  if (t >= rows * nst) return;
+  const int r = (int)(t % rows), j = (int)(t / rows);
+  const int ias = r / maxnlo, q = r % maxnlo;
+  cplx v = cmk(0.0, 0.0);
+  if (lo_first[ias] >= 0 && lo_lm[q + maxnlo * ias] >= 0) {
+    v = evec[(size_t)(ngp + lo_first[ias] + q) + ldev * j];
+    if (fabs(v.x) < WF_EPS) v.x = 0.0;
+    if (fabs(v.y) < WF_EPS) v.y = 0.0;
+  }
+  lo[t] = v;
+}
+
+// one spin's rows of evecsv (ld 2n), entries with |Re| + |Im| <= epsocc dropped
+__global__ void k_rho_esv(int n, int spin, const cplx* evecsv, double epsocc, cplx* esv) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * 2 * n) return;
+  const int ist = (int)(t % n), j = (int)(t / n);
+  cplx v = evecsv[(size_t)(spin * n + ist) + (size_t)2 * n * j];
+  if (fabs(v.x) + fabs(v.y) <= epsocc) v = cmk(0.0, 0.0);
+  esv[t] = v;
 }
 
 template <typename T>
@@ -138,7 +191,8 @@ int dup(T** d, const T* h, size_t n) {
 
 void free_rho(DevRho& r) {
   for (void* p : {(void*)r.nrmt, (void*)r.ucoarse, (void*)r.vcoarse, (void*)r.zb, (void*)r.rf, (void*)r.rhomt,
-                  (void*)r.coef, (void*)r.w, (void*)r.lo_first, (void*)r.lorbl})
+                  (void*)r.coef, (void*)r.w, (void*)r.lo_first, (void*)r.lorbl, (void*)r.magmt, (void*)r.coef2,
+                  (void*)r.lo1, (void*)r.lo2, (void*)r.esv})
     if (p) cudaFree(p);
   r = DevRho();
 }
@@ -195,9 +249,15 @@ int stage_set_rho(excfv_handle* h, const excfv_rhoset* r) {
       (rc = dup(&d.zb, reinterpret_cast<const cplx*>(r->zbshtvr), L * L)) || (rc = dup(&d.rf, r->rfshtvr, L * L)) ||
       (rc = dup(&d.rhomt, (const double*)nullptr, L * r->nrmtmax * st.natmtot)) ||
       (rc = dup(&d.coef, (const cplx*)nullptr, d.ncoef)) ||
-      (rc = dup(&d.w, (const double*)nullptr, (size_t)std::max(st.nstfv, 1))) ||
+      (rc = dup(&d.w, (const double*)nullptr, (size_t)2 * std::max(st.nstfv, 1))) ||
       (rc = dup(&d.lo_first, first.data(), st.natmtot)) ||
-      (rc = dup(&d.lorbl, st.h_lorbl.data(), st.h_lorbl.size()))) {
+      (rc = dup(&d.lorbl, st.h_lorbl.data(), st.h_lorbl.size())) ||
+      (rc = dup(&d.magmt, (const double*)nullptr, L * r->nrmtmax * st.natmtot)) ||
+      (rc = dup(&d.coef2, (const cplx*)nullptr, 2 * d.ncoef)) ||
+      (rc = dup(&d.lo1, (const cplx*)nullptr, (size_t)std::max(st.maxnlo, 1) * st.natmtot * std::max(st.nstfv, 1))) ||
+      (rc = dup(&d.lo2, (const cplx*)nullptr,
+                (size_t)2 * std::max(st.maxnlo, 1) * st.natmtot * std::max(st.nstfv, 1))) ||
+      (rc = dup(&d.esv, (const cplx*)nullptr, (size_t)2 * std::max(st.nstfv, 1) * std::max(st.nstfv, 1)))) {
     free_rho(d);
     return rc;
   }
@@ -238,11 +298,84 @@ int stage_rhovalk(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, cons
   a.lo_lm = st.lo_lm; a.lo_ilo = st.lo_ilo; a.lo_first = d.lo_first; a.lorbl = d.lorbl;
   a.ucoarse = d.ucoarse; a.vcoarse = d.vcoarse; a.zb = d.zb; a.rf = d.rf; a.coef = d.coef;
   a.evec = evec; a.ldev = ldev; a.w = d.w; a.rhomt = d.rhomt;
+  a.locoef = nullptr; a.ldlo = 0; a.cut = 1; a.magmt = nullptr; a.msign = 0.0;
   const size_t smem = sizeof(cplx) * ((size_t)L * L + (size_t)L * JB) + sizeof(double) * L;
   if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(k_rho_mt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid(d.nrcmax, st.natmtot);
   k_rho_mt<<<grid, 128, smem, s>>>(a);
   count_launch();
   CUDA_TRY(cudaGetLastError());
+  return EXCFV_OK;
+}
+
+// rhomt and magmt += the k-point's density with second-variational vectors
+// evecsv (2 nstfv x 2 nstfv, device, ld 2 nstfv) for a collinear field; the
+// weights wocc (2 nstfv) on the host
+int stage_rhovalk_sv(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, const cplx* evec, long long ldev,
+                     const cplx* evecsv, const double* wocc, double epsocc) {
+  DevStatic& st = h->st;
+  DevRho& d = h->rho;
+  cudaStream_t s = h->stream;
+  const int n = st.nstfv, n2 = 2 * st.nstfv;
+  const int L = d.lmmaxvr;
+  const long long M = (long long)st.apwordmax * L;
+  const int nlo1 = std::max(st.maxnlo, 1);
+  const long long LM = (long long)nlo1 * st.natmtot;
+  std::vector<double> w(n2);
+  for (int j = 0; j < n2; ++j) w[j] = (fabs(wocc[j]) > epsocc) ? wocc[j] : 0.0;
+  CUDA_TRY(cudaMemcpyAsync(d.w, w.data(), sizeof(double) * n2, cudaMemcpyHostToDevice, s));
+  bind_gemm_ctx(h);
+  int rc;
+  // first-variational coefficients, then wavefmt_add's cut-off
+  ZgemmArgs z;
+  z.m = (int)M; z.n = n; z.k = ngp;
+  z.alpha = cmk(1.0, 0.0); z.beta = cmk(0.0, 0.0);
+  z.A = apwalm; z.lda = ngkmax; z.strideA = (long long)ngkmax * st.apwordmax * st.lmmaxapw;
+  z.B = evec; z.ldb = ldev; z.strideB = 0;
+  z.C = d.coef; z.ldc = M; z.strideC = M * n;
+  z.batch = st.natmtot; z.uplo_c = TRI_NONE; z.tri_a = TRI_NONE; z.tri_b = TRI_NONE;
+  z.splitk = 1; z.part = nullptr; z.kdec = 0;
+  if ((rc = zgemm(s, OP_T, OP_N, z))) return rc;
+  const long long nc = M * n * st.natmtot;
+  k_rho_cut<<<(unsigned)((nc + 255) / 256), 256, 0, s>>>(nc, d.coef);
+  count_launch();
+  k_rho_gather_lo<<<(unsigned)((LM * n + 255) / 256), 256, 0, s>>>(st.natmtot, nlo1, n, ngp, st.lo_lm,
+                                                                    d.lo_first, evec, ldev, d.lo1);
+  count_launch();
+  CUDA_TRY(cudaGetLastError());
+  RhoArgs a;
+  a.natmtot = st.natmtot; a.lmaxvr = d.lmaxvr; a.lmmaxvr = L; a.lradstep = d.lradstep; a.nrcmax = d.nrcmax;
+  a.nrmtmax = d.nrmtmax; a.apwordmax = st.apwordmax; a.nlomax = std::max(st.nlomax, 1);
+  a.maxnlo = nlo1; a.nst = n2; a.ngp = ngp;
+  a.idxis = st.idxis; a.nrmt = d.nrmt; a.apword = st.apword; a.lmaxapw = st.lmaxapw;
+  a.lo_lm = st.lo_lm; a.lo_ilo = st.lo_ilo; a.lo_first = d.lo_first; a.lorbl = d.lorbl;
+  a.ucoarse = d.ucoarse; a.vcoarse = d.vcoarse; a.zb = d.zb; a.rf = d.rf; a.coef = d.coef2;
+  a.evec = evec; a.ldev = ldev; a.locoef = d.lo2; a.ldlo = LM; a.cut = 0;
+  a.w = d.w; a.rhomt = d.rhomt; a.magmt = d.magmt;
+  const size_t smem = sizeof(cplx) * ((size_t)L * L + (size_t)L * JB) + sizeof(double) * L;
+  if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(k_rho_mt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  for (int spin = 0; spin < 2; ++spin) {
+    k_rho_esv<<<(unsigned)(((long long)n * n2 + 255) / 256), 256, 0, s>>>(n, spin, evecsv, epsocc, d.esv);
+    count_launch();
+    CUDA_TRY(cudaGetLastError());
+    // the spinor component's coefficients: c (per atom) and the LO rows times esv
+    ZgemmArgs g;
+    g.m = (int)M; g.n = n2; g.k = n;
+    g.alpha = cmk(1.0, 0.0); g.beta = cmk(0.0, 0.0);
+    g.A = d.coef; g.lda = M; g.strideA = M * n;
+    g.B = d.esv; g.ldb = n; g.strideB = 0;
+    g.C = d.coef2; g.ldc = M; g.strideC = M * n2;
+    g.batch = st.natmtot; g.uplo_c = TRI_NONE; g.tri_a = TRI_NONE; g.tri_b = TRI_NONE;
+    g.splitk = 1; g.part = nullptr; g.kdec = 0;
+    if ((rc = zgemm(s, OP_N, OP_N, g))) return rc;
+    g.m = (int)LM; g.A = d.lo1; g.lda = LM; g.strideA = 0;
+    g.C = d.lo2; g.ldc = LM; g.strideC = 0; g.batch = 1;
+    if ((rc = zgemm(s, OP_N, OP_N, g))) return rc;
+    a.msign = spin == 0 ? 1.0 : -1.0;
+    dim3 grid(d.nrcmax, st.natmtot);
+    k_rho_mt<<<grid, 128, smem, s>>>(a);
+    count_launch();
+    CUDA_TRY(cudaGetLastError());
+  }
   return EXCFV_OK;
 }

@@ -92,6 +92,9 @@ SIGNATURES = {
     "excfv_rhovalk_dev": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_int32, C.c_void_p, C.c_void_p, C.c_double]),
     "excfv_get_rhomt": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "excfv_get_magmt": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "excfv_rhovalk_sv": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]),
     "excfv_set_bfield": (C.c_int, [C.c_void_p, C.POINTER(ExcfvBfield)]),
     "excfv_seceqnsv": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

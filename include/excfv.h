@@ -248,9 +248,21 @@ int excfv_rhovalk(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gp
 int excfv_rhovalk_dev(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
                       const double* sfacgp, int32_t nmatmax, const double* evecfv, const double* wocc,
                       double epsocc);
+/* rhovalk with second-variational vectors for a collinear field
+ * (src/rhovalk.f90:74-160, nspinor = 2, ncmag false): each spinor component
+ * of state j is sum_ist evecsv((ispn-1) nstfv + ist, j) times the
+ * first-variational state ist (entries with |Re| + |Im| <= epsocc skipped);
+ * rhomt += up + down and the handle's magmt += up - down.  evecsv complex
+ * (2 nstfv, 2 nstfv) as excfv_seceqnsv returns it, wocc(2 nstfv) =
+ * wkpt(ik) occsv(j, ik); host arrays, synchronous. */
+int excfv_rhovalk_sv(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
+                     const double* sfacgp, int32_t nmatmax, const double* evecfv, const double* evecsv,
+                     const double* wocc, double epsocc);
 /* Copies rhomt (lmmaxvr, nrmtmax, natmtot) to the host (rhomt may be NULL)
  * and, when reset != 0, zeroes the accumulator. */
 int excfv_get_rhomt(excfv_handle* h, double* rhomt, int32_t reset);
+/* The same for the collinear magnetisation magmt (lmmaxvr, nrmtmax, natmtot). */
+int excfv_get_magmt(excfv_handle* h, double* magmt, int32_t reset);
 
 /* ---- the muffin-tin Hamiltonian build (once per SCF iteration) ---------- */
 

@@ -1,7 +1,8 @@
 """Muffin-tin valence density of one k-point (oracle only).
 
 TEST INFRASTRUCTURE ONLY.  Restates, for the spin-unpolarised ground state
-without second-variational vectors (tevecsv false, nspinor = 1):
+without second-variational vectors (tevecsv false, nspinor = 1), and for a
+collinear spin-polarised one with them (``rhovalk_sv``):
 
 ====================  ========================================================
 ``sphcover``          ``src/sphcover.f90``: the generalised spiral covering
@@ -128,3 +129,47 @@ def rhovalk(st, rad, lradstep: int, lmaxvr: int, ngp: int, apwalm: np.ndarray, e
                 rfmt += t1 * (wf3.real ** 2 + wf3.imag ** 2)
         rho[:, irs, ias] += rfsht @ rfmt                                    # dgemv per radial point
     return rho
+
+
+def rhovalk_sv(st, rad, lradstep: int, lmaxvr: int, ngp: int, apwalm: np.ndarray, evecfv: np.ndarray,
+               evecsv: np.ndarray, wocc: np.ndarray, epsocc: float, zbsht: np.ndarray, rfsht: np.ndarray):
+    """rhovalk's branch with spin and second-variational vectors for a
+    collinear field (``src/rhovalk.f90:74-160``: nspinor = 2, ncmag false,
+    no spin spiral): (rhomt_k, magmt_k), each (lmmaxvr, nrmtmax, natmtot).
+
+    For each state j with |wkpt occsv| > epsocc, the spinor component ispn is
+    sum_ist evecsv((ispn-1) nstfv + ist, j) wfmt2(ist), coefficients with
+    |Re| + |Im| <= epsocc skipped, wfmt2(ist) the backward SHT of the
+    first-variational state's wavefmt (taken once per state, the reference's
+    ``done`` cache); rfmt(:,:,ispn) += t1 |.|^2; per coarse radial point
+    rhomt += rflm(1) + rflm(2), magmt += rflm(1) - rflm(2)."""
+    n = st.nstfv
+    lmmaxvr = (lmaxvr + 1) ** 2
+    nrmtmax = rad.spr.shape[0]
+    rho = np.zeros((lmmaxvr, nrmtmax, st.natmtot), order="F")
+    mag = np.zeros((lmmaxvr, nrmtmax, st.natmtot), order="F")
+    for ias in range(st.natmtot):
+        is_ = int(st.idxis[ias])
+        nr = int(rad.nrmt[is_])
+        irs = np.arange(0, nr, lradstep)
+        rfmt = np.zeros((2, lmmaxvr, irs.shape[0]))
+        done = {}
+        for j in range(2 * n):
+            t1 = wocc[j]
+            if abs(t1) <= epsocc:
+                continue
+            wf3 = np.zeros((2, lmmaxvr, irs.shape[0]), dtype=np.complex128)
+            for ispn in range(2):
+                for ist in range(n):
+                    zt1 = evecsv[ispn * n + ist, j]
+                    if abs(zt1.real) + abs(zt1.imag) > epsocc:
+                        if ist not in done:
+                            done[ist] = zbsht @ wavefmt(st, rad, lradstep, lmaxvr, ias, ngp, apwalm,
+                                                        evecfv[:, ist])
+                        wf3[ispn] += zt1 * done[ist]
+            rfmt += t1 * (wf3.real ** 2 + wf3.imag ** 2)
+        up = rfsht @ rfmt[0]
+        dn = rfsht @ rfmt[1]
+        rho[:, irs, ias] += up + dn
+        mag[:, irs, ias] += up - dn
+    return rho, mag

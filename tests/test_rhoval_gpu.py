@@ -79,3 +79,43 @@ def test_rhovalk_device_pointers_equal_host_form():
         fv.sync()
         got = fv.rhomt()
     assert _rel(got, host) < 1e-14
+
+
+@pytest.mark.parametrize("name,kw,lmaxvr,lradstep", [("diamond2", dict(ngk=60, nstfv=6), 4, 2),
+                                                     ("cubic8", dict(ngk=300, nstfv=20), 6, 3)])
+def test_rhovalk_with_second_variational_vectors(name, kw, lmaxvr, lradstep):
+    """The collinear spin-polarised branch: rhomt and magmt against the oracle,
+    with evecsv from the oracle's second variation under a field."""
+    from oracle import secvar
+    p = syn.make_problem(name, **kw)
+    st, kp = p.static, p.kpts[0]
+    rad = syn.make_radial(st, nrmt=140, lmaxvr=lmaxvr)
+    ng, v, c = syn.make_interstitial_real(st)
+    n = st.nstfv
+    apwalm = fvref.match(st, kp)
+    w, X, info = fvref.seceqn(st, kp)
+    assert info == 0
+    L = (lmaxvr + 1) ** 2
+    bxc = np.zeros((L, rad.spr.shape[0], st.natmtot), order="F")
+    for ias in range(st.natmtot):
+        r = rad.spr[:, int(st.idxis[ias])]
+        bxc[0, :, ias] = 0.05 * np.exp(-r) / secvar.Y00
+        bxc[2, :, ias] = 0.01 * r * np.exp(-r)
+    alpha = secvar.bfield_blocks(st, rad, bxc, np.full(st.natmtot, 0.002))
+    evalsv, evecsv = secvar.seceqnsv(st, kp, apwalm, w, X, alpha, 0.004 * c, ng)
+    order = np.argsort(evalsv)
+    wocc = np.zeros(2 * n)
+    wocc[order[:n]] = 1.0                  # the lower half occupied
+    wocc[order[n]] = 1e-12                 # below epsocc: skipped
+    epsocc = 1e-8
+    zb, _, _, rf = rhoval.sht_matrices(lmaxvr)
+    rho_ref, mag_ref = rhoval.rhovalk_sv(st, rad, lradstep, lmaxvr, kp.ngp, apwalm, X, evecsv, wocc, epsocc, zb, rf)
+    with FirstVariational(0) as fv:
+        fv.set_static(st)
+        fv.set_rho(rad, lmaxvr, lradstep, zb, rf)
+        fv.rhovalk_sv(kp, X, evecsv, wocc, epsocc)
+        rho = fv.rhomt(reset=True)
+        mag = fv.magmt(reset=True)
+    assert _rel(rho, rho_ref) < TOL
+    assert np.abs(mag - mag_ref).max() < TOL * np.abs(rho_ref).max()
+    assert np.abs(mag_ref).max() > 1e-6 * np.abs(rho_ref).max()   # the field polarises the density
