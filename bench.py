@@ -535,10 +535,12 @@ def main():
     g_flops = 2 * 8.0 * (N * (N + 1) / 2) * AM
     g_ach = (g_flops / (g_ms / args.steps / 1e3) / 1e12) if g_cnt else None
     # tridiagonal panel: bytes of the lower triangle of the trailing block read
-    # by y = C22 v for every reduced column; p_ms and p_cnt cover all timed
-    # steps, so per launch: (steps * bytes per step / p_cnt) / (p_ms / p_cnt)
+    # by y = C22 v for every column the panel kernel reduces (those before the
+    # cluster kernel's tail); p_ms and p_cnt cover all timed steps, so per
+    # launch: (steps * bytes per step / p_cnt) / (p_ms / p_cnt)
     p_ms, p_cnt = prof["trd_panel"]
-    tot_bytes = sum(16.0 * (n - c - 1) * (n - c) / 2 for c in range(n - 1))
+    c_tail = fv.tridiag_tail_start(n)
+    tot_bytes = sum(16.0 * (n - c - 1) * (n - c) / 2 for c in range(c_tail))
     p_ach = (args.steps * tot_bytes / p_cnt / (p_ms / p_cnt / 1e3) / 1e9) if p_cnt else None
     hbm = peaks.get("hbm_gbs") or 6650.0
     hbm_src = "measured" if peaks.get("hbm_gbs") else "fallback"
@@ -547,6 +549,7 @@ def main():
                 "unit": "GB/s", "frac": (p_ach / hbm) if p_ach else None,
                 "traffic": traffic.get("k_tridiag_panel"),
                 "algorithmic": "16*m(m+1)/2 bytes (lower triangle of the m x m trailing block, y = C22 v) per reduced column, summed over the launch's columns",
+                "panel_columns": c_tail, "tail_columns": n - 1 - c_tail,
                 "peak_source": f"{hbm_src} HBM copy (MEASURED_PEAKS.json)"}
     else:
         roof = {"kernel": "zgemm_kernel (H/O setup)", "bound": "tensor", "achieved": g_ach,

@@ -985,6 +985,11 @@ int excfv_sync(excfv_handle* h) {
 
 long long excfv_launch_count(void) { return g_launches.load(); }
 
+int excfv_tridiag_tail_start(int n, int complex64) {
+  if (n < 1) return 0;
+  return tridiag_tail_start(n, complex64 != 0);
+}
+
 int excfv_set_lattice(excfv_handle* h, const double* vgc, const double* atposc) {
   if (!h || !vgc || !atposc) return EXCFV_ERR_ARG;
   if (!h->have_static) {

@@ -151,7 +151,7 @@ struct DevSV {
 // EXCFV_PROF_* in include/excfv.h.
 enum {
   PROF_MATCH = 0, PROF_SETUP_GEMM, PROF_SETUP_OTHER, PROF_POTRF, PROF_HEGST, PROF_TRD_PANEL,
-  PROF_TRD_UPDATE, PROF_STEIG, PROF_BACKTR, PROF_TRD_CHASE, PROF_NCLS
+  PROF_TRD_UPDATE, PROF_STEIG, PROF_BACKTR, PROF_TRD_CHASE, PROF_TRD_TAIL, PROF_NCLS
 };
 
 struct Prof {
@@ -266,6 +266,9 @@ int stage_solve(excfv_handle* h, int n, int nstfv, double evaltol, double* d_eva
 int mixed_states(int n, int k);
 // rows one CTA of the tridiagonal reduction can own (FP64 or complex64 storage)
 int tridiag_rows_per_cta(bool complex64);
+// the first column of an n x n reduction that goes to the cluster kernel of
+// the last columns (tridiag_tail.cu); n - 1 when the panels take them all
+int tridiag_tail_start(int n, bool complex64);
 int status_to_info(const int* st, int n);
 // device status -> LAPACK-style info (synchronises the stream)
 int stage_status(excfv_handle* h, int n);

@@ -990,6 +990,18 @@ static int make_tile_map(CUtensorMap* tm, const T2* C, int n, long long ld) {
   return EXCFV_OK;
 }
 
+template <typename T2>
+int tridiag_tail_max();
+template <typename T2>
+int tridiag_tail(excfv_handle* h, int n, int c0, T2* C, long long ld);
+
+int tridiag_tail_start(int n, bool complex64) {
+  const int tail_max = complex64 ? tridiag_tail_max<float2>() : tridiag_tail_max<double2>();
+  for (int p = 0; p < n - 1; p += NBT)
+    if (n - p <= tail_max) return p;
+  return n > 0 ? n - 1 : 0;
+}
+
 template <typename T2, int MC>
 static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
   Workspace& ws = h->ws;
@@ -1030,7 +1042,16 @@ static int tridiag_reduce_t(excfv_handle* h, int n, T2* C, long long ld) {
   CUDA_TRY(cudaMemsetAsync(ws.bar, 0, 2 * sizeof(unsigned), s));
   const long long wait_ns = wait_limit_ns();
   const unsigned planted = take_planted_stall() ? 1u : 0u;
+  // the last columns (a trailing block the cluster's shared memory holds) go
+  // to the cluster kernel (tridiag_tail.cu); a planted stall keeps the panels
+  const int p_tail = planted ? n : tridiag_tail_start(n, sizeof(T2) == 8);
   for (int p = 0; p < n - 1; p += NBT) {
+    if (p == p_tail) {
+      prof_begin(h, PROF_TRD_TAIL);
+      if (int rc = tridiag_tail<T2>(h, n, p, C, ld)) return rc;
+      prof_end(h, PROF_TRD_TAIL);
+      break;
+    }
     const int nbp = min(NBT, n - 1 - p);
     const int final_panel = (p + nbp == n - 1) ? 1 : 0;
     const int pi = p / NBT;

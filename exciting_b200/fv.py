@@ -525,6 +525,11 @@ class FirstVariational:
     def launch_count(self) -> int:
         return int(self._L.excfv_launch_count())
 
+    def tridiag_tail_start(self, n: int, complex64: bool = False) -> int:
+        """First column of an n x n tridiagonal reduction that the cluster
+        kernel of the last columns reduces (n - 1: none)."""
+        return int(self._L.excfv_tridiag_tail_start(int(n), 1 if complex64 else 0))
+
     def timings(self):
         t = np.zeros(4)
         self._L.excfv_get_timings(self._h, _ptr(t))

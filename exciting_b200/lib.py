@@ -123,6 +123,7 @@ SIGNATURES = {
     "excfv_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "excfv_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "excfv_launch_count": (C.c_longlong, []),
+    "excfv_tridiag_tail_start": (C.c_int, [C.c_int, C.c_int]),
     "excfv_test_set_wait_limit": (C.c_int, [C.c_int64, C.c_int32]),
     "excfv_set_reduction": (C.c_int, [C.c_void_p, C.c_int]),
     "excfv_set_lattice": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -160,7 +161,7 @@ SIGNATURES = {
 NOALLOC_SCRATCH_BYTES = 32 << 20
 
 PROF_CLASSES = ["match", "setup_gemm", "setup_other", "potrf", "hegst", "trd_panel",
-                "trd_update", "steig", "backtr", "trd_chase"]
+                "trd_update", "steig", "backtr", "trd_chase", "trd_tail"]
 
 EXCFV_REDUCTION_AUTO = 0
 EXCFV_REDUCTION_ONE_STAGE = 1

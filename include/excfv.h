@@ -443,12 +443,20 @@ int excfv_get_timings(excfv_handle* h, double* t4);
 #define EXCFV_PROF_STEIG 7       /* bisection + inverse iteration            */
 #define EXCFV_PROF_BACKTR 8      /* orthonormalisation + back-transforms     */
 #define EXCFV_PROF_TRD_CHASE 9   /* band -> tridiagonal bulge chase + phase  */
-#define EXCFV_PROF_NCLS 10
+#define EXCFV_PROF_TRD_TAIL 10   /* last columns of the tridiagonal reduction */
+#define EXCFV_PROF_NCLS 11
 int excfv_profile(excfv_handle* h, int enable);
 int excfv_profile_read(excfv_handle* h, double* ms, long long* count, int nclasses);
 
 /* Number of kernels this library has launched in the process so far. */
 long long excfv_launch_count(void);
+
+/* The first column of the tridiagonal reduction of an n x n matrix that its
+ * cluster kernel reduces (the trailing block from there on fits in the
+ * cluster's shared memory; the panel kernel takes the columns before it);
+ * n - 1 when no column goes there.  complex64 != 0 for the precision form's
+ * complex64 storage, 0 for FP64. */
+int excfv_tridiag_tail_start(int n, int complex64);
 
 /*
  * Test aid (no counterpart in the reference): sets the time limit of every
