@@ -352,7 +352,7 @@ int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax) {
       (rc = dalloc(&ws.stein_ws, tridiag_eig_scratch_doubles((int)n, (int)K))) ||
       (rc = dalloc(&ws.icl, K)) || (rc = dalloc(&ws.ybuf, 2 * n)) || (rc = dalloc(&ws.Z, n * K)) ||
       (rc = dalloc(&ws.Z2, n * K)) || (rc = dalloc(&ws.Gk, K * K)) || (rc = dalloc(&ws.Gki, K * K)) ||
-      (rc = dalloc(&ws.Tf, 2 * ((n + 63) / 64 + 1) * 64 * 64)) || (rc = dalloc(&ws.Xs, 2 * 64 * K)) ||
+      (rc = dalloc(&ws.Tf, backtr_factor_elems((int)n))) || (rc = dalloc(&ws.Xs, 2 * 256 * K)) ||
       (rc = dalloc(&ws.status, (size_t)ST_NWORDS)) || (rc = dalloc(&ws.bar, (size_t)4)) ||
       (rc = dalloc(&ws.prog, n)) ||
       (rc = dalloc(&ws.part, std::max((size_t)(8u << 20), n * 64 * 4)))) {

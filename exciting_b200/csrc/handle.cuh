@@ -269,6 +269,10 @@ int tridiag_rows_per_cta(bool complex64);
 // the first column of an n x n reduction that goes to the cluster kernel of
 // the last columns (tridiag_tail.cu); n - 1 when the panels take them all
 int tridiag_tail_start(int n, bool complex64);
+// elements of ws.Tf the back-transform needs for nrefl reflectors: the Gram
+// matrices and block-reflector factors of 256-wide blocks and their merge
+// scratch (solve.cu); ws.Xs holds 2 x 256 x kmax
+size_t backtr_factor_elems(int nrefl);
 int status_to_info(const int* st, int n);
 // device status -> LAPACK-style info (synchronises the stream)
 int stage_status(excfv_handle* h, int n);

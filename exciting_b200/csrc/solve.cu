@@ -24,14 +24,24 @@ int tridiag_reduce_f32(excfv_handle* h, int n, float2* C, long long ld);
 
 namespace {
 
-constexpr int NBQ = 64;  // reflectors per block of the back-transform
+constexpr int NBQ = 64;   // reflectors per block of k_larft's recurrence
+constexpr int NBW = 256;  // reflectors per block of the back-transform
+constexpr long long WST = (long long)NBW * (NBW + 1);  // storage stride of one NBW block
 constexpr int LT = 256;
+
+// The Gram matrices G = V^H V and the factors T of the NBW-wide blocks are
+// stored with leading dimension NBW and a block stride of NBW (NBW + 1)
+// elements: element (r, c) of block B at B NBW (NBW + 1) + r + NBW c.  The
+// diagonal sub-block starting at reflector g (global index) then sits at
+// g (NBW + 1), whichever block it belongs to, so every level of the T merge
+// below is one batched GEMM with a uniform stride.
 
 // Triangular factor of the block reflector H_p ... H_{p+nb-1} = I - V T V^H
 // (forward, columnwise: T(i,i) = tau_i, T(0:i,i) = -tau_i T(0:i,0:i) G(0:i,i)
-// with G = V^H V from a batched GEMM).  One CTA per block; G and T live in
-// shared memory, four threads share each row of the triangular product.
-__global__ void __launch_bounds__(LT) k_larft(int n, const cplx* Gall, const cplx* tau, cplx* Tf) {
+// with G = V^H V), for the NBQ-wide diagonal sub-blocks of the NBW blocks.
+// One CTA per sub-block; G and T live in shared memory, four threads share
+// each row of the triangular product.
+__global__ void __launch_bounds__(LT) k_larft(int n, const cplx* Gbig, const cplx* tau, cplx* Tbig) {
   extern __shared__ __align__(16) unsigned char dsm[];
   cplx (*G)[NBQ + 1] = reinterpret_cast<cplx (*)[NBQ + 1]>(dsm);
   cplx (*T)[NBQ + 1] = reinterpret_cast<cplx (*)[NBQ + 1]>(dsm + sizeof(cplx) * NBQ * (NBQ + 1));
@@ -40,10 +50,10 @@ __global__ void __launch_bounds__(LT) k_larft(int n, const cplx* Gall, const cpl
   const int nb = min(NBQ, n - 1 - p);
   if (nb <= 0) return;
   const int tid = threadIdx.x;
-  const cplx* Gb = Gall + (size_t)blk * NBQ * NBQ;
+  const cplx* Gb = Gbig + (size_t)p * (NBW + 1);
   for (int t = tid; t < NBQ * NBQ; t += LT) {
     const int r = t % NBQ, c = t / NBQ;
-    G[r][c] = Gb[t];
+    G[r][c] = Gb[r + (size_t)NBW * c];
     T[r][c] = cmk(0.0, 0.0);
   }
   __syncthreads();
@@ -64,8 +74,8 @@ __global__ void __launch_bounds__(LT) k_larft(int n, const cplx* Gall, const cpl
     if (tid == 0) T[i][i] = ti;
     __syncthreads();
   }
-  cplx* out = Tf + (size_t)blk * NBQ * NBQ;
-  for (int t = tid; t < NBQ * NBQ; t += LT) out[t] = T[t % NBQ][t / NBQ];
+  cplx* out = Tbig + (size_t)p * (NBW + 1);
+  for (int t = tid; t < NBQ * NBQ; t += LT) out[t % NBQ + (size_t)NBW * (t / NBQ)] = T[t % NBQ][t / NBQ];
 }
 
 // n x n FP64 (leading dimension ldi) -> complex64 (leading dimension ldo)
@@ -347,57 +357,93 @@ __global__ void k_copy_eval(int k, const double* w, double* out) {
 // Z (n x k) <- Q Z with Q = H_0 ... H_{n-1-off}: reflector c stored in
 // column c of C from row c + off down, unit entry explicit (off = 1 for the
 // one-stage reduction, the bandwidth for stage 1 of the two-stage one).
+size_t backtr_factor_elems(int nrefl) {
+  const long long nblk = (nrefl + NBW - 1) / NBW;
+  return (size_t)(2 * nblk * WST + nblk * (NBW / 2) * (NBW / 2) + NBW);
+}
+
 int apply_q(excfv_handle* h, int n, int k, const cplx* C, long long ld, cplx* Z, long long ldz,
             int off) {
   Workspace& ws = h->ws;
   cudaStream_t s = h->stream;
   const int nrefl = n - off;
   if (nrefl < 1) return EXCFV_OK;
-  const int nblk = (nrefl + NBQ - 1) / NBQ;
+  const int nblk = (nrefl + NBW - 1) / NBW;
   const cplx one = cmk(1.0, 0.0), mone = cmk(-1.0, 0.0), zero = cmk(0.0, 0.0);
-  cplx* Gall = ws.Tf + (size_t)nblk * NBQ * NBQ;
-  // Gram matrices G_b = V_b^H V_b: the full blocks in one batched GEMM
-  // (K shrinks by NBQ from block to block), the last partial block alone.
-  const int nfull = nrefl / NBQ;
+  cplx* Tbig = ws.Tf;
+  cplx* Gbig = ws.Tf + (size_t)nblk * WST;
+  cplx* Xm = Gbig + (size_t)nblk * WST;  // scratch of the T merge
+  const int nfull = nrefl / NBW;
+  // a partial last block: the parts past nrefl must read as zero (identity
+  // reflectors) in the T recurrence and the merge
+  if (nfull < nblk) {
+    CUDA_TRY(cudaMemsetAsync(Tbig + (size_t)nfull * WST, 0, sizeof(cplx) * WST, s));
+    CUDA_TRY(cudaMemsetAsync(Gbig + (size_t)nfull * WST, 0, sizeof(cplx) * WST, s));
+  }
+  // Gram matrices G_B = V_B^H V_B (upper): the full blocks in one batched
+  // GEMM (K shrinks by NBW from block to block), the last partial block alone
   if (nfull > 0) {
     ZgemmArgs g;
-    g.m = NBQ; g.n = NBQ; g.k = n - off; g.kdec = NBQ;
+    g.m = NBW; g.n = NBW; g.k = n - off; g.kdec = NBW;
     g.alpha = one; g.beta = zero;
-    g.A = C + off; g.lda = ld; g.strideA = (long long)NBQ * (ld + 1);
-    g.B = C + off; g.ldb = ld; g.strideB = (long long)NBQ * (ld + 1);
-    g.C = Gall; g.ldc = NBQ; g.strideC = (long long)NBQ * NBQ;
+    g.A = C + off; g.lda = ld; g.strideA = (long long)NBW * (ld + 1);
+    g.B = C + off; g.ldb = ld; g.strideB = (long long)NBW * (ld + 1);
+    g.C = Gbig; g.ldc = NBW; g.strideC = WST;
     g.batch = nfull; g.uplo_c = TRI_UPPER; g.tri_a = TRI_UPPER; g.tri_b = TRI_LOWER;
     g.splitk = 1; g.part = nullptr;
     int rc = zgemm(s, OP_C, OP_N, g);
     if (rc) return rc;
   }
   if (nfull < nblk) {
-    const int p = nfull * NBQ;
+    const int p = nfull * NBW;
     const int nb = nrefl - p, m = n - p - off;
     const cplx* V = C + (p + off) + ld * p;
-    int rc = zgemm1(s, OP_C, OP_N, nb, nb, m, one, V, ld, V, ld, zero, Gall + (size_t)nfull * NBQ * NBQ,
-                    NBQ, TRI_UPPER, TRI_UPPER, TRI_LOWER);
+    int rc = zgemm1(s, OP_C, OP_N, nb, nb, m, one, V, ld, V, ld, zero, Gbig + (size_t)nfull * WST, NBW,
+                    TRI_UPPER, TRI_UPPER, TRI_LOWER);
     if (rc) return rc;
   }
+  // T of the NBQ-wide diagonal sub-blocks, then merged level by level:
+  //   T([V1 V2]) = [[T1, -T1 (V1^H V2) T2], [0, T2]]
+  // (all pairs of one level in two batched GEMMs over the uniform stride)
   const int smem = (int)(2 * sizeof(cplx) * NBQ * (NBQ + 1));
   CUDA_TRY(cudaFuncSetAttribute(k_larft, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  k_larft<<<nblk, LT, smem, s>>>(nrefl + 1, Gall, ws.tau, ws.Tf); count_launch();
+  k_larft<<<nblk * (NBW / NBQ), LT, smem, s>>>(nrefl + 1, Gbig, ws.tau, Tbig); count_launch();
   CUDA_TRY(cudaGetLastError());
+  for (int bs = NBQ; bs < NBW; bs *= 2) {
+    const long long step = 2LL * bs * (NBW + 1);
+    const int npair = nblk * (NBW / (2 * bs));
+    ZgemmArgs g;
+    g.m = bs; g.n = bs; g.k = bs; g.kdec = 0; g.alpha = one; g.beta = zero;
+    g.A = Gbig + (size_t)bs * NBW; g.lda = NBW; g.strideA = step;         // G12
+    g.B = Tbig + (size_t)bs * (NBW + 1); g.ldb = NBW; g.strideB = step;  // T2
+    g.C = Xm; g.ldc = bs; g.strideC = (long long)bs * bs;                 // G12 T2
+    g.batch = npair; g.uplo_c = TRI_NONE; g.tri_a = TRI_NONE; g.tri_b = TRI_UPPER;
+    g.splitk = 1; g.part = nullptr;
+    int rc = zgemm(s, OP_N, OP_N, g);
+    if (rc) return rc;
+    g.alpha = mone;
+    g.A = Tbig; g.strideA = step;                                         // T1
+    g.B = Xm; g.ldb = bs; g.strideB = (long long)bs * bs;
+    g.C = Tbig + (size_t)bs * NBW; g.ldc = NBW; g.strideC = step;         // T12
+    g.tri_a = TRI_UPPER; g.tri_b = TRI_NONE;
+    rc = zgemm(s, OP_N, OP_N, g);
+    if (rc) return rc;
+  }
   cplx* X1 = ws.Xs;
-  cplx* X2 = ws.Xs + (size_t)NBQ * ws.kmax;
+  cplx* X2 = ws.Xs + (size_t)NBW * ws.kmax;
   for (int b = nblk - 1; b >= 0; --b) {
-    const int p = b * NBQ;
-    const int nb = min(NBQ, nrefl - p);
+    const int p = b * NBW;
+    const int nb = min(NBW, nrefl - p);
     const int m = n - p - off;
     const cplx* V = C + (p + off) + ld * p;
     cplx* Zs = Z + (p + off);
-    int rc = zgemm1(s, OP_C, OP_N, nb, k, m, one, V, ld, Zs, ldz, zero, X1, NBQ, TRI_NONE,
+    int rc = zgemm1(s, OP_C, OP_N, nb, k, m, one, V, ld, Zs, ldz, zero, X1, NBW, TRI_NONE,
                     TRI_UPPER, TRI_NONE);
     if (rc) return rc;
-    rc = zgemm1(s, OP_N, OP_N, nb, k, nb, one, ws.Tf + (size_t)b * NBQ * NBQ, NBQ, X1, NBQ, zero,
-                X2, NBQ, TRI_NONE, TRI_UPPER, TRI_NONE);
+    rc = zgemm1(s, OP_N, OP_N, nb, k, nb, one, Tbig + (size_t)b * WST, NBW, X1, NBW, zero,
+                X2, NBW, TRI_NONE, TRI_UPPER, TRI_NONE);
     if (rc) return rc;
-    rc = zgemm1(s, OP_N, OP_N, m, k, nb, mone, V, ld, X2, NBQ, one, Zs, ldz, TRI_NONE, TRI_LOWER,
+    rc = zgemm1(s, OP_N, OP_N, m, k, nb, mone, V, ld, X2, NBW, one, Zs, ldz, TRI_NONE, TRI_LOWER,
                 TRI_NONE);
     if (rc) return rc;
   }
