@@ -604,16 +604,30 @@ int excfv_set_bfield(excfv_handle* h, const excfv_bfield* b) {
   return stage_set_bfield(h, b);
 }
 
+int excfv_set_bfield_nc(excfv_handle* h, const excfv_bfield_nc* b) {
+  if (!h || !b) return EXCFV_ERR_ARG;
+  if (!h->have_static) {
+    excfv_set_error("excfv_set_static must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  DeviceGuard g(h->device);
+  cudaStreamSynchronize(h->stream);
+  return stage_set_bfield_nc(h, b);
+}
+
 // the k-point's G+k data into the workspace and its packed matching coefficients
 static int sv_stage_k(excfv_handle* h, int ngp, int ngkmax, int nmatmax, const double* gpc, const double* tpgpc,
                       const double* sfacgp, const int32_t* igpig, cudaMemcpyKind kind) {
   int rc;
-  if ((rc = stage_reserve(h, nmatmax, ngkmax, std::max(1, h->st.nstfv)))) return rc;
+  // the eigenproblem's order: nstfv per spin block, 2 nstfv for a non-collinear field
+  const int nsv = std::max(1, h->st.nstfv) * (h->sv.nc ? 2 : 1);
+  const int nmat = std::max(nmatmax, nsv);
+  if ((rc = stage_reserve(h, nmat, ngkmax, nsv))) return rc;
   Workspace& ws = h->ws;
   if (ngkmax != ws.ngkmax) {
     cudaStreamSynchronize(h->stream);
     free_workspace(ws);
-    if ((rc = stage_reserve(h, nmatmax, ngkmax, std::max(1, h->st.nstfv)))) return rc;
+    if ((rc = stage_reserve(h, nmat, ngkmax, nsv))) return rc;
   }
   cudaStream_t s = h->stream;
   CUDA_TRY(cudaMemcpyAsync(ws.gpc, gpc, sizeof(double) * ngp, kind, s));

@@ -133,7 +133,16 @@ struct DevRho {
 // interstitial field over the whole grid, scratch.
 struct DevSV {
   bool ready = false;
+  bool nc = false;        // non-collinear field (ndmag = 3): one solve of order 2 nstfv
+  bool so = false;        // spin-orbit terms in the blocks: alpha's alo = loa^H, else loa^T
   int ngrid[3] = {0, 0, 0};
+  // non-collinear: the up-down blocks (ab of mt_hscf, alo explicit) and field
+  cplx* ab_aa = nullptr;     // (maxaa, maxaa, natmtot)
+  cplx* ab_loa = nullptr;    // (maxnlo, maxaa, natmtot)
+  cplx* ab_alo = nullptr;    // (maxaa, maxnlo, natmtot)
+  cplx* ab_lolo = nullptr;   // (maxnlo, maxnlo, natmtot)
+  cplx* birhat_xy = nullptr; // (ngrtot) forward transform of (bir1 - i bir2) / ngrtot
+  cplx* Sud = nullptr;       // (nstfv, nstfv) the up-down block
   cplx* aa = nullptr;     // (maxaa, maxaa, natmtot)
   cplx* loa = nullptr;    // (maxnlo, maxaa, natmtot)
   cplx* lolo = nullptr;   // (maxnlo, maxnlo, natmtot)
@@ -238,6 +247,10 @@ int stage_rhovalk_sv(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, c
 void free_rho(DevRho& r);
 // second variation, collinear field (secvar.cu)
 int stage_set_bfield(excfv_handle* h, const excfv_bfield* b);
+int stage_set_bfield_nc(excfv_handle* h, const excfv_bfield_nc* b);
+// spline.f90's cubic spline on the host: the integral over the mesh, and
+// (d1 != NULL) the first derivative at each point (fderiv(1)) (mtbuild.cu)
+double host_spline(int n, const double* x, const double* f, double* d1);
 int stage_seceqnsv(excfv_handle* h, int ngp, const cplx* evec, long long ldev, const double* d_evalfv,
                    double* d_evalsv, cplx* d_evecsv);
 void free_sv(DevSV& v);

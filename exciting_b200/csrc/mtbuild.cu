@@ -558,3 +558,24 @@ int stage_mt_field(excfv_handle* h, const excfv_mtrad* r, const double* field, c
                    double* aa_out, double* loa_out, double* lolo_out) {
   return mt_build(h, r, field, false, false, aa, loa, lolo, aa_out, loa_out, lolo_out, nullptr, nullptr);
 }
+
+// The cubic spline of spline.f90 on the host: d1 = cf(1, :), the first
+// derivative at each mesh point (fderiv(1)); returns the integral over the
+// whole mesh (fderiv(-1) at the last point) of f.
+double host_spline(int n, const double* x, const double* f, double* d1) {
+  std::vector<double> c1(n), c2(n), c3(n), w(n);
+  const double g = spline_integral(n, x, f, c1, c2, c3, w);
+  if (d1) {
+    // spline_integral leaves c1 = the divided differences and c2 = the second
+    // coefficients; the first coefficients follow as in spline.f90
+    for (int i = 0; i < n - 1; ++i) {
+      const double d3 = (1.0 / 3.0) * (c2[i + 1] - c2[i]) * w[i];
+      const double dx = x[i + 1] - x[i];
+      d1[i] = c1[i] - (c2[i] + d3 * dx) * dx;
+    }
+    const double dxl = x[n - 1] - x[n - 2];
+    const double d3l = (1.0 / 3.0) * (c2[n - 1] - c2[n - 2]) * w[n - 2];
+    d1[n - 1] = d1[n - 2] + (2.0 * c2[n - 2] + 3.0 * d3l * dxl) * dxl;
+  }
+  return g;
+}

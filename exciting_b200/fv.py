@@ -222,8 +222,31 @@ class FirstVariational:
         b.birconst = float(birconst)
         self._check(self._L.excfv_set_bfield(self._h, C.byref(b)), "excfv_set_bfield")
 
+    def set_bfield_nc(self, rad, bxcmt, bmtconst, ngrid, bxcir, cfunir, birconst, spinorb: bool = False) -> None:
+        """A non-collinear field (bxcmt (lmmaxvr, nrmtmax, natmtot, 3), bmtconst
+        (3, natmtot), bxcir (ngrtot, 3), birconst (3)) and, with ``spinorb``,
+        the spin-orbit terms of mt_so: mt_hscf%alpha and ab and the
+        interstitial fields, built on the device.  ``seceqnsv`` then solves
+        the whole matrix of order 2 nstfv."""
+        keep = []
+        r = self._mtrad(rad, keep)
+        arrs = [_f(bxcmt, np.float64), _f(bmtconst, np.float64), _f(ngrid, np.int32), _f(bxcir, np.float64),
+                _f(cfunir, np.float64)]
+        b = _lib.ExcfvBfieldNc()
+        b.rad = C.pointer(r)
+        b.bxcmt = arrs[0].ctypes.data_as(_lib._f64p)
+        b.bmtconst = arrs[1].ctypes.data_as(_lib._f64p)
+        b.ngrid = arrs[2].ctypes.data_as(_lib._i32p)
+        b.bxcir = arrs[3].ctypes.data_as(_lib._f64p)
+        b.cfunir = arrs[4].ctypes.data_as(_lib._f64p)
+        for d in range(3):
+            b.birconst[d] = float(birconst[d])
+        b.spinorb = 1 if spinorb else 0
+        self._check(self._L.excfv_set_bfield_nc(self._h, C.byref(b)), "excfv_set_bfield_nc")
+
     def seceqnsv(self, kp, evalfv, evecfv) -> Tuple[np.ndarray, np.ndarray]:
-        """``seceqnsv`` for the collinear field: (evalsv (2 nstfv), evecsv (2 nstfv, 2 nstfv))."""
+        """``seceqnsv``: (evalsv (2 nstfv), evecsv (2 nstfv, 2 nstfv)); block
+        diagonal for a collinear field, full after ``set_bfield_nc``."""
         n = self.static.nstfv
         w = _f(evalfv, np.float64)
         ev = _f(evecfv, np.complex128)

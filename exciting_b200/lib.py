@@ -73,6 +73,14 @@ class ExcfvBfield(C.Structure):
     ]
 
 
+class ExcfvBfieldNc(C.Structure):
+    """Mirror of ``struct excfv_bfield_nc`` (field order and types must match)."""
+    _fields_ = [
+        ("rad", C.POINTER(ExcfvMtrad)), ("bxcmt", _f64p), ("bmtconst", _f64p), ("ngrid", _i32p),
+        ("bxcir", _f64p), ("cfunir", _f64p), ("birconst", C.c_double * 3), ("spinorb", C.c_int32),
+    ]
+
+
 #: name -> (restype, argtypes); every symbol declared in include/excfv.h
 SIGNATURES = {
     "excfv_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -96,6 +104,7 @@ SIGNATURES = {
     "excfv_rhovalk_sv": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]),
     "excfv_set_bfield": (C.c_int, [C.c_void_p, C.POINTER(ExcfvBfield)]),
+    "excfv_set_bfield_nc": (C.c_int, [C.c_void_p, C.POINTER(ExcfvBfieldNc)]),
     "excfv_seceqnsv": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "excfv_seceqnsv_dev": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -313,6 +313,28 @@ typedef struct excfv_bfield {
  * and the interstitial field bir = (bxcir + birconst) cfunir in Fourier space
  * on the device. */
 int excfv_set_bfield(excfv_handle* h, const excfv_bfield* b);
+/* The non-collinear field (ndmag = 3: a field with x or y parts, or spin-orbit
+ * coupling, init0.f90:190-203) of seceqnsv on its default path.  Host
+ * pointers, read during excfv_set_bfield_nc. */
+typedef struct excfv_bfield_nc {
+  const excfv_mtrad* rad;   /* radial data; veffmt's lm = 0 part feeds the spin-orbit term */
+  const double* bxcmt;      /* (lmmaxvr, nrmtmax, natmtot, 3): bxcmt(:,:,:,1:3) */
+  const double* bmtconst;   /* (3, natmtot): ga4 (bfcmt(:) + bfieldc(:)) of each atom, added to the
+                               spherical part of each component (hmlint.f90:63-135) */
+  const int32_t* ngrid;     /* (3) the real-space grid */
+  const double* bxcir;      /* (ngrtot, 3) bxcir(:,1:3) */
+  const double* cfunir;     /* (ngrtot) */
+  double birconst[3];       /* ga4 bfieldc(1:3) (seceqnsv.f90:662-665) */
+  int32_t spinorb;          /* != 0: add the spin-orbit terms of mt_so (isspinorb) */
+} excfv_bfield_nc;
+
+/* Builds mt_hscf%alpha (mt_pot of the z field), beta = -alpha and ab =
+ * mt_pot(x field) - i mt_pot(y field) (hmlint.f90:63-135), with spinorb the
+ * spin-orbit terms of src/src_eigensystem/mt_so.f90 (level_zora; alpha's alo
+ * then conj(loa)^T), and the interstitial fields bir3 and bir1 - i bir2 in
+ * Fourier space.  excfv_seceqnsv then solves the whole second-variational
+ * matrix at once. */
+int excfv_set_bfield_nc(excfv_handle* h, const excfv_bfield_nc* b);
 /* seceqnsv (src/seceqnsv.f90:10) for a collinear field without spin-orbit
  * coupling and LDA+U: the first-variational states' matrix of the field (the
  * muffin-tin contractions with alpha, the interstitial product of each
@@ -321,8 +343,13 @@ int excfv_set_bfield(excfv_handle* h, const excfv_bfield* b);
  * k-point's G+k data as excfv_seceqn (gpc, tpgpc, sfacgp, igpig), evalfv
  * (nstfv) and evecfv complex (nmatmax, nstfv); outputs evalsv (2 nstfv: the
  * up block's eigenvalues, then the down block's) and evecsv complex
- * (2 nstfv, 2 nstfv), block diagonal.  The host form is synchronous; the
- * _dev form takes device arrays (all of them) and is asynchronous. */
+ * (2 nstfv, 2 nstfv), block diagonal.  After excfv_set_bfield_nc the whole
+ * matrix is one Hermitian eigenproblem of order 2 nstfv (ZHEEV('V','U'),
+ * ndmag = 3): up-up from alpha and bir3, down-down from beta = -alpha and
+ * -bir3, each with evalfv on the diagonal, up-down from ab and bir1 - i bir2;
+ * evalsv ascending, evecsv full.  The host form
+ * is synchronous; the _dev form takes device arrays (all of them) and is
+ * asynchronous. */
 int excfv_seceqnsv(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
                    const double* sfacgp, const int32_t* igpig, int32_t nmatmax, const double* evalfv,
                    const double* evecfv, double* evalsv, double* evecsv);

@@ -42,13 +42,17 @@ def test_library_exports_every_declared_symbol(lib):
         assert name in L.SIGNATURES, f"{name} has no ctypes signature"
 
 
-def test_static_struct_layout_matches_c(lib):
-    from exciting_b200.lib import ExcfvStatic
-    fields = [f for f, _ in ExcfvStatic._fields_]
+@pytest.mark.parametrize("pyname,cname", [("ExcfvStatic", "excfv_static"), ("ExcfvMtrad", "excfv_mtrad"),
+                                           ("ExcfvRhoset", "excfv_rhoset"), ("ExcfvBfield", "excfv_bfield"),
+                                           ("ExcfvBfieldNc", "excfv_bfield_nc")])
+def test_struct_layout_matches_c(lib, pyname, cname):
+    from exciting_b200 import lib as L
+    cls = getattr(L, pyname)
+    fields = [f for f, _ in cls._fields_]
     prog = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){",
-            'printf("%zu\\n", sizeof(excfv_static));']
+            f'printf("%zu\\n", sizeof({cname}));']
     for f in fields:
-        prog.append(f'printf("%zu\\n", offsetof(excfv_static, {f}));')
+        prog.append(f'printf("%zu\\n", offsetof({cname}, {f}));')
     prog.append("return 0;}")
     with tempfile.TemporaryDirectory() as d:
         c = os.path.join(d, "t.c")
@@ -57,9 +61,9 @@ def test_static_struct_layout_matches_c(lib):
         subprocess.run(["gcc", "-O0", "-o", exe, c], check=True)
         out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
     vals = [int(x) for x in out]
-    assert vals[0] == C.sizeof(ExcfvStatic)
+    assert vals[0] == C.sizeof(cls)
     for f, off in zip(fields, vals[1:]):
-        assert getattr(ExcfvStatic, f).offset == off, f
+        assert getattr(cls, f).offset == off, f
 
 
 def test_status_codes_match_header():
