@@ -694,7 +694,7 @@ int excfv_seceqnsv_dev(excfv_handle* h, int32_t ngp, int32_t ngkmax, const doubl
                         reinterpret_cast<cplx*>(evecsv));
 }
 
-int excfv_rhovalk_sv(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
+static int rhovalk_sv_host(excfv_handle* h, bool nc, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
                      const double* sfacgp, int32_t nmatmax, const double* evecfv, const double* evecsv,
                      const double* wocc, double epsocc) {
   int rc = check_rho(h, ngp, ngkmax, nmatmax);
@@ -711,10 +711,38 @@ int excfv_rhovalk_sv(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double*
   if (cudaMemcpyAsync(dsv, evecsv, sizeof(cplx) * (size_t)4 * n * n, cudaMemcpyHostToDevice, h->stream) !=
       cudaSuccess)
     rc = EXCFV_ERR_CUDA;
-  if (rc == EXCFV_OK) rc = stage_rhovalk_sv(h, ngp, ngkmax, ws.apwalm, ws.Z, nmatmax, dsv, wocc, epsocc);
+  if (rc == EXCFV_OK)
+    rc = nc ? stage_rhovalk_sv_nc(h, ngp, ngkmax, ws.apwalm, ws.Z, nmatmax, dsv, wocc, epsocc)
+            : stage_rhovalk_sv(h, ngp, ngkmax, ws.apwalm, ws.Z, nmatmax, dsv, wocc, epsocc);
   if (cudaStreamSynchronize(h->stream) != cudaSuccess && rc == EXCFV_OK) rc = EXCFV_ERR_CUDA;
   cudaFree(dsv);
   return rc;
+}
+
+int excfv_rhovalk_sv(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
+                     const double* sfacgp, int32_t nmatmax, const double* evecfv, const double* evecsv,
+                     const double* wocc, double epsocc) {
+  return rhovalk_sv_host(h, false, ngp, ngkmax, gpc, tpgpc, sfacgp, nmatmax, evecfv, evecsv, wocc, epsocc);
+}
+
+int excfv_rhovalk_sv_nc(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
+                        const double* sfacgp, int32_t nmatmax, const double* evecfv, const double* evecsv,
+                        const double* wocc, double epsocc) {
+  return rhovalk_sv_host(h, true, ngp, ngkmax, gpc, tpgpc, sfacgp, nmatmax, evecfv, evecsv, wocc, epsocc);
+}
+
+int excfv_get_magmt3(excfv_handle* h, double* magmt, int32_t reset) {
+  if (!h) return EXCFV_ERR_ARG;
+  if (!h->rho.ready) {
+    excfv_set_error("excfv_set_rho must be called first");
+    return EXCFV_ERR_STATE;
+  }
+  DeviceGuard g(h->device);
+  const size_t n = (size_t)3 * h->rho.lmmaxvr * h->rho.nrmtmax * h->st.natmtot;
+  if (magmt) CUDA_TRY(cudaMemcpyAsync(magmt, h->rho.magmt3, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+  if (reset) CUDA_TRY(cudaMemsetAsync(h->rho.magmt3, 0, sizeof(double) * n, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return EXCFV_OK;
 }
 
 int excfv_get_magmt(excfv_handle* h, double* magmt, int32_t reset) {

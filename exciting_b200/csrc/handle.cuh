@@ -126,6 +126,10 @@ struct DevRho {
   cplx* lo1 = nullptr;       // (maxnlo * natmtot, nstfv) LO rows of evecfv
   cplx* lo2 = nullptr;       // (maxnlo * natmtot, 2 nstfv)
   cplx* esv = nullptr;       // (nstfv, 2 nstfv) one spin's rows of evecsv
+  // the non-collinear branch: magmt(:,:,:,1:3) and the down component's coefficients
+  double* magmt3 = nullptr;  // (lmmaxvr, nrmtmax, natmtot, 3)
+  cplx* coef3 = nullptr;     // as coef2
+  cplx* lo3 = nullptr;       // as lo2
 };
 
 // Second-variational state (secvar.cu): the collinear field's muffin-tin
@@ -244,6 +248,8 @@ int stage_rhovalk(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, cons
                   const double* wocc, double epsocc);
 int stage_rhovalk_sv(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, const cplx* evec, long long ldev,
                      const cplx* evecsv, const double* wocc, double epsocc);
+int stage_rhovalk_sv_nc(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, const cplx* evec, long long ldev,
+                        const cplx* evecsv, const double* wocc, double epsocc);
 void free_rho(DevRho& r);
 // second variation, collinear field (secvar.cu)
 int stage_set_bfield(excfv_handle* h, const excfv_bfield* b);

@@ -140,6 +140,103 @@ __global__ void k_rho_mt(RhoArgs a) {
   }
 }
 
+// The wavefunction's lm expansion at coarse point irc of atom ias for state
+// j from coefficients cf (APW, per atom) and lo (LO rows), without cut-off.
+__device__ __forceinline__ cplx wf_lm(const RhoArgs& a, const cplx* cf, const cplx* lo, int ias, int is, int irc,
+                                      int lm, int j) {
+  cplx v = cmk(0.0, 0.0);
+  int l = 0;
+  while ((l + 1) * (l + 1) <= lm) ++l;
+  const int nap = a.apword[l + (a.lmaxapw + 1) * is];
+  for (int io = 0; io < nap; ++io) {
+    const cplx c = cf[(size_t)(io + a.apwordmax * lm) + (size_t)a.apwordmax * a.lmmaxvr * j];
+    const double u = a.ucoarse[irc + (size_t)a.nrcmax * (io + (size_t)a.apwordmax * (l + (size_t)(a.lmaxvr + 1) * ias))];
+    v.x += c.x * u;
+    v.y += c.y * u;
+  }
+  if (a.lo_first[ias] >= 0)
+    for (int q = 0; q < a.maxnlo; ++q) {
+      if (a.lo_lm[q + a.maxnlo * ias] != lm) continue;
+      const int ilo = a.lo_ilo[q + a.maxnlo * ias];
+      const cplx c = lo[(size_t)(q + a.maxnlo * ias) + (size_t)a.ldlo * j];
+      const double f = a.vcoarse[irc + (size_t)a.nrcmax * (ilo + (size_t)a.nlomax * ias)];
+      v.x += c.x * f;
+      v.y += c.y * f;
+    }
+  return v;
+}
+
+// The non-collinear density (rhovalk.f90:151-195, ncmag): both spinor
+// components of each state at each covering point, z1 (a.coef, a.locoef)
+// and z2 (cdn, ldn); sums of w |z1|^2, w |z2|^2, w Re(z1 z2*), w Im(z1 z2*),
+// each taken back to real harmonics: rhomt += r1 + r2, magmt(1) += 2 r3,
+// magmt(2) -= 2 r4, magmt(3) += r1 - r2.
+__global__ void k_rho_mt_nc(RhoArgs a, const cplx* cdn, const cplx* ldn, double* magmt3) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  const int irc = blockIdx.x, ias = blockIdx.y;
+  const int is = a.idxis[ias];
+  const int nr = a.nrmt[is];
+  const int nrc = (nr + a.lradstep - 1) / a.lradstep;
+  if (irc >= nrc) return;
+  const int L = a.lmmaxvr;
+  cplx* zb = reinterpret_cast<cplx*>(dsm);      // L x L
+  cplx* w1 = zb + L * L;                        // L x JB
+  cplx* w2 = w1 + L * JB;                       // L x JB
+  double* rfmt = reinterpret_cast<double*>(w2 + L * JB);  // 4 x L
+  for (int e = threadIdx.x; e < L * L; e += blockDim.x) zb[e] = a.zb[e];
+  double s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;  // thread tp < L
+  const size_t off = (size_t)a.apwordmax * L * a.nst * ias;
+  for (int j0 = 0; j0 < a.nst; j0 += JB) {
+    const int nj = min(JB, a.nst - j0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < L * nj; e += blockDim.x) {
+      const int lm = e % L, jj = e / L, j = j0 + jj;
+      const bool on = a.w[j] != 0.0;
+      w1[lm + L * jj] = on ? wf_lm(a, a.coef + off, a.locoef, ias, is, irc, lm, j) : cmk(0.0, 0.0);
+      w2[lm + L * jj] = on ? wf_lm(a, cdn + off, ldn, ias, is, irc, lm, j) : cmk(0.0, 0.0);
+    }
+    __syncthreads();
+    if (threadIdx.x < L) {
+      const int tp = threadIdx.x;
+      for (int jj = 0; jj < nj; ++jj) {
+        const double wj = a.w[j0 + jj];
+        if (wj == 0.0) continue;
+        cplx z1 = cmk(0.0, 0.0), z2 = cmk(0.0, 0.0);
+        for (int lm = 0; lm < L; ++lm) {
+          const cplx y = zb[tp + L * lm];
+          z1 = cadd(z1, cmul(y, w1[lm + L * jj]));
+          z2 = cadd(z2, cmul(y, w2[lm + L * jj]));
+        }
+        s1 += wj * (z1.x * z1.x + z1.y * z1.y);
+        s2 += wj * (z2.x * z2.x + z2.y * z2.y);
+        s3 += wj * (z1.x * z2.x + z1.y * z2.y);   // Re(z1 conj(z2))
+        s4 += wj * (z1.y * z2.x - z1.x * z2.y);   // Im(z1 conj(z2))
+      }
+    }
+  }
+  if (threadIdx.x < L) {
+    rfmt[threadIdx.x] = s1;
+    rfmt[L + threadIdx.x] = s2;
+    rfmt[2 * L + threadIdx.x] = s3;
+    rfmt[3 * L + threadIdx.x] = s4;
+  }
+  __syncthreads();
+  if (threadIdx.x < L) {
+    const int lm = threadIdx.x;
+    double r[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int tp = 0; tp < L; ++tp) {
+      const double f = a.rf[lm + (size_t)L * tp];
+      for (int k = 0; k < 4; ++k) r[k] += f * rfmt[k * L + tp];
+    }
+    const size_t at = lm + (size_t)L * (irc * a.lradstep + (size_t)a.nrmtmax * ias);
+    const size_t comp = (size_t)L * a.nrmtmax * a.natmtot;
+    a.rhomt[at] += r[0] + r[1];
+    magmt3[at] += 2.0 * r[2];
+    magmt3[at + comp] -= 2.0 * r[3];
+    magmt3[at + 2 * comp] += r[0] - r[1];
+  }
+}
+
 // drop real and imaginary parts below the cut-off (wavefmt_add)
 __global__ void k_rho_cut(long long n, cplx* c) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -192,7 +289,7 @@ int dup(T** d, const T* h, size_t n) {
 void free_rho(DevRho& r) {
   for (void* p : {(void*)r.nrmt, (void*)r.ucoarse, (void*)r.vcoarse, (void*)r.zb, (void*)r.rf, (void*)r.rhomt,
                   (void*)r.coef, (void*)r.w, (void*)r.lo_first, (void*)r.lorbl, (void*)r.magmt, (void*)r.coef2,
-                  (void*)r.lo1, (void*)r.lo2, (void*)r.esv})
+                  (void*)r.lo1, (void*)r.lo2, (void*)r.esv, (void*)r.magmt3, (void*)r.coef3, (void*)r.lo3})
     if (p) cudaFree(p);
   r = DevRho();
 }
@@ -257,7 +354,11 @@ int stage_set_rho(excfv_handle* h, const excfv_rhoset* r) {
       (rc = dup(&d.lo1, (const cplx*)nullptr, (size_t)std::max(st.maxnlo, 1) * st.natmtot * std::max(st.nstfv, 1))) ||
       (rc = dup(&d.lo2, (const cplx*)nullptr,
                 (size_t)2 * std::max(st.maxnlo, 1) * st.natmtot * std::max(st.nstfv, 1))) ||
-      (rc = dup(&d.esv, (const cplx*)nullptr, (size_t)2 * std::max(st.nstfv, 1) * std::max(st.nstfv, 1)))) {
+      (rc = dup(&d.esv, (const cplx*)nullptr, (size_t)2 * std::max(st.nstfv, 1) * std::max(st.nstfv, 1))) ||
+      (rc = dup(&d.magmt3, (const double*)nullptr, 3 * L * r->nrmtmax * st.natmtot)) ||
+      (rc = dup(&d.coef3, (const cplx*)nullptr, 2 * d.ncoef)) ||
+      (rc = dup(&d.lo3, (const cplx*)nullptr,
+                (size_t)2 * std::max(st.maxnlo, 1) * st.natmtot * std::max(st.nstfv, 1)))) {
     free_rho(d);
     return rc;
   }
@@ -311,8 +412,13 @@ int stage_rhovalk(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, cons
 // rhomt and magmt += the k-point's density with second-variational vectors
 // evecsv (2 nstfv x 2 nstfv, device, ld 2 nstfv) for a collinear field; the
 // weights wocc (2 nstfv) on the host
-int stage_rhovalk_sv(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, const cplx* evec, long long ldev,
-                     const cplx* evecsv, const double* wocc, double epsocc) {
+namespace {
+
+// The first-variational coefficients of every state (wavefmt_add's cut-off
+// applied), the LO rows, and the weights (0 below epsocc) for the branches
+// with second-variational vectors; then RhoArgs for the coarse-mesh kernels.
+int sv_prepare(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, const cplx* evec, long long ldev,
+               const double* wocc, double epsocc, RhoArgs& a) {
   DevStatic& st = h->st;
   DevRho& d = h->rho;
   cudaStream_t s = h->stream;
@@ -324,9 +430,9 @@ int stage_rhovalk_sv(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, c
   std::vector<double> w(n2);
   for (int j = 0; j < n2; ++j) w[j] = (fabs(wocc[j]) > epsocc) ? wocc[j] : 0.0;
   CUDA_TRY(cudaMemcpyAsync(d.w, w.data(), sizeof(double) * n2, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaStreamSynchronize(s));  // w is a host temporary
   bind_gemm_ctx(h);
   int rc;
-  // first-variational coefficients, then wavefmt_add's cut-off
   ZgemmArgs z;
   z.m = (int)M; z.n = n; z.k = ngp;
   z.alpha = cmk(1.0, 0.0); z.beta = cmk(0.0, 0.0);
@@ -343,7 +449,6 @@ int stage_rhovalk_sv(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, c
                                                                     d.lo_first, evec, ldev, d.lo1);
   count_launch();
   CUDA_TRY(cudaGetLastError());
-  RhoArgs a;
   a.natmtot = st.natmtot; a.lmaxvr = d.lmaxvr; a.lmmaxvr = L; a.lradstep = d.lradstep; a.nrcmax = d.nrcmax;
   a.nrmtmax = d.nrmtmax; a.apwordmax = st.apwordmax; a.nlomax = std::max(st.nlomax, 1);
   a.maxnlo = nlo1; a.nst = n2; a.ngp = ngp;
@@ -351,31 +456,77 @@ int stage_rhovalk_sv(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, c
   a.lo_lm = st.lo_lm; a.lo_ilo = st.lo_ilo; a.lo_first = d.lo_first; a.lorbl = d.lorbl;
   a.ucoarse = d.ucoarse; a.vcoarse = d.vcoarse; a.zb = d.zb; a.rf = d.rf; a.coef = d.coef2;
   a.evec = evec; a.ldev = ldev; a.locoef = d.lo2; a.ldlo = LM; a.cut = 0;
-  a.w = d.w; a.rhomt = d.rhomt; a.magmt = d.magmt;
-  const size_t smem = sizeof(cplx) * ((size_t)L * L + (size_t)L * JB) + sizeof(double) * L;
+  a.w = d.w; a.rhomt = d.rhomt; a.magmt = d.magmt; a.msign = 1.0;
+  return EXCFV_OK;
+}
+
+// one spinor component's coefficients: cf = coef esv_spin (per atom), lo = lo1 esv_spin
+int sv_spin(excfv_handle* h, int spin, const cplx* evecsv, double epsocc, cplx* cf, cplx* lo) {
+  DevStatic& st = h->st;
+  DevRho& d = h->rho;
+  cudaStream_t s = h->stream;
+  const int n = st.nstfv, n2 = 2 * st.nstfv;
+  const long long M = (long long)st.apwordmax * d.lmmaxvr;
+  const long long LM = (long long)std::max(st.maxnlo, 1) * st.natmtot;
+  k_rho_esv<<<(unsigned)(((long long)n * n2 + 255) / 256), 256, 0, s>>>(n, spin, evecsv, epsocc, d.esv);
+  count_launch();
+  CUDA_TRY(cudaGetLastError());
+  ZgemmArgs g;
+  g.m = (int)M; g.n = n2; g.k = n;
+  g.alpha = cmk(1.0, 0.0); g.beta = cmk(0.0, 0.0);
+  g.A = d.coef; g.lda = M; g.strideA = M * n;
+  g.B = d.esv; g.ldb = n; g.strideB = 0;
+  g.C = cf; g.ldc = M; g.strideC = M * n2;
+  g.batch = st.natmtot; g.uplo_c = TRI_NONE; g.tri_a = TRI_NONE; g.tri_b = TRI_NONE;
+  g.splitk = 1; g.part = nullptr; g.kdec = 0;
+  int rc;
+  if ((rc = zgemm(s, OP_N, OP_N, g))) return rc;
+  g.m = (int)LM; g.A = d.lo1; g.lda = LM; g.strideA = 0;
+  g.C = lo; g.ldc = LM; g.strideC = 0; g.batch = 1;
+  return zgemm(s, OP_N, OP_N, g);
+}
+
+size_t rho_smem(int L, int ncomp) {
+  return sizeof(cplx) * ((size_t)L * L + (size_t)ncomp * L * JB) + sizeof(double) * (ncomp == 1 ? 1 : 4) * L;
+}
+
+}  // namespace
+
+int stage_rhovalk_sv(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, const cplx* evec, long long ldev,
+                     const cplx* evecsv, const double* wocc, double epsocc) {
+  DevRho& d = h->rho;
+  cudaStream_t s = h->stream;
+  RhoArgs a;
+  int rc;
+  if ((rc = sv_prepare(h, ngp, ngkmax, apwalm, evec, ldev, wocc, epsocc, a))) return rc;
+  const size_t smem = rho_smem(d.lmmaxvr, 1);
   if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(k_rho_mt, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int spin = 0; spin < 2; ++spin) {
-    k_rho_esv<<<(unsigned)(((long long)n * n2 + 255) / 256), 256, 0, s>>>(n, spin, evecsv, epsocc, d.esv);
-    count_launch();
-    CUDA_TRY(cudaGetLastError());
-    // the spinor component's coefficients: c (per atom) and the LO rows times esv
-    ZgemmArgs g;
-    g.m = (int)M; g.n = n2; g.k = n;
-    g.alpha = cmk(1.0, 0.0); g.beta = cmk(0.0, 0.0);
-    g.A = d.coef; g.lda = M; g.strideA = M * n;
-    g.B = d.esv; g.ldb = n; g.strideB = 0;
-    g.C = d.coef2; g.ldc = M; g.strideC = M * n2;
-    g.batch = st.natmtot; g.uplo_c = TRI_NONE; g.tri_a = TRI_NONE; g.tri_b = TRI_NONE;
-    g.splitk = 1; g.part = nullptr; g.kdec = 0;
-    if ((rc = zgemm(s, OP_N, OP_N, g))) return rc;
-    g.m = (int)LM; g.A = d.lo1; g.lda = LM; g.strideA = 0;
-    g.C = d.lo2; g.ldc = LM; g.strideC = 0; g.batch = 1;
-    if ((rc = zgemm(s, OP_N, OP_N, g))) return rc;
+    if ((rc = sv_spin(h, spin, evecsv, epsocc, d.coef2, d.lo2))) return rc;
     a.msign = spin == 0 ? 1.0 : -1.0;
-    dim3 grid(d.nrcmax, st.natmtot);
+    dim3 grid(d.nrcmax, h->st.natmtot);
     k_rho_mt<<<grid, 128, smem, s>>>(a);
     count_launch();
     CUDA_TRY(cudaGetLastError());
   }
+  return EXCFV_OK;
+}
+
+int stage_rhovalk_sv_nc(excfv_handle* h, int ngp, int ngkmax, const cplx* apwalm, const cplx* evec, long long ldev,
+                        const cplx* evecsv, const double* wocc, double epsocc) {
+  DevRho& d = h->rho;
+  cudaStream_t s = h->stream;
+  RhoArgs a;
+  int rc;
+  if ((rc = sv_prepare(h, ngp, ngkmax, apwalm, evec, ldev, wocc, epsocc, a))) return rc;
+  if ((rc = sv_spin(h, 0, evecsv, epsocc, d.coef2, d.lo2)) || (rc = sv_spin(h, 1, evecsv, epsocc, d.coef3, d.lo3)))
+    return rc;
+  const size_t smem = rho_smem(d.lmmaxvr, 2);
+  if (smem > 48 * 1024)
+    CUDA_TRY(cudaFuncSetAttribute(k_rho_mt_nc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(d.nrcmax, h->st.natmtot);
+  k_rho_mt_nc<<<grid, 128, smem, s>>>(a, d.coef3, d.lo3, d.magmt3);
+  count_launch();
+  CUDA_TRY(cudaGetLastError());
   return EXCFV_OK;
 }

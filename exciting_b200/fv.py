@@ -302,6 +302,23 @@ class FirstVariational:
         self._check(self._L.excfv_get_magmt(self._h, _ptr(out), int(reset)), "excfv_get_magmt")
         return out
 
+    def rhovalk_sv_nc(self, kp, evecfv: np.ndarray, evecsv: np.ndarray, wocc, epsocc: float = 1e-8) -> None:
+        """Adds the k-point's density for a non-collinear field (full spinor
+        second-variational vectors) to the handle's rhomt and magmt3."""
+        ev = _f(evecfv, np.complex128)
+        sv = _f(evecsv, np.complex128)
+        w = _f(wocc, np.float64)
+        rc = self._L.excfv_rhovalk_sv_nc(self._h, kp.ngp, kp.ngkmax, _ptr(kp.gpc), _ptr(kp.tpgpc),
+                                         _ptr(kp.sfacgp), int(ev.shape[0]), _ptr(ev), _ptr(sv), _ptr(w),
+                                         float(epsocc))
+        self._check(rc, "excfv_rhovalk_sv_nc")
+
+    def magmt3(self, reset: bool = False) -> np.ndarray:
+        """The non-collinear magnetisation (lmmaxvr, nrmtmax, natmtot, 3)."""
+        out = np.zeros(self._rho_shape + (3,), order="F")
+        self._check(self._L.excfv_get_magmt3(self._h, _ptr(out), int(reset)), "excfv_get_magmt3")
+        return out
+
     def rhomt(self, reset: bool = False) -> np.ndarray:
         out = np.zeros(self._rho_shape, order="F")
         self._check(self._L.excfv_get_rhomt(self._h, _ptr(out), int(reset)), "excfv_get_rhomt")

@@ -103,6 +103,9 @@ SIGNATURES = {
     "excfv_get_magmt": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
     "excfv_rhovalk_sv": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]),
+    "excfv_rhovalk_sv_nc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]),
+    "excfv_get_magmt3": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
     "excfv_set_bfield": (C.c_int, [C.c_void_p, C.POINTER(ExcfvBfield)]),
     "excfv_set_bfield_nc": (C.c_int, [C.c_void_p, C.POINTER(ExcfvBfieldNc)]),
     "excfv_seceqnsv": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -258,11 +258,22 @@ int excfv_rhovalk_dev(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double
 int excfv_rhovalk_sv(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
                      const double* sfacgp, int32_t nmatmax, const double* evecfv, const double* evecsv,
                      const double* wocc, double epsocc);
+/* The same for a non-collinear field (src/rhovalk.f90:151-195, ncmag): per
+ * covering point, with z1, z2 the spinor components of state j, rhomt +=
+ * w (|z1|^2 + |z2|^2) and the handle's magmt3(:,:,:,1:3) += w (2 Re(z1 z2*),
+ * -2 Im(z1 z2*), |z1|^2 - |z2|^2), each taken back to real harmonics;
+ * evecsv the full (2 nstfv, 2 nstfv) of excfv_seceqnsv after
+ * excfv_set_bfield_nc.  Host arrays, synchronous. */
+int excfv_rhovalk_sv_nc(excfv_handle* h, int32_t ngp, int32_t ngkmax, const double* gpc, const double* tpgpc,
+                        const double* sfacgp, int32_t nmatmax, const double* evecfv, const double* evecsv,
+                        const double* wocc, double epsocc);
 /* Copies rhomt (lmmaxvr, nrmtmax, natmtot) to the host (rhomt may be NULL)
  * and, when reset != 0, zeroes the accumulator. */
 int excfv_get_rhomt(excfv_handle* h, double* rhomt, int32_t reset);
 /* The same for the collinear magnetisation magmt (lmmaxvr, nrmtmax, natmtot). */
 int excfv_get_magmt(excfv_handle* h, double* magmt, int32_t reset);
+/* The same for the non-collinear magnetisation magmt3 (lmmaxvr, nrmtmax, natmtot, 3). */
+int excfv_get_magmt3(excfv_handle* h, double* magmt, int32_t reset);
 
 /* ---- the muffin-tin Hamiltonian build (once per SCF iteration) ---------- */
 

@@ -21,6 +21,9 @@ collinear spin-polarised one with them (``rhovalk_sv``):
                       with |wkpt occsv| > epsocc, the backward SHT of wfmt,
                       |.|^2 summed with that weight, then per coarse radial
                       point the forward real SHT into rhomt_k(lm, ir, ias)
+``rhovalk_sv_nc``     the non-collinear branch (ncmag): the up-down product
+                      of the spinor components gives the x and y
+                      magnetisation
 ====================  ========================================================
 """
 from __future__ import annotations
@@ -172,4 +175,52 @@ def rhovalk_sv(st, rad, lradstep: int, lmaxvr: int, ngp: int, apwalm: np.ndarray
         dn = rfsht @ rfmt[1]
         rho[:, irs, ias] += up + dn
         mag[:, irs, ias] += up - dn
+    return rho, mag
+
+
+def rhovalk_sv_nc(st, rad, lradstep: int, lmaxvr: int, ngp: int, apwalm: np.ndarray, evecfv: np.ndarray,
+                  evecsv: np.ndarray, wocc: np.ndarray, epsocc: float, zbsht: np.ndarray, rfsht: np.ndarray):
+    """rhovalk's branch with second-variational vectors for a non-collinear
+    field (``src/rhovalk.f90:74-195``: nspinor = 2, ncmag true, no spin
+    spiral): (rhomt_k (lmmaxvr, nrmtmax, natmtot), magmt_k (lmmaxvr, nrmtmax,
+    natmtot, 3)).  The spinor components are formed as in rhovalk_sv; per
+    point, with z1, z2 the up and down components and t1 the weight,
+    rfmt(1) += t1 |z1|^2, rfmt(2) += t1 |z2|^2, rfmt(3) += t1 Re(z1 conj(z2)),
+    rfmt(4) += t1 Im(z1 conj(z2)); per coarse radial point magmt(1) +=
+    2 rflm(3), magmt(2) -= 2 rflm(4), magmt(3) += rflm(1) - rflm(2), rhomt +=
+    rflm(1) + rflm(2)."""
+    n = st.nstfv
+    lmmaxvr = (lmaxvr + 1) ** 2
+    nrmtmax = rad.spr.shape[0]
+    rho = np.zeros((lmmaxvr, nrmtmax, st.natmtot), order="F")
+    mag = np.zeros((lmmaxvr, nrmtmax, st.natmtot, 3), order="F")
+    for ias in range(st.natmtot):
+        is_ = int(st.idxis[ias])
+        nr = int(rad.nrmt[is_])
+        irs = np.arange(0, nr, lradstep)
+        rfmt = np.zeros((4, lmmaxvr, irs.shape[0]))
+        done = {}
+        for j in range(2 * n):
+            t1 = wocc[j]
+            if abs(t1) <= epsocc:
+                continue
+            wf3 = np.zeros((2, lmmaxvr, irs.shape[0]), dtype=np.complex128)
+            for ispn in range(2):
+                for ist in range(n):
+                    zt1 = evecsv[ispn * n + ist, j]
+                    if abs(zt1.real) + abs(zt1.imag) > epsocc:
+                        if ist not in done:
+                            done[ist] = zbsht @ wavefmt(st, rad, lradstep, lmaxvr, ias, ngp, apwalm,
+                                                        evecfv[:, ist])
+                        wf3[ispn] += zt1 * done[ist]
+            z3 = wf3[0] * np.conj(wf3[1])
+            rfmt[0] += t1 * (wf3[0].real ** 2 + wf3[0].imag ** 2)
+            rfmt[1] += t1 * (wf3[1].real ** 2 + wf3[1].imag ** 2)
+            rfmt[2] += t1 * z3.real
+            rfmt[3] += t1 * z3.imag
+        fl = [rfsht @ rfmt[i] for i in range(4)]
+        mag[:, irs, ias, 0] += 2.0 * fl[2]
+        mag[:, irs, ias, 1] -= 2.0 * fl[3]
+        mag[:, irs, ias, 2] += fl[0] - fl[1]
+        rho[:, irs, ias] += fl[0] + fl[1]
     return rho, mag

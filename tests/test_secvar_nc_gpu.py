@@ -7,7 +7,10 @@ so_add, seceqnsv_nc):
 - the eigenvectors by their residuals in the oracle's matrix (<= 1e-12
   relative to its largest entry) and their orthonormality (<= 1e-12);
 - a field along x through the non-collinear route gives the collinear
-  route's eigenvalues for the same field along z (1e-10 Ha).
+  route's eigenvalues for the same field along z (1e-10 Ha);
+- the non-collinear density (excfv_rhovalk_sv_nc) from the device's own
+  spinor vectors: rhomt and magmt3 against the oracle's rhovalk_sv_nc to
+  1e-12 of the largest density entry.
 """
 import numpy as np
 import pytest
@@ -83,3 +86,40 @@ def test_field_along_x_matches_collinear_z():
         fv.set_bfield_nc(rad, bx, bc, ng, bi, c, np.array([birconst[2], 0.0, 0.0]))
         w_nc, _ = fv.seceqnsv(kp, w, X)
     assert np.abs(np.sort(w_col) - w_nc).max() < 1e-10
+
+
+@pytest.mark.parametrize("name,kw,lmaxvr,lradstep", [("diamond2", dict(ngk=60, nstfv=6), 4, 2),
+                                                     ("cubic8", dict(ngk=300, nstfv=20), 6, 3)])
+def test_noncollinear_density_matches_oracle(name, kw, lmaxvr, lradstep):
+    """The device chain seceqnsv (non-collinear, spin-orbit) -> rhovalk_sv_nc:
+    rhomt and magmt3 against the oracle's rhovalk_sv_nc on the device's own
+    second-variational vectors (1e-12 of the largest density entry)."""
+    from oracle import rhoval
+    p = syn.make_problem(name, **kw)
+    st, kp = p.static, p.kpts[0]
+    rad = syn.make_radial(st, nrmt=140, lmaxvr=lmaxvr)
+    ng, _, c = syn.make_interstitial_real(st)
+    bxc, bconst, bxcir, birconst = _fields(st, rad, lmaxvr, c.shape[0])
+    n = st.nstfv
+    apwalm = fvref.match(st, kp)
+    w, X, info = fvref.seceqn(st, kp)
+    assert info == 0
+    zb, _, _, rf = rhoval.sht_matrices(lmaxvr)
+    wocc = np.zeros(2 * n)
+    wocc[:n] = 1.0
+    wocc[n] = 1e-12                        # below epsocc: skipped
+    epsocc = 1e-8
+    with FirstVariational(0) as fv:
+        fv.set_static(st)
+        fv.set_bfield_nc(rad, bxc, bconst, ng, bxcir, c, birconst, spinorb=True)
+        ws, vs = fv.seceqnsv(kp, w, X)
+        fv.set_rho(rad, lmaxvr, lradstep, zb, rf)
+        fv.rhovalk_sv_nc(kp, X, vs, wocc, epsocc)
+        rho = fv.rhomt(reset=True)
+        mag = fv.magmt3(reset=True)
+    rho_ref, mag_ref = rhoval.rhovalk_sv_nc(st, rad, lradstep, lmaxvr, kp.ngp, apwalm, X, vs, wocc, epsocc, zb, rf)
+    scale = np.abs(rho_ref).max()
+    assert np.abs(rho - rho_ref).max() < 1e-12 * scale
+    assert np.abs(mag - mag_ref).max() < 1e-12 * scale
+    for d in range(3):                    # every component is polarised by the field
+        assert np.abs(mag_ref[..., d]).max() > 1e-6 * scale
