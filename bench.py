@@ -237,7 +237,17 @@ def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn, prec)
         tot = timed(args.batch_steps)
         info = fvb.batch_info(nk)
         fvb.set_batch_graph(False)
+        l0 = fvb.launch_count()
         tot_eager = timed(1)
+        launches_batch = fvb.launch_count() - l0
+        mode = fvb.batch_mode()
+        # launches of the other form on the same batch (one eager, untimed run)
+        fvb.set_batch_mode(0 if mode == 1 else 1)
+        l0 = fvb.launch_count()
+        fvb.seceqn_batched_dev(*bargs)
+        torch.cuda.synchronize()
+        launches_other = fvb.launch_count() - l0
+        fvb.set_batch_mode(mode)
         fvb.profile(True)                   # stage breakdown: one more (eager) batch
         fvb.seceqn_batched_dev(*bargs)
         torch.cuda.synchronize()
@@ -294,6 +304,10 @@ def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn, prec)
             "ms_per_batch": tot / args.batch_steps, "ms_per_batch_eager": tot_eager,
             "execution": "one CUDA graph per batch (captured on the second identical call)",
             "lanes": lanes,
+            "form": "grouped front (Cholesky, inverse factor, two-sided reduction of all k-points "
+                    "as grouped launches), lanes for the rest" if mode == 1 else "lanes (whole chains)",
+            "launches_per_batch": int(launches_batch),
+            "launches_per_batch_other_form": int(launches_other),
             "lane_stage_ms_per_k": {kk: round(v[0] / nk, 3) for kk, v in bprof.items()},
             "all_info_zero": bool(np.all(info == 0)),
             **({"plain_fp64_same_k_points": plain} if plain else {})}, evals

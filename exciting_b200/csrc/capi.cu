@@ -432,6 +432,7 @@ int excfv_destroy(excfv_handle* h) {
   }
   h->lanes.clear();
   drop_graph(h);
+  free_group(h->gplan);
   free_rho(h->rho);
   free_sv(h->sv);
   if (h->kinfo) cudaFree(h->kinfo);
@@ -1284,13 +1285,143 @@ static int run_batch(excfv_handle* h, const BatchArgs& b, int L) {
   }
   h->batch_nmat.assign(b.nmatp, b.nmatp + b.nk);
   h->last_nk = b.nk;
+  h->batch_form = h->batch_mode;
+  if (h->batch_mode == EXCFV_BATCH_AUTO) {
+    size_t fr = 0, tot = 0;
+    CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+    const double need = 4.0 * sizeof(cplx) * (double)nmax * nmax * b.nk;
+    const bool have = group_slots_hold(h, b.nk, nmax);
+    h->batch_form = (have || need <= 0.25 * (double)fr) ? EXCFV_BATCH_GROUPED : EXCFV_BATCH_LANES;
+  }
+  if (h->batch_form == EXCFV_BATCH_GROUPED && (rc = group_plan_front(h, b.nk, b.nmatp, nmax))) return rc;
   if (!b.host && h->graph_on && !h->prof.on) return run_batch_graph(h, b, L);
   return enqueue_batch(h, b, L);
+}
+
+// Longest-processing-time-first: k-points by decreasing nmatp^3 (the
+// eigensolver's cost), each to the lane with the least work so far, so the
+// lanes finish together although the basis sizes differ.
+static void deal_lanes(const BatchArgs& b, int L, std::vector<int>& order, std::vector<int>& lane_of) {
+  order.resize(b.nk);
+  lane_of.resize(b.nk);
+  for (int k = 0; k < b.nk; ++k) order[k] = k;
+  auto cost = [&](int k) { const double x = b.nmatp[k]; return x * x * x; };
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
+  std::vector<double> load(L, 0.0);
+  for (int k : order) {
+    const int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    lane_of[k] = l;
+    load[l] += cost(k);
+  }
+}
+
+static int fork_lanes(excfv_handle* h, int L) {
+  cudaEvent_t fork;
+  CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  CUDA_TRY(cudaEventRecord(fork, h->stream));
+  for (int i = 0; i < L; ++i) CUDA_TRY(cudaStreamWaitEvent(h->lanes[i]->stream, fork, 0));
+  cudaEventDestroy(fork);
+  return EXCFV_OK;
+}
+
+static int join_lanes(excfv_handle* h, int L) {
+  for (int i = 0; i < L; ++i) {
+    cudaEvent_t join;
+    CUDA_TRY(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventRecord(join, h->lanes[i]->stream));
+    CUDA_TRY(cudaStreamWaitEvent(h->stream, join, 0));
+    cudaEventDestroy(join);
+  }
+  return EXCFV_OK;
+}
+
+// The lane's matrices pointed at k-point k's slots of the grouped batch for
+// the scope of one k-point's enqueue (launches take the pointers by value).
+struct SlotScope {
+  Workspace& ws;
+  cplx *H, *O, *Ui, *T;
+  SlotScope(excfv_handle* h, excfv_handle* c, int k) : ws(c->ws), H(ws.H), O(ws.O), Ui(ws.Ui), T(ws.T) {
+    ws.H = group_slot(h, 0, k);
+    ws.O = group_slot(h, 1, k);
+    ws.Ui = group_slot(h, 2, k);
+    ws.T = group_slot(h, 3, k);
+  }
+  ~SlotScope() { ws.H = H; ws.O = O; ws.Ui = Ui; ws.T = T; }
+};
+
+// The grouped batch: per lane match + setup into the k-points' slots; the
+// grouped front (Cholesky, inverse factor, two-sided reduction) of all
+// k-points on h->stream; per lane the rest of each k-point's solve.
+static int enqueue_grouped(excfv_handle* h, const BatchArgs& b, int L) {
+  int rc = EXCFV_OK;
+  const cudaMemcpyKind in = b.host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  const cudaMemcpyKind out = b.host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  const int k_st = h->st.nstfv;
+  std::vector<int> order, lane_of;
+  deal_lanes(b, L, order, lane_of);
+  if ((rc = fork_lanes(h, L))) return rc;
+  for (int idx = 0; idx < b.nk && rc == EXCFV_OK; ++idx) {
+    const int k = order[idx];
+    excfv_handle* c = h->lanes[lane_of[k]];
+    Workspace& ws = c->ws;
+    cudaStream_t s = c->stream;
+    const int ngp = b.ngp[k], n = b.nmatp[k];
+    CUDA_TRY(cudaMemcpyAsync(ws.gpc, b.gpc[k], sizeof(double) * ngp, in, s));
+    CUDA_TRY(cudaMemcpyAsync(ws.tpgpc, b.tpgpc[k], sizeof(double) * 2 * ngp, in, s));
+    CUDA_TRY(cudaMemcpyAsync(ws.sfacgp, b.sfacgp[k], sizeof(cplx) * (size_t)b.ngkmax * h->st.natmtot,
+                             in, s));
+    CUDA_TRY(cudaMemcpyAsync(ws.igpig, b.igpig[k], sizeof(int) * ngp, in, s));
+    CUDA_TRY(cudaMemcpyAsync(ws.vgpc, b.vgpc[k], sizeof(double) * 3 * ngp, in, s));
+    if ((rc = stage_match(c, ngp, b.ngkmax, nullptr))) break;
+    {
+      SlotScope sc(h, c, k);
+      if ((rc = stage_setup(c, n, ngp, false))) break;
+    }
+    CUDA_TRY(cudaMemcpyAsync(h->kinfo + (size_t)k * ST_NWORDS, ws.status, sizeof(int) * ST_NWORDS,
+                             cudaMemcpyDeviceToDevice, s));
+  }
+  if (rc) return rc;
+  if ((rc = join_lanes(h, L))) return rc;
+  if ((rc = group_enqueue_front(h))) return rc;
+  if ((rc = fork_lanes(h, L))) return rc;
+  for (int idx = 0; idx < b.nk && rc == EXCFV_OK; ++idx) {
+    const int k = order[idx];
+    excfv_handle* c = h->lanes[lane_of[k]];
+    Workspace& ws = c->ws;
+    cudaStream_t s = c->stream;
+    const int n = b.nmatp[k];
+    CUDA_TRY(cudaMemcpyAsync(ws.status, h->kinfo + (size_t)k * ST_NWORDS, sizeof(int) * ST_NWORDS,
+                             cudaMemcpyDeviceToDevice, s));
+    {
+      SlotScope sc(h, c, k);
+      if (b.host) {
+        cplx* ov = ws.apwalm;
+        const size_t na = (size_t)b.ngkmax * h->st.apwordmax * h->st.lmmaxapw * h->st.natmtot;
+        if ((size_t)n * k_st > na) {
+          excfv_set_error("batched host path: nmatp*nstfv exceeds the lane staging buffer");
+          rc = EXCFV_ERR_UNSUPPORTED;
+          break;
+        }
+        if ((rc = stage_solve_back(c, n, k_st, h->st.evaltol, ws.w, ov, n))) break;
+        CUDA_TRY(cudaMemcpy2DAsync(b.evecfv[k], sizeof(cplx) * b.nmatmax, ov, sizeof(cplx) * n,
+                                   sizeof(cplx) * n, k_st, out, s));
+        CUDA_TRY(cudaMemcpyAsync(b.evalfv[k], ws.w, sizeof(double) * k_st, out, s));
+      } else {
+        if ((rc = stage_solve_back(c, n, k_st, h->st.evaltol, b.evalfv[k], (cplx*)b.evecfv[k], b.nmatmax)))
+          break;
+      }
+    }
+    CUDA_TRY(cudaMemcpyAsync(h->kinfo + (size_t)k * ST_NWORDS, ws.status, sizeof(int) * ST_NWORDS,
+                             cudaMemcpyDeviceToDevice, s));
+  }
+  if (rc) return rc;
+  return join_lanes(h, L);
 }
 
 // Stream work of one batch (no allocation, no host synchronisation), so that
 // it can also be captured into a CUDA graph.
 static int enqueue_batch(excfv_handle* h, const BatchArgs& b, int L) {
+  if (h->batch_form == EXCFV_BATCH_GROUPED) return enqueue_grouped(h, b, L);
   int rc = EXCFV_OK;
   cudaEvent_t fork;
   CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
@@ -1381,9 +1512,21 @@ int excfv_set_lanes(excfv_handle* h, int32_t nlanes) {
 
 int excfv_get_lanes(excfv_handle* h) { return h ? h->nlanes_pref : EXCFV_ERR_ARG; }
 
+int excfv_set_batch_mode(excfv_handle* h, int32_t mode) {
+  if (!h || (mode != EXCFV_BATCH_LANES && mode != EXCFV_BATCH_GROUPED && mode != EXCFV_BATCH_AUTO))
+    return EXCFV_ERR_ARG;
+  h->batch_mode = mode;
+  return EXCFV_OK;
+}
+
+int excfv_get_batch_mode(excfv_handle* h) { return h ? h->batch_mode : EXCFV_ERR_ARG; }
+
+long long excfv_group_launches(excfv_handle* h) { return h ? group_front_launches(h) : 0; }
+
 static std::vector<unsigned long long> batch_key(const excfv_handle* h, const BatchArgs& b, int L) {
   std::vector<unsigned long long> k = {(unsigned long long)b.nk, (unsigned long long)L,
                                        (unsigned long long)h->prec, h->static_gen,
+                                       (unsigned long long)h->batch_form,
                                        (unsigned long long)b.nmatmax, (unsigned long long)b.ngkmax,
                                        (unsigned long long)(uintptr_t)h->stream};
   for (int i = 0; i < b.nk; ++i) {
@@ -1504,8 +1647,9 @@ int excfv_batch_info(excfv_handle* h, int32_t nk, int32_t* info) {
   return batch_info(h, nk, info);
 }
 
-// Times the batch with 1, 2, 4, 6, 8, 12, ... lanes (those the SM budget allows) and
-// keeps the fastest for later batched calls.  Device pointers; the outputs of
+// Times the batch in both forms (lanes; grouped front) with 1, 2, 4, 6, 8,
+// 12, ... lanes (those the SM budget allows) and keeps the fastest form and
+// lane count for later batched calls.  Device pointers; the outputs of
 // the last timed run are valid.  best_ms (optional) receives the winning time.
 int excfv_autotune_lanes(excfv_handle* h, int32_t nk, const int32_t* nmatp, const int32_t* ngp,
                          int32_t ngkmax, const double* const* gpc, const double* const* tpgpc,
@@ -1524,25 +1668,30 @@ int excfv_autotune_lanes(excfv_handle* h, int32_t nk, const int32_t* nmatp, cons
   CUDA_TRY(cudaEventCreate(&e0));
   CUDA_TRY(cudaEventCreate(&e1));
   float best = 1e30f;
-  int bestL = 1;
+  int bestL = 1, bestMode = EXCFV_BATCH_LANES;
   const int cand[] = {1, 2, 4, 6, 8, 12, 16, 24, 32};
-  for (int L : cand) {
-    if (L > lmax) break;
-    for (int rep = 0; rep < 2; ++rep) {  // the first run of a lane count sizes its workspaces
-      CUDA_TRY(cudaEventRecord(e0, h->stream));
-      if ((rc = run_batch(h, b, L))) break;
-      CUDA_TRY(cudaEventRecord(e1, h->stream));
-      CUDA_TRY(cudaEventSynchronize(e1));
+  for (int mode : {EXCFV_BATCH_LANES, EXCFV_BATCH_GROUPED}) {
+    h->batch_mode = mode;
+    for (int L : cand) {
+      if (L > lmax) break;
+      for (int rep = 0; rep < 2; ++rep) {  // the first run of a lane count sizes its workspaces
+        CUDA_TRY(cudaEventRecord(e0, h->stream));
+        if ((rc = run_batch(h, b, L))) break;
+        CUDA_TRY(cudaEventRecord(e1, h->stream));
+        CUDA_TRY(cudaEventSynchronize(e1));
+      }
+      if (rc) break;
+      float ms = 0.f;
+      CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best) { best = ms; bestL = L; bestMode = mode; }
     }
     if (rc) break;
-    float ms = 0.f;
-    CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-    if (ms < best) { best = ms; bestL = L; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
   h->nlanes_pref = bestL;
+  h->batch_mode = bestMode;
   if (best_ms) *best_ms = best;
   rc = run_batch(h, b, bestL);
   if (rc) return rc;

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <vector>
 
 typedef double2 cplx;
 
@@ -103,6 +104,20 @@ void gemm_ctx_set(const GemmCtx& c);
 const GemmCtx& gemm_ctx();
 
 int zgemm(cudaStream_t s, int opA, int opB, const ZgemmArgs& a);
+
+// Grouped products: many unbatched products of different sizes in one
+// launch, one CTA per 64 x 64 output tile.  The host appends each product and
+// its tiles to shared lists (zgemm_group_add; tile entries carry the global
+// product index), orders one launch's tiles heaviest first
+// (zgemm_group_order), uploads both lists and launches zgemm_grouped with the
+// device copies, the tiles as int4 {product, row tile, column tile, 0}.
+struct GroupTile {
+  int prob, ti, tj;
+  long long klen;  // K range of the tile: the ordering key, not uploaded
+};
+void zgemm_group_add(const ZgemmArgs& p, std::vector<ZgemmArgs>& probs, std::vector<GroupTile>& tiles);
+void zgemm_group_order(std::vector<GroupTile>& tiles, size_t from);
+int zgemm_grouped(cudaStream_t s, int opA, int opB, const ZgemmArgs* d_probs, const int4* d_tiles, int ntiles);
 
 // convenience: single (non-batched) product
 int zgemm1(cudaStream_t s, int opA, int opB, int m, int n, int k, cplx alpha,

@@ -175,11 +175,16 @@ struct Prof {
   long long cnt[PROF_NCLS] = {};
 };
 
+struct GroupPlan;  // the grouped front of the batching form (group.cu)
+
 struct excfv_handle {
   int device = 0;
   int grid_ctas = 0;          // CTAs of the cooperative panel kernel (0 = all SMs)
   bool owns_static = true;    // lanes share the parent's static data
   int nlanes_pref = 0;        // lanes of the batched path (0 = autotune)
+  int batch_mode = EXCFV_BATCH_AUTO;   // whole chains on lanes, the grouped front, or auto
+  int batch_form = EXCFV_BATCH_LANES;  // the form the current batch runs in
+  GroupPlan* gplan = nullptr;
   std::vector<excfv_handle*> lanes;
   int* kinfo = nullptr;       // per-k status words of the last batch (device)
   int kinfo_cap = 0;
@@ -235,6 +240,20 @@ void prof_begin(excfv_handle* h, int cls);
 void prof_end(excfv_handle* h, int cls);
 void prof_collect(excfv_handle* h);
 
+// One problem of the grouped Cholesky: its order, overlap (factored in
+// place), inverse factor and status words (potrf.cu).
+struct PotrfProb {
+  int n;
+  long long ld;
+  cplx* O;
+  cplx* Ui;
+  int* status;
+};
+int potrf_smem_bytes();
+int potrf_block();
+// diagonal block kb of every listed problem (each with n > kb), one CTA each
+int potrf_diag_grouped(cudaStream_t s, const PotrfProb* d_probs, int nprob, int kb);
+
 // ---- stages (each enqueues work on h->stream) ------------------------------
 int stage_reserve(excfv_handle* h, int nmatmax, int ngkmax, int kmax);
 int stage_set_static(excfv_handle* h, const excfv_static* s);
@@ -280,6 +299,33 @@ int stage_setup(excfv_handle* h, int nmatp, int ngp, bool mirror_o);
 // generalized eigensolve on ws.H (full) / ws.O (upper) -> evalfv, evecfv
 int stage_solve(excfv_handle* h, int n, int nstfv, double evaltol, double* d_eval,
                 cplx* d_evec, long long ldevec);
+// the solve from C = U^-H H U^-1 onwards (ws.H = C with both triangles,
+// ws.Ui = U^-1 and, in the precision form, C's complex64 copy in ws.T with
+// leading dimension n rounded up to even): what remains of stage_solve
+// after its front, which the grouped batch runs for all k-points together
+int stage_solve_back(excfv_handle* h, int n, int k, double evaltol, double* d_eval, cplx* d_evec,
+                     long long ldevec);
+// whether the front of an order-n solve also writes C's complex64 copy
+int solve_front_f32copy(excfv_handle* h, int n);
+// One problem of the grouped mirror: M's lower triangle <- conj(upper) and,
+// when F is set, a complex64 copy of the whole Hermitian M into F (setup.cu).
+struct MirrorProb {
+  int n;
+  long long ld;
+  cplx* M;
+  float2* F;
+  long long ldf;
+};
+int mirror_grouped(cudaStream_t s, const MirrorProb* d_probs, int nprob, int nmax);
+// the grouped front of a batch (group.cu): plan (before any capture), enqueue,
+// the k-point slots of H, O, U^-1 and T (which = 0..3), launches per front
+int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax);
+int group_enqueue_front(excfv_handle* h);
+cplx* group_slot(excfv_handle* h, int which, int k);
+long long group_front_launches(const excfv_handle* h);
+// whether the slots already allocated hold a batch of nk k-points of order <= nmax
+bool group_slots_hold(const excfv_handle* h, int nk, int nmax);
+void free_group(GroupPlan*& g);
 // per-k status -> LAPACK-style info
 // states carried by the precision form (k plus a Rayleigh-Ritz buffer)
 int mixed_states(int n, int k);

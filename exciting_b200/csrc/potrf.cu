@@ -66,8 +66,7 @@ __device__ __forceinline__ void inv32(const cplx* A, cplx* X, const double* rinv
   }
 }
 
-__global__ void __launch_bounds__(1024) k_potrf_diag(int n, int kb, cplx* O, long long ld, cplx* Ui,
-                                                     int* status) {
+__device__ __forceinline__ void potrf_diag_block(int n, int kb, cplx* O, long long ld, cplx* Ui, int* status) {
   extern __shared__ __align__(16) unsigned char dsm[];
   cplx* A = reinterpret_cast<cplx*>(dsm);   // 64 x LDB, row-major [r][c]
   cplx* X = A + NBP * LDB;
@@ -130,7 +129,30 @@ __global__ void __launch_bounds__(1024) k_potrf_diag(int n, int kb, cplx* O, lon
   }
 }
 
+__global__ void __launch_bounds__(1024) k_potrf_diag(int n, int kb, cplx* O, long long ld, cplx* Ui,
+                                                     int* status) {
+  potrf_diag_block(n, kb, O, ld, Ui, status);
+}
+
+// Grouped form: CTA b factors diagonal block kb of problem b.
+__global__ void __launch_bounds__(1024) k_potrf_diag_grouped(const PotrfProb* __restrict__ probs, int kb) {
+  const PotrfProb p = probs[blockIdx.x];
+  potrf_diag_block(p.n, kb, p.O, p.ld, p.Ui, p.status);
+}
+
 }  // namespace
+
+int potrf_smem_bytes() { return (int)(2 * sizeof(cplx) * NBP * LDB); }
+int potrf_block() { return NBP; }
+
+int potrf_diag_grouped(cudaStream_t s, const PotrfProb* d_probs, int nprob, int kb) {
+  if (nprob <= 0) return EXCFV_OK;
+  const int smem = potrf_smem_bytes();
+  CUDA_TRY(cudaFuncSetAttribute(k_potrf_diag_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_potrf_diag_grouped<<<nprob, 1024, smem, s>>>(d_probs, kb); count_launch();
+  CUDA_TRY(cudaGetLastError());
+  return EXCFV_OK;
+}
 
 int potrf_upper(excfv_handle* h, int n, cplx* O, cplx* Ui, long long ld) {
   cudaStream_t s = h->stream;

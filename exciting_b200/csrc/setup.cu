@@ -187,6 +187,42 @@ int mirror_upper(cudaStream_t s, int n, cplx* M, long long ld) {
   return EXCFV_OK;
 }
 
+// Grouped form of k_mirror_upper over problems of different order
+// (blockIdx.z), optionally writing the complex64 copy of the full matrix.
+__global__ void k_mirror_grouped(const MirrorProb* __restrict__ probs) {
+  __shared__ cplx tile[32][33];
+  const MirrorProb p = probs[blockIdx.z];
+  const int bi = blockIdx.x, bj = blockIdx.y;
+  const int n = p.n;
+  if (bi < bj || bi * 32 >= n) return;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int y = ty; y < 32; y += blockDim.y) {
+    const int r = bj * 32 + tx, c = bi * 32 + y;  // upper tile (bj, bi)
+    if (r < n && c < n) {
+      const cplx v = p.M[r + p.ld * c];
+      tile[y][tx] = v;
+      if (p.F && r <= c) p.F[r + p.ldf * c] = make_float2((float)v.x, (float)v.y);
+    }
+  }
+  __syncthreads();
+  for (int y = ty; y < 32; y += blockDim.y) {
+    const int r = bi * 32 + tx, c = bj * 32 + y;
+    if (r < n && c < n && r > c) {
+      const cplx v = tile[tx][y];
+      p.M[r + p.ld * c] = cmk(v.x, -v.y);
+      if (p.F) p.F[r + p.ldf * c] = make_float2((float)v.x, (float)-v.y);
+    }
+  }
+}
+
+int mirror_grouped(cudaStream_t s, const MirrorProb* d_probs, int nprob, int nmax) {
+  if (nprob <= 0) return EXCFV_OK;
+  dim3 grid((nmax + 31) / 32, (nmax + 31) / 32, nprob);
+  k_mirror_grouped<<<grid, dim3(32, 8), 0, s>>>(d_probs); count_launch();
+  CUDA_TRY(cudaGetLastError());
+  return EXCFV_OK;
+}
+
 int stage_setup(excfv_handle* h, int nmatp, int ngp, bool mirror_o) {
   DevStatic& st = h->st;
   Workspace& ws = h->ws;

@@ -486,20 +486,18 @@ int mixed_states(int n, int k) { return std::min(n, k + std::max(16, k / 8)); }
 static int stage_solve_mixed(excfv_handle* h, int n, int k, double evaltol, double* d_eval,
                              cplx* d_evec, long long ldevec);
 
-int stage_solve(excfv_handle* h, int n, int k, double evaltol, double* d_eval, cplx* d_evec,
-                long long ldevec) {
-  if (h->prec == EXCFV_PREC_MIXED && n > 64)
-    return stage_solve_mixed(h, n, k, evaltol, d_eval, d_evec, ldevec);
+// The front of the solve: O = U^H U, Ui = U^-1, C = Ui^H H Ui in ws.H (both
+// triangles) and, in the precision form, C's complex64 copy in ws.T (leading
+// dimension n rounded up to even).  The grouped batch runs this step for all
+// of its k-points together and then only stage_solve_back per k-point.
+static int solve_front(excfv_handle* h, int n, bool f32copy) {
   Workspace& ws = h->ws;
   cudaStream_t s = h->stream;
   const long long ld = n;
   const cplx one = cmk(1.0, 0.0), zero = cmk(0.0, 0.0);
   int rc;
-  if (k < 1 || k > n) return EXCFV_ERR_ARG;
   bind_gemm_ctx(h);
-  if (k > ws.kmax) return EXCFV_ERR_ARG;
   CUDA_TRY(cudaMemsetAsync(ws.status, 0, ST_SETUP * sizeof(int), s));
-  // O = U^H U, Ui = U^-1
   prof_begin(h, PROF_POTRF);
   if ((rc = potrf_upper(h, n, ws.O, ws.Ui, ld))) return rc;
   if ((rc = trtri_upper(h, n, ws.O, ws.Ui, ld, ws.T))) return rc;
@@ -513,7 +511,55 @@ int stage_solve(excfv_handle* h, int n, int k, double evaltol, double* d_eval, c
                    TRI_LOWER, TRI_NONE)))
     return rc;
   if ((rc = mirror_upper(s, n, ws.H, ld))) return rc;
+  if (f32copy) {
+    // complex64 copy of C for the reduction (ws.T is free now); an even
+    // leading dimension keeps its columns 16-byte aligned for the tile loads
+    float2* Cf = reinterpret_cast<float2*>(ws.T);
+    const long long ldf = (n + 1) & ~1;
+    k_to_f32<<<dim3((n + 255) / 256, n), 256, 0, s>>>(n, ws.H, ld, Cf, ldf); count_launch();
+    CUDA_TRY(cudaGetLastError());
+  }
   prof_end(h, PROF_HEGST);
+  return EXCFV_OK;
+}
+
+static int solve_back_fp64(excfv_handle* h, int n, int k, double evaltol, double* d_eval, cplx* d_evec,
+                           long long ldevec);
+
+int stage_solve(excfv_handle* h, int n, int k, double evaltol, double* d_eval, cplx* d_evec,
+                long long ldevec) {
+  if (k < 1 || k > n) return EXCFV_ERR_ARG;
+  const bool mixed = h->prec == EXCFV_PREC_MIXED && n > 64;
+  if (mixed && mixed_states(n, k) > h->ws.kmax) {
+    excfv_set_error("mixed solve: workspace holds %d states, needs %d", h->ws.kmax, mixed_states(n, k));
+    return EXCFV_ERR_ARG;
+  }
+  if (!mixed && k > h->ws.kmax) return EXCFV_ERR_ARG;
+  int rc = solve_front(h, n, mixed);
+  if (rc) return rc;
+  return stage_solve_back(h, n, k, evaltol, d_eval, d_evec, ldevec);
+}
+
+int solve_front_f32copy(excfv_handle* h, int n) { return h->prec == EXCFV_PREC_MIXED && n > 64; }
+
+int stage_solve_back(excfv_handle* h, int n, int k, double evaltol, double* d_eval, cplx* d_evec,
+                     long long ldevec) {
+  if (h->prec == EXCFV_PREC_MIXED && n > 64)
+    return stage_solve_mixed(h, n, k, evaltol, d_eval, d_evec, ldevec);
+  return solve_back_fp64(h, n, k, evaltol, d_eval, d_evec, ldevec);
+}
+
+// From C (ws.H) and Ui onwards: tridiagonal reduction, eigenpairs of T,
+// back-transforms.
+static int solve_back_fp64(excfv_handle* h, int n, int k, double evaltol, double* d_eval, cplx* d_evec,
+                           long long ldevec) {
+  Workspace& ws = h->ws;
+  cudaStream_t s = h->stream;
+  const long long ld = n;
+  const cplx one = cmk(1.0, 0.0), zero = cmk(0.0, 0.0);
+  int rc;
+  if (k < 1 || k > n || k > ws.kmax) return EXCFV_ERR_ARG;
+  bind_gemm_ctx(h);
   // tridiagonal reduction: C = Q T Q^H, Q's reflectors in C (and, two-stage,
   // the chase reflectors in ws.O, the band in ws.T, the phase in ws.ybuf)
   const bool two = use_two_stage(h, n);
@@ -570,26 +616,9 @@ static int stage_solve_mixed(excfv_handle* h, int n, int k, double evaltol, doub
     return EXCFV_ERR_ARG;
   }
   bind_gemm_ctx(h);
-  CUDA_TRY(cudaMemsetAsync(ws.status, 0, ST_SETUP * sizeof(int), s));
-  prof_begin(h, PROF_POTRF);
-  if ((rc = potrf_upper(h, n, ws.O, ws.Ui, ld))) return rc;
-  if ((rc = trtri_upper(h, n, ws.O, ws.Ui, ld, ws.T))) return rc;
-  prof_end(h, PROF_POTRF);
-  prof_begin(h, PROF_HEGST);
-  if ((rc = zgemm1(s, OP_N, OP_N, n, n, n, one, ws.H, ld, ws.Ui, ld, zero, ws.T, ld, TRI_NONE,
-                   TRI_NONE, TRI_UPPER)))
-    return rc;
-  if ((rc = zgemm1(s, OP_C, OP_N, n, n, n, one, ws.Ui, ld, ws.T, ld, zero, ws.H, ld, TRI_UPPER,
-                   TRI_LOWER, TRI_NONE)))
-    return rc;
-  if ((rc = mirror_upper(s, n, ws.H, ld))) return rc;
-  // complex64 copy of C for the reduction (ws.T is free now); an even leading
-  // dimension keeps its columns 16-byte aligned for the tile loads
+  // C in ws.H, its complex64 copy in ws.T (solve_front)
   float2* Cf = reinterpret_cast<float2*>(ws.T);
   const long long ldf = (n + 1) & ~1;
-  k_to_f32<<<dim3((n + 255) / 256, n), 256, 0, s>>>(n, ws.H, ld, Cf, ldf); count_launch();
-  CUDA_TRY(cudaGetLastError());
-  prof_end(h, PROF_HEGST);
   if ((rc = tridiag_reduce_f32(h, n, Cf, ldf))) return rc;
   // reflectors back to FP64 into ws.O (the Cholesky factor is no longer needed)
   k_lower_to_f64<<<dim3((n + 255) / 256, n), 256, 0, s>>>(n, Cf, ldf, ws.O, ld); count_launch();

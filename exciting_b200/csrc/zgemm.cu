@@ -18,6 +18,9 @@
 // (lane%4 -> k row, lane/4 -> column) are bank-conflict free.
 #include "common.cuh"
 
+#include <algorithm>
+#include <vector>
+
 namespace {
 
 constexpr int BM = 64, BN = 64, BK = 8, PAD = 4, NT = 128;
@@ -29,24 +32,18 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-template <int OPA, int OPB>
-__global__ void __launch_bounds__(NT) zgemm_kernel(ZgemmArgs p) {
-  __shared__ __align__(16) double As[2][2][BK][LDS];
-  __shared__ __align__(16) double Bs[2][2][BK][LDS];
+typedef double SmemTile[2][2][BK][LDS];
 
+// One 64 x 64 output tile (rows i0.., columns j0..) of batch entry bz and
+// split-K piece split; As / Bs are the CTA's two-stage operand buffers.
+template <int OPA, int OPB>
+__device__ __forceinline__ void zgemm_tile(const ZgemmArgs& p, int i0, int j0, long long bz, int split,
+                                           SmemTile& As, SmemTile& Bs) {
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
-  // Tiles whose K range grows with the row (tri_a lower) or the column
-  // (tri_b upper) index are dispatched heaviest first, so that the last wave
-  // holds the short ones.
-  const bool rev_x = p.tri_a == TRI_LOWER;
-  const bool rev_y = p.tri_b == TRI_UPPER || (p.tri_a == TRI_LOWER && p.uplo_c == TRI_UPPER);
-  const int i0 = (rev_x ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x) * BM;
-  const int j0 = (rev_y ? (int)(gridDim.y - 1 - blockIdx.y) : (int)blockIdx.y) * BN;
   if (p.uplo_c == TRI_UPPER && i0 > j0 + BN - 1) return;
   if (p.uplo_c == TRI_LOWER && j0 > i0 + BM - 1) return;
-  const long long bz = (p.splitk > 1) ? blockIdx.z / p.splitk : blockIdx.z;
 
   const cplx* __restrict__ A = p.A + bz * p.strideA;
   const cplx* __restrict__ B = p.B + bz * p.strideB;
@@ -58,7 +55,6 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(ZgemmArgs p) {
   if (p.tri_b == TRI_UPPER) kend = min(kend, j0 + BN);
   if (p.tri_b == TRI_LOWER) kbeg = max(kbeg, j0);
   kbeg = (kbeg / BK) * BK;
-  const int split = (p.splitk > 1) ? (int)(blockIdx.z % p.splitk) : 0;
   if (p.splitk > 1 && kend > kbeg) {
     const int span = kend - kbeg;
     const int chunk = ((span + p.splitk - 1) / p.splitk + BK - 1) / BK * BK;
@@ -222,6 +218,36 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(ZgemmArgs p) {
   }
 }
 
+template <int OPA, int OPB>
+__global__ void __launch_bounds__(NT) zgemm_kernel(ZgemmArgs p) {
+  __shared__ __align__(16) SmemTile As;
+  __shared__ __align__(16) SmemTile Bs;
+  // Tiles whose K range grows with the row (tri_a lower) or the column
+  // (tri_b upper) index are dispatched heaviest first, so that the last wave
+  // holds the short ones.
+  const bool rev_x = p.tri_a == TRI_LOWER;
+  const bool rev_y = p.tri_b == TRI_UPPER || (p.tri_a == TRI_LOWER && p.uplo_c == TRI_UPPER);
+  const int i0 = (rev_x ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x) * BM;
+  const int j0 = (rev_y ? (int)(gridDim.y - 1 - blockIdx.y) : (int)blockIdx.y) * BN;
+  const long long bz = (p.splitk > 1) ? blockIdx.z / p.splitk : blockIdx.z;
+  const int split = (p.splitk > 1) ? (int)(blockIdx.z % p.splitk) : 0;
+  zgemm_tile<OPA, OPB>(p, i0, j0, bz, split, As, Bs);
+}
+
+// Grouped form: one launch over the tiles of many independent products of
+// different sizes.  tiles[b] = (problem, row tile, column tile, -) of CTA b,
+// listed by the host heaviest first; probs[problem] is an unbatched product
+// (batch 1, no split-K).
+template <int OPA, int OPB>
+__global__ void __launch_bounds__(NT) zgemm_grouped_kernel(const ZgemmArgs* __restrict__ probs,
+                                                           const int4* __restrict__ tiles) {
+  __shared__ __align__(16) SmemTile As;
+  __shared__ __align__(16) SmemTile Bs;
+  const int4 t = tiles[blockIdx.x];
+  const ZgemmArgs p = probs[t.x];
+  zgemm_tile<OPA, OPB>(p, t.y * BM, t.z * BN, 0, 0, As, Bs);
+}
+
 // C = alpha * sum_s P_s + beta * C over the split-K slabs (fixed order).
 __global__ void k_splitk_reduce(ZgemmArgs p) {
   const long long mn = (long long)p.m * p.n;
@@ -291,6 +317,57 @@ int zgemm(cudaStream_t s, int opA, int opB, const ZgemmArgs& a_in) {
     case OP_T * 3 + OP_N: return launch<OP_T, OP_N>(s, a);
     case OP_T * 3 + OP_C: return launch<OP_T, OP_C>(s, a);
     case OP_T * 3 + OP_T: return launch<OP_T, OP_T>(s, a);
+  }
+  return EXCFV_ERR_ARG;
+}
+
+// Length of the K range tile (ti, tj) of p runs over (the same rules as
+// zgemm_tile), or -1 for a tile outside the written triangle of C.
+static long long group_tile_k(const ZgemmArgs& p, int ti, int tj) {
+  const int i0 = ti * BM, j0 = tj * BN;
+  if (p.uplo_c == TRI_UPPER && i0 > j0 + BN - 1) return -1;
+  if (p.uplo_c == TRI_LOWER && j0 > i0 + BM - 1) return -1;
+  int kbeg = 0, kend = p.k;
+  if (p.tri_a == TRI_LOWER) kend = std::min(kend, i0 + BM);
+  if (p.tri_a == TRI_UPPER) kbeg = std::max(kbeg, i0);
+  if (p.tri_b == TRI_UPPER) kend = std::min(kend, j0 + BN);
+  if (p.tri_b == TRI_LOWER) kbeg = std::max(kbeg, j0);
+  return std::max(0, kend - (kbeg / BK) * BK);
+}
+
+void zgemm_group_add(const ZgemmArgs& p_in, std::vector<ZgemmArgs>& probs, std::vector<GroupTile>& tiles) {
+  ZgemmArgs p = p_in;
+  if (p.m <= 0 || p.n <= 0) return;
+  p.batch = 1; p.splitk = 1; p.part = nullptr; p.kdec = 0;
+  p.strideA = p.strideB = p.strideC = 0;
+  const int pi = (int)probs.size();
+  probs.push_back(p);
+  const int tm = (p.m + BM - 1) / BM, tn = (p.n + BN - 1) / BN;
+  for (int tj = 0; tj < tn; ++tj)
+    for (int ti = 0; ti < tm; ++ti) {
+      const long long kl = group_tile_k(p, ti, tj);
+      if (kl >= 0) tiles.push_back(GroupTile{pi, ti, tj, kl});
+    }
+}
+
+void zgemm_group_order(std::vector<GroupTile>& tiles, size_t from) {
+  std::stable_sort(tiles.begin() + (long)from, tiles.end(),
+                   [](const GroupTile& a, const GroupTile& b) { return a.klen > b.klen; });
+}
+
+int zgemm_grouped(cudaStream_t s, int opA, int opB, const ZgemmArgs* d_probs, const int4* d_tiles, int ntiles) {
+  if (ntiles <= 0) return 0;
+  switch (opA * 3 + opB) {
+#define EXCFV_GROUPED_CASE(A_, B_)                                                     \
+  case A_ * 3 + B_:                                                                    \
+    zgemm_grouped_kernel<A_, B_><<<ntiles, NT, 0, s>>>(d_probs, d_tiles);             \
+    count_launch();                                                                    \
+    return cudaGetLastError() == cudaSuccess ? 0 : EXCFV_ERR_CUDA;
+    EXCFV_GROUPED_CASE(OP_N, OP_N)
+    EXCFV_GROUPED_CASE(OP_N, OP_C)
+    EXCFV_GROUPED_CASE(OP_C, OP_N)
+    EXCFV_GROUPED_CASE(OP_C, OP_C)
+#undef EXCFV_GROUPED_CASE
   }
   return EXCFV_ERR_ARG;
 }

@@ -491,6 +491,19 @@ class FirstVariational:
         """Replay repeated device-pointer batches as one captured CUDA graph."""
         self._check(self._L.excfv_set_batch_graph(self._h, int(enable)), "excfv_set_batch_graph")
 
+    def set_batch_mode(self, mode: int) -> None:
+        """EXCFV_BATCH_LANES (whole chains on lanes) or EXCFV_BATCH_GROUPED
+        (Cholesky, inverse factor and two-sided reduction of all k-points as
+        grouped launches)."""
+        self._check(self._L.excfv_set_batch_mode(self._h, mode), "excfv_set_batch_mode")
+
+    def batch_mode(self) -> int:
+        return int(self._L.excfv_get_batch_mode(self._h))
+
+    def group_launches(self) -> int:
+        """Launches of the grouped front of the last grouped batch."""
+        return int(self._L.excfv_group_launches(self._h))
+
     def set_lanes(self, nlanes: int) -> None:
         self._check(self._L.excfv_set_lanes(self._h, nlanes), "excfv_set_lanes")
 

@@ -25,6 +25,10 @@ EXCFV_ERR_NOCONV = -7
 EXCFV_PREC_FP64 = 0
 EXCFV_PREC_MIXED = 1
 
+EXCFV_BATCH_LANES = 0
+EXCFV_BATCH_GROUPED = 1
+EXCFV_BATCH_AUTO = 2
+
 _i32p = C.POINTER(C.c_int32)
 _f64p = C.POINTER(C.c_double)
 
@@ -161,6 +165,9 @@ SIGNATURES = {
                                        C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "excfv_batch_info": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     "excfv_set_lanes": (C.c_int, [C.c_void_p, C.c_int32]),
+    "excfv_set_batch_mode": (C.c_int, [C.c_void_p, C.c_int32]),
+    "excfv_get_batch_mode": (C.c_int, [C.c_void_p]),
+    "excfv_group_launches": (C.c_longlong, [C.c_void_p]),
     "excfv_get_lanes": (C.c_int, [C.c_void_p]),
     "excfv_autotune_lanes": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -451,11 +451,30 @@ int excfv_batch_info(excfv_handle* h, int32_t nk, int32_t* info);
  * captured on the second occurrence (default on; 0 = always launch eagerly).
  * Profiling (excfv_profile) runs batches eagerly. */
 int excfv_set_batch_graph(excfv_handle* h, int enable);
+/* How a batch runs.  EXCFV_BATCH_LANES: each k-point's whole chain (match,
+ * setup, Cholesky, two-sided reduction, tridiagonal reduction, eigenpairs,
+ * back-transforms) on its lane.  EXCFV_BATCH_GROUPED: match and setup on the
+ * lanes, then the Cholesky factorisation, the inverse factor and the
+ * two-sided reduction of ALL k-points as grouped launches (one launch per
+ * step over every k-point that has it, one CTA per diagonal block or output
+ * tile, sizes from per-k-point descriptors), then the tridiagonal reduction
+ * onwards on the lanes again.  The grouped form holds four nmax x nmax
+ * complex matrices per k-point of the batch in device memory. */
+#define EXCFV_BATCH_LANES 0
+#define EXCFV_BATCH_GROUPED 1
+/* EXCFV_BATCH_AUTO (the default): grouped when the batch's four matrices per
+ * k-point take at most a quarter of the device's free memory, else lanes. */
+#define EXCFV_BATCH_AUTO 2
+int excfv_set_batch_mode(excfv_handle* h, int32_t mode);
+int excfv_get_batch_mode(excfv_handle* h);
+/* Launches of the grouped front of the last grouped batch (0 if none). */
+long long excfv_group_launches(excfv_handle* h);
 /* Lane count for the batched calls (0 = heuristic default). */
 int excfv_set_lanes(excfv_handle* h, int32_t nlanes);
 int excfv_get_lanes(excfv_handle* h);
-/* The project's autotuner: times the batch with 1, 2, 4, ... lanes and keeps
- * the fastest (device pointers, same arguments as excfv_seceqn_batched_dev). */
+/* The project's autotuner: times the batch in both forms (EXCFV_BATCH_LANES,
+ * EXCFV_BATCH_GROUPED) with 1, 2, 4, ... lanes and keeps the fastest form and
+ * lane count (device pointers, same arguments as excfv_seceqn_batched_dev). */
 int excfv_autotune_lanes(excfv_handle* h, int32_t nk, const int32_t* nmatp, const int32_t* ngp,
                          int32_t ngkmax, const double* const* gpc, const double* const* tpgpc,
                          const double* const* sfacgp, const int32_t* const* igpig,
