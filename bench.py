@@ -242,7 +242,7 @@ def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn, prec)
         launches_batch = fvb.launch_count() - l0
         mode = fvb.batch_mode()
         # launches of the other form on the same batch (one eager, untimed run)
-        fvb.set_batch_mode(0 if mode == 1 else 1)
+        fvb.set_batch_mode(1 if mode == 0 else 0)
         l0 = fvb.launch_count()
         fvb.seceqn_batched_dev(*bargs)
         torch.cuda.synchronize()
@@ -304,8 +304,11 @@ def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn, prec)
             "ms_per_batch": tot / args.batch_steps, "ms_per_batch_eager": tot_eager,
             "execution": "one CUDA graph per batch (captured on the second identical call)",
             "lanes": lanes,
-            "form": "grouped front (Cholesky, inverse factor, two-sided reduction of all k-points "
-                    "as grouped launches), lanes for the rest" if mode == 1 else "lanes (whole chains)",
+            "form": {0: "lanes (whole chains)",
+                     1: "grouped front (Cholesky, inverse factor, two-sided reduction of all k-points "
+                        "as grouped launches), lanes for the rest",
+                     3: "grouped front per lane (each lane's k-points' Cholesky, inverse factor and "
+                        "two-sided reduction as grouped launches on its stream)"}.get(mode, str(mode)),
             "launches_per_batch": int(launches_batch),
             "launches_per_batch_other_form": int(launches_other),
             "lane_stage_ms_per_k": {kk: round(v[0] / nk, 3) for kk, v in bprof.items()},

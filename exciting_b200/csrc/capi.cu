@@ -1267,6 +1267,7 @@ static int check_batch(excfv_handle* h, const BatchArgs& b, int* nmax) {
 
 static int enqueue_batch(excfv_handle* h, const BatchArgs& b, int L);
 static int run_batch_graph(excfv_handle* h, const BatchArgs& b, int L);
+static void group_segments(excfv_handle* h, const BatchArgs& b, int L, std::vector<std::vector<int>>& segs);
 
 // Enqueues the whole batch on L lanes (largest k-points first, each to the
 // least-loaded lane), fork/join on h->stream.
@@ -1293,7 +1294,11 @@ static int run_batch(excfv_handle* h, const BatchArgs& b, int L) {
     const bool have = group_slots_hold(h, b.nk, nmax);
     h->batch_form = (have || need <= 0.25 * (double)fr) ? EXCFV_BATCH_GROUPED : EXCFV_BATCH_LANES;
   }
-  if (h->batch_form == EXCFV_BATCH_GROUPED && (rc = group_plan_front(h, b.nk, b.nmatp, nmax))) return rc;
+  if (h->batch_form == EXCFV_BATCH_GROUPED || h->batch_form == EXCFV_BATCH_GROUPED_LANES) {
+    std::vector<std::vector<int>> segs;
+    group_segments(h, b, L, segs);
+    if ((rc = group_plan_front(h, b.nk, b.nmatp, nmax, segs))) return rc;
+  }
   if (!b.host && h->graph_on && !h->prof.on) return run_batch_graph(h, b, L);
   return enqueue_batch(h, b, L);
 }
@@ -1313,6 +1318,25 @@ static void deal_lanes(const BatchArgs& b, int L, std::vector<int>& order, std::
     lane_of[k] = l;
     load[l] += cost(k);
   }
+}
+
+// The k-points of each lane in the order the lane runs them.
+static void lane_lists(const BatchArgs& b, int L, std::vector<std::vector<int>>& lists) {
+  std::vector<int> order, lane_of;
+  deal_lanes(b, L, order, lane_of);
+  lists.assign(L, {});
+  for (int k : order) lists[lane_of[k]].push_back(k);
+}
+
+// Segments of the grouped front: all k-points together (EXCFV_BATCH_GROUPED)
+// or each lane's k-points (EXCFV_BATCH_GROUPED_LANES).
+static void group_segments(excfv_handle* h, const BatchArgs& b, int L, std::vector<std::vector<int>>& segs) {
+  if (h->batch_form == EXCFV_BATCH_GROUPED_LANES) {
+    lane_lists(b, L, segs);
+    return;
+  }
+  segs.assign(1, {});
+  for (int k = 0; k < b.nk; ++k) segs[0].push_back(k);
 }
 
 static int fork_lanes(excfv_handle* h, int L) {
@@ -1349,79 +1373,99 @@ struct SlotScope {
   ~SlotScope() { ws.H = H; ws.O = O; ws.Ui = Ui; ws.T = T; }
 };
 
-// The grouped batch: per lane match + setup into the k-points' slots; the
-// grouped front (Cholesky, inverse factor, two-sided reduction) of all
-// k-points on h->stream; per lane the rest of each k-point's solve.
-static int enqueue_grouped(excfv_handle* h, const BatchArgs& b, int L) {
-  int rc = EXCFV_OK;
+// One k-point's inputs, match and setup (H and O into its slots) on lane c;
+// its status words (the setup's) are kept in the batch's status array.
+static int grouped_setup_k(excfv_handle* h, excfv_handle* c, const BatchArgs& b, int k) {
   const cudaMemcpyKind in = b.host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  Workspace& ws = c->ws;
+  cudaStream_t s = c->stream;
+  const int ngp = b.ngp[k], n = b.nmatp[k];
+  int rc;
+  CUDA_TRY(cudaMemcpyAsync(ws.gpc, b.gpc[k], sizeof(double) * ngp, in, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.tpgpc, b.tpgpc[k], sizeof(double) * 2 * ngp, in, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.sfacgp, b.sfacgp[k], sizeof(cplx) * (size_t)b.ngkmax * h->st.natmtot, in, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.igpig, b.igpig[k], sizeof(int) * ngp, in, s));
+  CUDA_TRY(cudaMemcpyAsync(ws.vgpc, b.vgpc[k], sizeof(double) * 3 * ngp, in, s));
+  if ((rc = stage_match(c, ngp, b.ngkmax, nullptr))) return rc;
+  {
+    SlotScope sc(h, c, k);
+    if ((rc = stage_setup(c, n, ngp, false))) return rc;
+  }
+  CUDA_TRY(cudaMemcpyAsync(h->kinfo + (size_t)k * ST_NWORDS, ws.status, sizeof(int) * ST_NWORDS,
+                           cudaMemcpyDeviceToDevice, s));
+  return EXCFV_OK;
+}
+
+// The rest of one k-point's solve after the grouped front, on lane c.
+static int grouped_back_k(excfv_handle* h, excfv_handle* c, const BatchArgs& b, int k) {
   const cudaMemcpyKind out = b.host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
   const int k_st = h->st.nstfv;
-  std::vector<int> order, lane_of;
-  deal_lanes(b, L, order, lane_of);
-  if ((rc = fork_lanes(h, L))) return rc;
-  for (int idx = 0; idx < b.nk && rc == EXCFV_OK; ++idx) {
-    const int k = order[idx];
-    excfv_handle* c = h->lanes[lane_of[k]];
-    Workspace& ws = c->ws;
-    cudaStream_t s = c->stream;
-    const int ngp = b.ngp[k], n = b.nmatp[k];
-    CUDA_TRY(cudaMemcpyAsync(ws.gpc, b.gpc[k], sizeof(double) * ngp, in, s));
-    CUDA_TRY(cudaMemcpyAsync(ws.tpgpc, b.tpgpc[k], sizeof(double) * 2 * ngp, in, s));
-    CUDA_TRY(cudaMemcpyAsync(ws.sfacgp, b.sfacgp[k], sizeof(cplx) * (size_t)b.ngkmax * h->st.natmtot,
-                             in, s));
-    CUDA_TRY(cudaMemcpyAsync(ws.igpig, b.igpig[k], sizeof(int) * ngp, in, s));
-    CUDA_TRY(cudaMemcpyAsync(ws.vgpc, b.vgpc[k], sizeof(double) * 3 * ngp, in, s));
-    if ((rc = stage_match(c, ngp, b.ngkmax, nullptr))) break;
-    {
-      SlotScope sc(h, c, k);
-      if ((rc = stage_setup(c, n, ngp, false))) break;
-    }
-    CUDA_TRY(cudaMemcpyAsync(h->kinfo + (size_t)k * ST_NWORDS, ws.status, sizeof(int) * ST_NWORDS,
-                             cudaMemcpyDeviceToDevice, s));
-  }
-  if (rc) return rc;
-  if ((rc = join_lanes(h, L))) return rc;
-  if ((rc = group_enqueue_front(h))) return rc;
-  if ((rc = fork_lanes(h, L))) return rc;
-  for (int idx = 0; idx < b.nk && rc == EXCFV_OK; ++idx) {
-    const int k = order[idx];
-    excfv_handle* c = h->lanes[lane_of[k]];
-    Workspace& ws = c->ws;
-    cudaStream_t s = c->stream;
-    const int n = b.nmatp[k];
-    CUDA_TRY(cudaMemcpyAsync(ws.status, h->kinfo + (size_t)k * ST_NWORDS, sizeof(int) * ST_NWORDS,
-                             cudaMemcpyDeviceToDevice, s));
-    {
-      SlotScope sc(h, c, k);
-      if (b.host) {
-        cplx* ov = ws.apwalm;
-        const size_t na = (size_t)b.ngkmax * h->st.apwordmax * h->st.lmmaxapw * h->st.natmtot;
-        if ((size_t)n * k_st > na) {
-          excfv_set_error("batched host path: nmatp*nstfv exceeds the lane staging buffer");
-          rc = EXCFV_ERR_UNSUPPORTED;
-          break;
-        }
-        if ((rc = stage_solve_back(c, n, k_st, h->st.evaltol, ws.w, ov, n))) break;
-        CUDA_TRY(cudaMemcpy2DAsync(b.evecfv[k], sizeof(cplx) * b.nmatmax, ov, sizeof(cplx) * n,
-                                   sizeof(cplx) * n, k_st, out, s));
-        CUDA_TRY(cudaMemcpyAsync(b.evalfv[k], ws.w, sizeof(double) * k_st, out, s));
-      } else {
-        if ((rc = stage_solve_back(c, n, k_st, h->st.evaltol, b.evalfv[k], (cplx*)b.evecfv[k], b.nmatmax)))
-          break;
+  Workspace& ws = c->ws;
+  cudaStream_t s = c->stream;
+  const int n = b.nmatp[k];
+  int rc;
+  CUDA_TRY(cudaMemcpyAsync(ws.status, h->kinfo + (size_t)k * ST_NWORDS, sizeof(int) * ST_NWORDS,
+                           cudaMemcpyDeviceToDevice, s));
+  {
+    SlotScope sc(h, c, k);
+    if (b.host) {
+      cplx* ov = ws.apwalm;
+      const size_t na = (size_t)b.ngkmax * h->st.apwordmax * h->st.lmmaxapw * h->st.natmtot;
+      if ((size_t)n * k_st > na) {
+        excfv_set_error("batched host path: nmatp*nstfv exceeds the lane staging buffer");
+        return EXCFV_ERR_UNSUPPORTED;
       }
+      if ((rc = stage_solve_back(c, n, k_st, h->st.evaltol, ws.w, ov, n))) return rc;
+      CUDA_TRY(cudaMemcpy2DAsync(b.evecfv[k], sizeof(cplx) * b.nmatmax, ov, sizeof(cplx) * n, sizeof(cplx) * n,
+                                 k_st, out, s));
+      CUDA_TRY(cudaMemcpyAsync(b.evalfv[k], ws.w, sizeof(double) * k_st, out, s));
+    } else {
+      if ((rc = stage_solve_back(c, n, k_st, h->st.evaltol, b.evalfv[k], (cplx*)b.evecfv[k], b.nmatmax)))
+        return rc;
     }
-    CUDA_TRY(cudaMemcpyAsync(h->kinfo + (size_t)k * ST_NWORDS, ws.status, sizeof(int) * ST_NWORDS,
-                             cudaMemcpyDeviceToDevice, s));
   }
-  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(h->kinfo + (size_t)k * ST_NWORDS, ws.status, sizeof(int) * ST_NWORDS,
+                           cudaMemcpyDeviceToDevice, s));
+  return EXCFV_OK;
+}
+
+// The grouped batch.  EXCFV_BATCH_GROUPED: per lane match + setup into the
+// k-points' slots; the grouped front (Cholesky, inverse factor, two-sided
+// reduction) of all k-points on h->stream; per lane the rest of each
+// k-point's solve.  EXCFV_BATCH_GROUPED_LANES: each lane sets up its own
+// k-points, runs their grouped front on its stream and goes on with their
+// solves, with no batch-wide join in between.
+static int enqueue_grouped(excfv_handle* h, const BatchArgs& b, int L) {
+  int rc = EXCFV_OK;
+  std::vector<std::vector<int>> lists;
+  lane_lists(b, L, lists);
+  if ((rc = fork_lanes(h, L))) return rc;
+  if (h->batch_form == EXCFV_BATCH_GROUPED_LANES) {
+    for (int l = 0; l < L; ++l) {
+      excfv_handle* c = h->lanes[l];
+      for (int k : lists[l])
+        if ((rc = grouped_setup_k(h, c, b, k))) return rc;
+      if (!lists[l].empty() && (rc = group_enqueue_front(h, l, c->stream, c))) return rc;
+      for (int k : lists[l])
+        if ((rc = grouped_back_k(h, c, b, k))) return rc;
+    }
+    return join_lanes(h, L);
+  }
+  for (int l = 0; l < L; ++l)
+    for (int k : lists[l])
+      if ((rc = grouped_setup_k(h, h->lanes[l], b, k))) return rc;
+  if ((rc = join_lanes(h, L))) return rc;
+  if ((rc = group_enqueue_front(h, 0, h->stream, h))) return rc;
+  if ((rc = fork_lanes(h, L))) return rc;
+  for (int l = 0; l < L; ++l)
+    for (int k : lists[l])
+      if ((rc = grouped_back_k(h, h->lanes[l], b, k))) return rc;
   return join_lanes(h, L);
 }
 
-// Stream work of one batch (no allocation, no host synchronisation), so that
-// it can also be captured into a CUDA graph.
 static int enqueue_batch(excfv_handle* h, const BatchArgs& b, int L) {
-  if (h->batch_form == EXCFV_BATCH_GROUPED) return enqueue_grouped(h, b, L);
+  if (h->batch_form == EXCFV_BATCH_GROUPED || h->batch_form == EXCFV_BATCH_GROUPED_LANES)
+    return enqueue_grouped(h, b, L);
   int rc = EXCFV_OK;
   cudaEvent_t fork;
   CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
@@ -1513,7 +1557,8 @@ int excfv_set_lanes(excfv_handle* h, int32_t nlanes) {
 int excfv_get_lanes(excfv_handle* h) { return h ? h->nlanes_pref : EXCFV_ERR_ARG; }
 
 int excfv_set_batch_mode(excfv_handle* h, int32_t mode) {
-  if (!h || (mode != EXCFV_BATCH_LANES && mode != EXCFV_BATCH_GROUPED && mode != EXCFV_BATCH_AUTO))
+  if (!h || (mode != EXCFV_BATCH_LANES && mode != EXCFV_BATCH_GROUPED && mode != EXCFV_BATCH_AUTO &&
+             mode != EXCFV_BATCH_GROUPED_LANES))
     return EXCFV_ERR_ARG;
   h->batch_mode = mode;
   return EXCFV_OK;
@@ -1670,7 +1715,7 @@ int excfv_autotune_lanes(excfv_handle* h, int32_t nk, const int32_t* nmatp, cons
   float best = 1e30f;
   int bestL = 1, bestMode = EXCFV_BATCH_LANES;
   const int cand[] = {1, 2, 4, 6, 8, 12, 16, 24, 32};
-  for (int mode : {EXCFV_BATCH_LANES, EXCFV_BATCH_GROUPED}) {
+  for (int mode : {EXCFV_BATCH_LANES, EXCFV_BATCH_GROUPED, EXCFV_BATCH_GROUPED_LANES}) {
     h->batch_mode = mode;
     for (int L : cand) {
       if (L > lmax) break;

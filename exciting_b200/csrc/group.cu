@@ -43,6 +43,8 @@ struct GroupPlan {
     int kind, a, b, off, cnt, kb;
   };
   std::vector<Op> ops;
+  std::vector<int> seg_begin;  // ops of segment s: [seg_begin[s], seg_begin[s+1])
+  std::vector<int> zero_k;     // k-points whose eigensolve status words a ZERO op clears
   long long launches = 0;
 };
 
@@ -105,18 +107,23 @@ bool group_slots_hold(const excfv_handle* h, int nk, int nmax) {
 }
 
 // Builds (or keeps) the plan of the grouped front for a batch of nk k-points
-// of orders nmatp[k] (status words of k-point k at h->kinfo + k ST_NWORDS).
+// of orders nmatp[k] (status words of k-point k at h->kinfo + k ST_NWORDS),
+// one op sequence per segment (a list of k-points grouped together).
 // Allocates the slots and descriptors and uploads them; when the plan
 // changes, the handle's stream is synchronised first (a previous batch may
 // still read the old descriptors).  Must not run inside a stream capture.
-int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax) {
+int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax,
+                     const std::vector<std::vector<int>>& segs) {
   if (!h->gplan) h->gplan = new GroupPlan();
   GroupPlan& P = *h->gplan;
-  const bool f32 = solve_front_f32copy(h, nmax) != 0;
   std::vector<unsigned long long> key = {(unsigned long long)nk, (unsigned long long)nmax,
                                          (unsigned long long)h->prec,
                                          (unsigned long long)(uintptr_t)h->kinfo};
   for (int k = 0; k < nk; ++k) key.push_back((unsigned long long)nmatp[k]);
+  for (const std::vector<int>& ks : segs) {
+    key.push_back(~0ull);
+    for (int k : ks) key.push_back((unsigned long long)k);
+  }
   const size_t S = (size_t)nmax * nmax;
   const bool slots_ok = P.slot[0] && P.slot_elems == S && P.slot_k >= nk;
   if (slots_ok && key == P.key) return EXCFV_OK;
@@ -138,6 +145,8 @@ int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax) {
   P.nk = nk;
   P.nmax = nmax;
   P.ops.clear();
+  P.seg_begin.clear();
+  P.zero_k.clear();
   P.launches = 0;
 
   std::vector<ZgemmArgs> probs;
@@ -156,112 +165,120 @@ int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax) {
     P.launches++;
   };
   const int NB = potrf_block();
-  P.ops.push_back({GroupPlan::OPK_ZERO_STATUS, 0, 0, 0, nk, 0});
-  P.ops.push_back({GroupPlan::OPK_PROF_BEGIN, PROF_POTRF, 0, 0, 0, 0});
-  // ZPOTRF, blocked right-looking: diagonal block, row panel, trailing update
-  for (int kb = 0; kb < nmax; kb += NB) {
-    const size_t p0 = pp.size();
-    for (int k = 0; k < nk; ++k)
-      if (nmatp[k] > kb) pp.push_back(PotrfProb{nmatp[k], (long long)nmatp[k], Os(k), Us(k), h->kinfo + (size_t)k * ST_NWORDS});
-    if (pp.size() > p0) {
-      P.ops.push_back({GroupPlan::OPK_POTRF, 0, 0, (int)p0, (int)(pp.size() - p0), kb});
-      P.launches++;
-    }
-    size_t t0 = tiles.size();
-    for (int k = 0; k < nk; ++k) {
-      const int n = nmatp[k];
-      const long long ld = n;
-      if (n <= kb) continue;
-      const int b = std::min(NB, n - kb), rest = n - kb - b;
-      if (rest <= 0) continue;
-      cplx* panel = Os(k) + kb + ld * (kb + b);
-      zgemm_group_add(gemm(b, rest, b, one, Us(k) + kb + ld * kb, ld, panel, ld, zero, panel, ld, TRI_NONE,
-                           TRI_LOWER, TRI_NONE),
-                      probs, tiles);
-    }
-    gemm_op(OP_C, OP_N, t0);
-    t0 = tiles.size();
-    for (int k = 0; k < nk; ++k) {
-      const int n = nmatp[k];
-      const long long ld = n;
-      if (n <= kb) continue;
-      const int b = std::min(NB, n - kb), rest = n - kb - b;
-      if (rest <= 0) continue;
-      const cplx* panel = Os(k) + kb + ld * (kb + b);
-      zgemm_group_add(gemm(rest, rest, b, mone, panel, ld, panel, ld, one, Os(k) + (kb + b) * (ld + 1), ld,
-                           TRI_UPPER),
-                      probs, tiles);
-    }
-    gemm_op(OP_C, OP_N, t0);
-  }
-  // U^-1: inverted diagonal blocks merged pairwise, level by level
-  //   inv([[U11, U12], [0, U22]]) = [[X11, -X11 U12 X22], [0, X22]]
-  for (int bs = NB; bs < nmax; bs *= 2) {
-    for (int half = 0; half < 2; ++half) {
-      const size_t t0 = tiles.size();
-      for (int k = 0; k < nk; ++k) {
+  for (const std::vector<int>& ks : segs) {
+    P.seg_begin.push_back((int)P.ops.size());
+    int smax = 0;
+    for (int k : ks) smax = std::max(smax, (int)nmatp[k]);
+    const bool f32 = solve_front_f32copy(h, smax) != 0;
+    P.ops.push_back({GroupPlan::OPK_ZERO_STATUS, 0, 0, (int)P.zero_k.size(), (int)ks.size(), 0});
+    P.zero_k.insert(P.zero_k.end(), ks.begin(), ks.end());
+    P.ops.push_back({GroupPlan::OPK_PROF_BEGIN, PROF_POTRF, 0, 0, 0, 0});
+    // ZPOTRF, blocked right-looking: diagonal block, row panel, trailing update
+    for (int kb = 0; kb < smax; kb += NB) {
+      const size_t p0 = pp.size();
+      for (int k : ks)
+        if (nmatp[k] > kb)
+          pp.push_back(PotrfProb{nmatp[k], (long long)nmatp[k], Os(k), Us(k), h->kinfo + (size_t)k * ST_NWORDS});
+      if (pp.size() > p0) {
+        P.ops.push_back({GroupPlan::OPK_POTRF, 0, 0, (int)p0, (int)(pp.size() - p0), kb});
+        P.launches++;
+      }
+      size_t t0 = tiles.size();
+      for (int k : ks) {
         const int n = nmatp[k];
         const long long ld = n;
-        if (bs >= n) continue;
-        const cplx* U = Os(k);
-        cplx* Ui = Us(k);
-        cplx* T = Ts(k);
-        const int nfull = n / (2 * bs), rem = n - nfull * 2 * bs;
-        const long long step = 2LL * bs * (ld + 1);
-        for (int q = 0; q < nfull; ++q) {
-          if (half == 0)  // T = U12 X22
-            zgemm_group_add(gemm(bs, bs, bs, one, U + ld * bs + q * step, ld, Ui + bs * (ld + 1) + q * step, ld, zero,
-                                 T + (size_t)q * bs * bs, bs, TRI_NONE, TRI_NONE, TRI_UPPER),
-                            probs, tiles);
-          else  // X12 = -X11 T
-            zgemm_group_add(gemm(bs, bs, bs, mone, Ui + q * step, ld, T + (size_t)q * bs * bs, bs, zero,
-                                 Ui + ld * bs + q * step, ld, TRI_NONE, TRI_UPPER, TRI_NONE),
-                            probs, tiles);
-        }
-        if (rem > bs) {  // a trailing pair whose second block is shorter
-          const int a0 = nfull * 2 * bs, d0 = a0 + bs, sd = n - d0;
-          cplx* Tq = T + (size_t)nfull * bs * bs;
-          if (half == 0)
-            zgemm_group_add(gemm(bs, sd, sd, one, U + a0 + ld * d0, ld, Ui + d0 + ld * d0, ld, zero, Tq, bs,
-                                 TRI_NONE, TRI_NONE, TRI_UPPER),
-                            probs, tiles);
-          else
-            zgemm_group_add(gemm(bs, sd, bs, mone, Ui + a0 + ld * a0, ld, Tq, bs, zero, Ui + a0 + ld * d0, ld,
-                                 TRI_NONE, TRI_UPPER, TRI_NONE),
-                            probs, tiles);
-        }
+        if (n <= kb) continue;
+        const int b = std::min(NB, n - kb), rest = n - kb - b;
+        if (rest <= 0) continue;
+        cplx* panel = Os(k) + kb + ld * (kb + b);
+        zgemm_group_add(gemm(b, rest, b, one, Us(k) + kb + ld * kb, ld, panel, ld, zero, panel, ld, TRI_NONE,
+                             TRI_LOWER, TRI_NONE),
+                        probs, tiles);
       }
-      gemm_op(OP_N, OP_N, t0);
+      gemm_op(OP_C, OP_N, t0);
+      t0 = tiles.size();
+      for (int k : ks) {
+        const int n = nmatp[k];
+        const long long ld = n;
+        if (n <= kb) continue;
+        const int b = std::min(NB, n - kb), rest = n - kb - b;
+        if (rest <= 0) continue;
+        const cplx* panel = Os(k) + kb + ld * (kb + b);
+        zgemm_group_add(gemm(rest, rest, b, mone, panel, ld, panel, ld, one, Os(k) + (kb + b) * (ld + 1), ld,
+                             TRI_UPPER),
+                        probs, tiles);
+      }
+      gemm_op(OP_C, OP_N, t0);
     }
-  }
-  P.ops.push_back({GroupPlan::OPK_PROF_END, PROF_POTRF, 0, 0, 0, 0});
-  P.ops.push_back({GroupPlan::OPK_PROF_BEGIN, PROF_HEGST, 0, 0, 0, 0});
-  // ZHEGST: T = H U^-1, C = U^-H T (upper), then both triangles
-  {
+    // U^-1: inverted diagonal blocks merged pairwise, level by level
+    //   inv([[U11, U12], [0, U22]]) = [[X11, -X11 U12 X22], [0, X22]]
+    for (int bs = NB; bs < smax; bs *= 2) {
+      for (int half = 0; half < 2; ++half) {
+        const size_t t0 = tiles.size();
+        for (int k : ks) {
+          const int n = nmatp[k];
+          const long long ld = n;
+          if (bs >= n) continue;
+          const cplx* U = Os(k);
+          cplx* Ui = Us(k);
+          cplx* T = Ts(k);
+          const int nfull = n / (2 * bs), rem = n - nfull * 2 * bs;
+          const long long step = 2LL * bs * (ld + 1);
+          for (int q = 0; q < nfull; ++q) {
+            if (half == 0)  // T = U12 X22
+              zgemm_group_add(gemm(bs, bs, bs, one, U + ld * bs + q * step, ld, Ui + bs * (ld + 1) + q * step, ld,
+                                   zero, T + (size_t)q * bs * bs, bs, TRI_NONE, TRI_NONE, TRI_UPPER),
+                              probs, tiles);
+            else  // X12 = -X11 T
+              zgemm_group_add(gemm(bs, bs, bs, mone, Ui + q * step, ld, T + (size_t)q * bs * bs, bs, zero,
+                                   Ui + ld * bs + q * step, ld, TRI_NONE, TRI_UPPER, TRI_NONE),
+                              probs, tiles);
+          }
+          if (rem > bs) {  // a trailing pair whose second block is shorter
+            const int a0 = nfull * 2 * bs, d0 = a0 + bs, sd = n - d0;
+            cplx* Tq = T + (size_t)nfull * bs * bs;
+            if (half == 0)
+              zgemm_group_add(gemm(bs, sd, sd, one, U + a0 + ld * d0, ld, Ui + d0 + ld * d0, ld, zero, Tq, bs,
+                                   TRI_NONE, TRI_NONE, TRI_UPPER),
+                              probs, tiles);
+            else
+              zgemm_group_add(gemm(bs, sd, bs, mone, Ui + a0 + ld * a0, ld, Tq, bs, zero, Ui + a0 + ld * d0, ld,
+                                   TRI_NONE, TRI_UPPER, TRI_NONE),
+                              probs, tiles);
+          }
+        }
+        gemm_op(OP_N, OP_N, t0);
+      }
+    }
+    P.ops.push_back({GroupPlan::OPK_PROF_END, PROF_POTRF, 0, 0, 0, 0});
+    P.ops.push_back({GroupPlan::OPK_PROF_BEGIN, PROF_HEGST, 0, 0, 0, 0});
+    // ZHEGST: T = H U^-1, C = U^-H T (upper), then both triangles
     size_t t0 = tiles.size();
-    for (int k = 0; k < nk; ++k) {
+    for (int k : ks) {
       const int n = nmatp[k];
       zgemm_group_add(gemm(n, n, n, one, Hs(k), n, Us(k), n, zero, Ts(k), n, TRI_NONE, TRI_NONE, TRI_UPPER), probs,
                       tiles);
     }
     gemm_op(OP_N, OP_N, t0);
     t0 = tiles.size();
-    for (int k = 0; k < nk; ++k) {
+    for (int k : ks) {
       const int n = nmatp[k];
       zgemm_group_add(gemm(n, n, n, one, Us(k), n, Ts(k), n, zero, Hs(k), n, TRI_UPPER, TRI_LOWER, TRI_NONE), probs,
                       tiles);
     }
     gemm_op(OP_C, OP_N, t0);
-    for (int k = 0; k < nk; ++k) {
+    const int m0 = (int)mp.size();
+    for (int k : ks) {
       const int n = nmatp[k];
       const bool fk = f32 && solve_front_f32copy(h, n);
       mp.push_back(MirrorProb{n, (long long)n, Hs(k), fk ? reinterpret_cast<float2*>(Ts(k)) : nullptr,
                               (long long)((n + 1) & ~1)});
     }
-    P.ops.push_back({GroupPlan::OPK_MIRROR, 0, 0, 0, (int)mp.size(), 0});
+    P.ops.push_back({GroupPlan::OPK_MIRROR, 0, 0, m0, (int)ks.size(), smax});
     P.launches++;
+    P.ops.push_back({GroupPlan::OPK_PROF_END, PROF_HEGST, 0, 0, 0, 0});
   }
-  P.ops.push_back({GroupPlan::OPK_PROF_END, PROF_HEGST, 0, 0, 0, 0});
+  P.seg_begin.push_back((int)P.ops.size());
 
   // upload
   std::vector<int4> t4(tiles.size());
@@ -277,17 +294,19 @@ int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax) {
   return EXCFV_OK;
 }
 
-// Enqueues the planned front on h->stream (no allocation, no host
-// synchronisation: safe inside a stream capture).
-int group_enqueue_front(excfv_handle* h) {
+// Enqueues segment seg of the planned front on stream s; its stage events go
+// to the profile of handle ph (no allocation, no host synchronisation: safe
+// inside a stream capture).
+int group_enqueue_front(excfv_handle* h, int seg, cudaStream_t s, excfv_handle* ph) {
   GroupPlan& P = *h->gplan;
-  cudaStream_t s = h->stream;
   int rc;
-  for (const GroupPlan::Op& op : P.ops) {
+  for (int i = P.seg_begin[seg]; i < P.seg_begin[seg + 1]; ++i) {
+    const GroupPlan::Op& op = P.ops[i];
     switch (op.kind) {
       case GroupPlan::OPK_ZERO_STATUS:
-        // eigensolve words of every k-point (the setup's word is kept)
-        CUDA_TRY(cudaMemset2DAsync(h->kinfo, sizeof(int) * ST_NWORDS, 0, sizeof(int) * ST_SETUP, op.cnt, s));
+        // eigensolve words of the segment's k-points (the setup's word is kept)
+        for (int q = 0; q < op.cnt; ++q)
+          CUDA_TRY(cudaMemsetAsync(h->kinfo + (size_t)P.zero_k[op.off + q] * ST_NWORDS, 0, sizeof(int) * ST_SETUP, s));
         break;
       case GroupPlan::OPK_POTRF:
         if ((rc = potrf_diag_grouped(s, P.d_potrf + op.off, op.cnt, op.kb))) return rc;
@@ -296,13 +315,13 @@ int group_enqueue_front(excfv_handle* h) {
         if ((rc = zgemm_grouped(s, op.a, op.b, P.d_probs, P.d_tiles + op.off, op.cnt))) return rc;
         break;
       case GroupPlan::OPK_MIRROR:
-        if ((rc = mirror_grouped(s, P.d_mirror + op.off, op.cnt, P.nmax))) return rc;
+        if ((rc = mirror_grouped(s, P.d_mirror + op.off, op.cnt, op.kb))) return rc;
         break;
       case GroupPlan::OPK_PROF_BEGIN:
-        prof_begin(h, op.a);
+        prof_begin(ph, op.a);
         break;
       case GroupPlan::OPK_PROF_END:
-        prof_end(h, op.a);
+        prof_end(ph, op.a);
         break;
     }
   }

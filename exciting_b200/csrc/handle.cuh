@@ -319,8 +319,11 @@ struct MirrorProb {
 int mirror_grouped(cudaStream_t s, const MirrorProb* d_probs, int nprob, int nmax);
 // the grouped front of a batch (group.cu): plan (before any capture), enqueue,
 // the k-point slots of H, O, U^-1 and T (which = 0..3), launches per front
-int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax);
-int group_enqueue_front(excfv_handle* h);
+// (segments: lists of k-points whose fronts are grouped together, each
+// enqueued on its own stream; stage events go to the profile of handle ph)
+int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax,
+                     const std::vector<std::vector<int>>& segs);
+int group_enqueue_front(excfv_handle* h, int seg, cudaStream_t s, excfv_handle* ph);
 cplx* group_slot(excfv_handle* h, int which, int k);
 long long group_front_launches(const excfv_handle* h);
 // whether the slots already allocated hold a batch of nk k-points of order <= nmax

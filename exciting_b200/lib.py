@@ -28,6 +28,7 @@ EXCFV_PREC_MIXED = 1
 EXCFV_BATCH_LANES = 0
 EXCFV_BATCH_GROUPED = 1
 EXCFV_BATCH_AUTO = 2
+EXCFV_BATCH_GROUPED_LANES = 3
 
 _i32p = C.POINTER(C.c_int32)
 _f64p = C.POINTER(C.c_double)

@@ -465,6 +465,10 @@ int excfv_set_batch_graph(excfv_handle* h, int enable);
 /* EXCFV_BATCH_AUTO (the default): grouped when the batch's four matrices per
  * k-point take at most a quarter of the device's free memory, else lanes. */
 #define EXCFV_BATCH_AUTO 2
+/* EXCFV_BATCH_GROUPED_LANES: as EXCFV_BATCH_GROUPED, but each lane groups the
+ * front of its own k-points on its own stream and goes on with their solves
+ * without waiting for the other lanes. */
+#define EXCFV_BATCH_GROUPED_LANES 3
 int excfv_set_batch_mode(excfv_handle* h, int32_t mode);
 int excfv_get_batch_mode(excfv_handle* h);
 /* Launches of the grouped front of the last grouped batch (0 if none). */
@@ -472,9 +476,10 @@ long long excfv_group_launches(excfv_handle* h);
 /* Lane count for the batched calls (0 = heuristic default). */
 int excfv_set_lanes(excfv_handle* h, int32_t nlanes);
 int excfv_get_lanes(excfv_handle* h);
-/* The project's autotuner: times the batch in both forms (EXCFV_BATCH_LANES,
- * EXCFV_BATCH_GROUPED) with 1, 2, 4, ... lanes and keeps the fastest form and
- * lane count (device pointers, same arguments as excfv_seceqn_batched_dev). */
+/* The project's autotuner: times the batch in every form (EXCFV_BATCH_LANES,
+ * EXCFV_BATCH_GROUPED, EXCFV_BATCH_GROUPED_LANES) with 1, 2, 4, ... lanes and
+ * keeps the fastest form and lane count (device pointers, same arguments as
+ * excfv_seceqn_batched_dev). */
 int excfv_autotune_lanes(excfv_handle* h, int32_t nk, const int32_t* nmatp, const int32_t* ngp,
                          int32_t ngkmax, const double* const* gpc, const double* const* tpgpc,
                          const double* const* sfacgp, const int32_t* const* igpig,

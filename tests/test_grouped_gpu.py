@@ -1,13 +1,15 @@
 """GPU parity of the grouped batch: the Cholesky factorisation, the inverse
-factor and the two-sided reduction of all k-points as grouped launches
-(excfv_set_batch_mode(EXCFV_BATCH_GROUPED)), the rest of each k-point's solve
-on the lanes; every k-point against the oracle's ZHEGVX."""
+factor and the two-sided reduction of all k-points (EXCFV_BATCH_GROUPED) or of
+each lane's k-points (EXCFV_BATCH_GROUPED_LANES) as grouped launches, the rest
+of each k-point's solve on the lanes; every k-point against the oracle's
+ZHEGVX."""
 import numpy as np
 import pytest
 import torch
 
 from exciting_b200 import synthetic as syn
-from exciting_b200.lib import EXCFV_BATCH_GROUPED, EXCFV_BATCH_LANES, EXCFV_PREC_MIXED
+from exciting_b200.lib import (EXCFV_BATCH_GROUPED, EXCFV_BATCH_GROUPED_LANES, EXCFV_BATCH_LANES,
+                               EXCFV_PREC_MIXED)
 from exciting_b200.fv import FirstVariational
 from oracle import fvref
 
@@ -43,14 +45,15 @@ def test_grouped_host_buffers(batch_problem):
     assert len({k.nmat for k in p.kpts}) == len(p.kpts)
     with FirstVariational(0) as fv:
         fv.set_static(p.static)
-        fv.set_batch_mode(EXCFV_BATCH_GROUPED)
-        assert fv.batch_mode() == EXCFV_BATCH_GROUPED
-        for lanes in (1, 3):
-            fv.set_lanes(lanes)
-            outs, info = fv.seceqn_batched(p.kpts, p.nmatmax)
-            assert np.all(info == 0)
-            _check(refs, p.kpts, outs, 1e-10, 1e-13, 1e-11)
-        assert fv.group_launches() > 0
+        for mode in (EXCFV_BATCH_GROUPED, EXCFV_BATCH_GROUPED_LANES):
+            fv.set_batch_mode(mode)
+            assert fv.batch_mode() == mode
+            for lanes in (1, 3):
+                fv.set_lanes(lanes)
+                outs, info = fv.seceqn_batched(p.kpts, p.nmatmax)
+                assert np.all(info == 0)
+                _check(refs, p.kpts, outs, 1e-10, 1e-13, 1e-11)
+            assert fv.group_launches() > 0
 
 
 def _dev(a, dtype):
@@ -78,7 +81,7 @@ def test_grouped_device_pointers_graph_replay(batch_problem, prec):
                 [e.data_ptr() for e in ev], [x.data_ptr() for x in X])
         torch.cuda.synchronize()
         fv.set_lanes(2)
-        for mode in (EXCFV_BATCH_GROUPED, EXCFV_BATCH_LANES):
+        for mode in (EXCFV_BATCH_GROUPED, EXCFV_BATCH_GROUPED_LANES, EXCFV_BATCH_LANES):
             fv.set_batch_mode(mode)
             for _ in range(3):
                 for e in ev:
