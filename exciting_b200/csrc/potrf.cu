@@ -16,159 +16,111 @@ namespace {
 
 constexpr int NBP = 64;
 
-// One CTA of DT threads factors the b x b diagonal block (b <= 64) and
-// inverts the factor, blocked in four 16-wide steps held in shared memory:
-//   step j:  U_jj = chol(A_jj), X_jj = U_jj^-1   (one warp, in registers)
-//            U_jc = X_jj^H A_jc            (c > j, the row panel)
-//            A_cd -= U_jc^H U_jd           (j < c <= d, the trailing update)
-// then X = U^-1 by merging the inverted diagonal blocks pairwise,
-//   inv([[U11, U12], [0, U22]]) = [[X11, -X11 U12 X22], [0, X22]],
-// for the 16-blocks (0,1), (2,3) and then the two 32-blocks.  Each 16 x 16
-// leaf is one warp: lane c (and lane c + 16, which repeats it) keeps column c
-// of the leaf in registers and takes the pivot row from the other lanes by
-// shuffles, so the whole block needs about twenty CTA barriers.  Rows and
-// columns past b are padded with the identity.
+// One CTA of 32 x 32 threads factors the b x b diagonal block (b <= 64) and
+// inverts the factor, as a 2 x 2 block recursion on 32 x 32 blocks held in
+// shared memory (thread (r, c) owns element (r, c) of a 32-block):
+//   U11 = chol(A11), X11 = U11^-1, U12 = X11^H A12, A22 -= U12^H U12,
+//   U22 = chol(A22), X22 = U22^-1, X12 = -X11 U12 X22.
+// FP64 vector throughput bounds this kernel, so the work is laid out such
+// that whole warps (one row each) drop out of every elimination step.
+// Rows/columns past b are padded with the identity.
 constexpr int LDB = 65;
-constexpr int DT = 256;   // threads of the diagonal-block kernel
-constexpr int LB = 16;    // leaf order
 
-// Factors A(o:o+16, o:o+16) in place (upper; zeros below the diagonal) and
-// writes its inverse into X(o:o+16, o:o+16).  Returns the 1-based position
-// within the 64-block of the first pivot that is not positive (0 if none).
-// Lanes apply every step to their whole column with a 0/1 weight instead of
-// a branch (entries below the diagonal are never read as part of U).
-__device__ __forceinline__ int leaf16(cplx* A, cplx* X, int o, int lane) {
-  const unsigned full = 0xffffffffu;
-  const int l = lane & (LB - 1);
-  cplx a[LB];
-#pragma unroll
-  for (int r = 0; r < LB; ++r) a[r] = A[(o + r) * LDB + o + l];
-  double rv[LB];
-  int fail = 0;
-#pragma unroll
-  for (int j = 0; j < LB; ++j) {
-    const double p = __shfl_sync(full, a[j].x, j);
-    const bool ok = p > 0.0;
-    if (!ok && fail == 0) fail = o + j + 1;
-    const double ri = ok ? 1.0 / sqrt(p) : 0.0;
-    rv[j] = ri;
-    a[j] = cscale(a[j], (l >= j) ? ri : 1.0);   // row j of U (columns c >= j)
-#pragma unroll
-    for (int r = j + 1; r < LB; ++r) {     // A(r, c) -= conj(U(j, r)) U(j, c), c >= r
-      const double m = (l >= r) ? 1.0 : 0.0;
-      const cplx u = cmk(m * __shfl_sync(full, a[j].x, r), m * __shfl_sync(full, a[j].y, r));
-      a[r] = csub(a[r], cmulc(u, a[j]));
-    }
+__device__ __forceinline__ bool chol32(cplx* A, double* rinv, int o, int tr, int tc, int* s_fail, int fail_base) {
+  // A is the 64 x LDB shared block; factor A(o:o+32, o:o+32) in place (upper)
+  if (tr == 0 && tc == 0) {
+    const double a = A[o * LDB + o].x;
+    rinv[o] = (a > 0.0) ? 1.0 / sqrt(a) : 0.0;
+    if (!(a > 0.0)) *s_fail = fail_base + 1;
   }
-  // back substitution U x = e_c for column c of X
-  cplx x[LB];
-#pragma unroll
-  for (int i = LB - 1; i >= 0; --i) {
-    cplx t = cmk(i == l ? 1.0 : 0.0, 0.0);
-#pragma unroll
-    for (int k = i + 1; k < LB; ++k) {
-      const cplx u = cmk(__shfl_sync(full, a[i].x, k), __shfl_sync(full, a[i].y, k));
-      t = csub(t, cmul(u, x[k]));
+  __syncthreads();
+  for (int j = 0; j < 32; ++j) {
+    if (*s_fail) return false;
+    if (tr == j && tc >= j) A[(o + j) * LDB + o + tc] = cscale(A[(o + j) * LDB + o + tc], rinv[o + j]);
+    __syncthreads();
+    if (tr > j && tc >= tr) {
+      cplx* x = &A[(o + tr) * LDB + o + tc];
+      *x = csub(*x, cmulc(A[(o + j) * LDB + o + tr], A[(o + j) * LDB + o + tc]));
+      if (tr == j + 1 && tc == j + 1) {
+        const double a = x->x;
+        rinv[o + j + 1] = (a > 0.0) ? 1.0 / sqrt(a) : 0.0;
+        if (!(a > 0.0)) *s_fail = fail_base + j + 2;
+      }
     }
-    x[i] = cscale(t, rv[i]);
+    __syncthreads();
   }
-  if (lane < LB) {
-#pragma unroll
-    for (int r = 0; r < LB; ++r) {
-      A[(o + r) * LDB + o + l] = (r <= l) ? a[r] : cmk(0.0, 0.0);
-      X[(o + r) * LDB + o + l] = (r <= l) ? x[r] : cmk(0.0, 0.0);
-    }
+  return true;
+}
+
+// X(o:o+32, o:o+32) = inverse of the upper factor U(o:o+32, o:o+32)
+__device__ __forceinline__ void inv32(const cplx* A, cplx* X, const double* rinv, int o, int tr, int tc) {
+  X[(o + tr) * LDB + o + tc] = cmk(tr == tc ? 1.0 : 0.0, 0.0);
+  __syncthreads();
+  for (int i = 31; i >= 0; --i) {
+    if (tr == i && tc >= i) X[(o + i) * LDB + o + tc] = cscale(X[(o + i) * LDB + o + tc], rinv[o + i]);
+    __syncthreads();
+    if (tr < i && tc >= i)
+      X[(o + tr) * LDB + o + tc] = csub(X[(o + tr) * LDB + o + tc],
+                                        cmul(A[(o + tr) * LDB + o + i], X[(o + i) * LDB + o + tc]));
+    __syncthreads();
   }
-  return fail;
 }
 
 __device__ __forceinline__ void potrf_diag_block(int n, int kb, cplx* O, long long ld, cplx* Ui, int* status) {
   extern __shared__ __align__(16) unsigned char dsm[];
   cplx* A = reinterpret_cast<cplx*>(dsm);   // 64 x LDB, row-major [r][c]
   cplx* X = A + NBP * LDB;
+  __shared__ double rinv[NBP];
   __shared__ int s_fail;
   if (status[ST_POTRF] != 0) return;
   const int b = min(NBP, n - kb);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int t = tid; t < NBP * NBP; t += DT) {
+  const int tc = threadIdx.x & 31, tr = threadIdx.x >> 5;
+  for (int t = threadIdx.x; t < NBP * NBP; t += 1024) {
     const int r = t % NBP, c = t / NBP;  // coalesced along r
     cplx a = cmk(r == c ? 1.0 : 0.0, 0.0);
     if (r < b && c < b && r <= c) a = O[(kb + r) + ld * (kb + c)];
     A[r * LDB + c] = a;
     X[r * LDB + c] = cmk(0.0, 0.0);
   }
+  if (threadIdx.x == 0) s_fail = 0;
   __syncthreads();
-  for (int j = 0; j < NBP / LB; ++j) {
-    const int o = j * LB;
-    if (warp == 0) {
-      const int f = leaf16(A, X, o, lane);
-      if (lane == 0) s_fail = f;
-    }
+  if (!chol32(A, rinv, 0, tr, tc, &s_fail, 0)) {
+    if (threadIdx.x == 0 && s_fail <= b) atomicCAS(&status[ST_POTRF], 0, kb + s_fail);
+    return;
+  }
+  inv32(A, X, rinv, 0, tr, tc);
+  // U12 = X11^H A12 (thread (r, c): column 32 + c)
+  {
+    cplx acc = cmk(0.0, 0.0);
+    for (int k = 0; k <= tr; ++k) acc = cadd(acc, cmulc(X[k * LDB + tr], A[k * LDB + 32 + tc]));
     __syncthreads();
-    if (s_fail) {
-      if (tid == 0 && s_fail <= b) atomicCAS(&status[ST_POTRF], 0, kb + s_fail);
-      return;
-    }
-    const int c0 = o + LB, nc = NBP - c0;
-    if (nc == 0) break;
-    // row panel U(o+r, c) = sum_{k <= r} conj(X(o+k, o+r)) A(o+k, c)
-    {
-      cplx acc[3];
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const int t = tid + q * DT;
-        acc[q] = cmk(0.0, 0.0);
-        if (t < LB * nc) {
-          const int r = t % LB, c = c0 + t / LB;
-          for (int k = 0; k <= r; ++k)
-            acc[q] = cadd(acc[q], cmulc(X[(o + k) * LDB + o + r], A[(o + k) * LDB + c]));
-        }
-      }
-      __syncthreads();
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const int t = tid + q * DT;
-        if (t < LB * nc) A[(o + t % LB) * LDB + c0 + t / LB] = acc[q];
-      }
-      __syncthreads();
-    }
-    // trailing update A(i, jj) -= sum_k conj(U(o+k, i)) U(o+k, jj), c0 <= i <= jj
-    for (int t = tid; t < nc * nc; t += DT) {
-      const int i = c0 + t % nc, jj = c0 + t / nc;
-      if (i > jj) continue;
-      cplx acc = cmk(0.0, 0.0);
-#pragma unroll
-      for (int k = 0; k < LB; ++k) acc = cadd(acc, cmulc(A[(o + k) * LDB + i], A[(o + k) * LDB + jj]));
-      A[i * LDB + jj] = csub(A[i * LDB + jj], acc);
-    }
+    A[tr * LDB + 32 + tc] = acc;
     __syncthreads();
   }
-  // X = U^-1: 16-blocks (0,1) and (2,3), then the 32-blocks; T goes to the
-  // (unused) lower part of X
-  for (int w = LB; w < NBP; w *= 2) {
-    const int npair = NBP / (2 * w);
-    // T = U12 X22 into X(p0 + w + r, p0 + c)
-    for (int t = tid; t < npair * w * w; t += DT) {
-      const int pr = t / (w * w), e = t % (w * w), r = e % w, c = e / w;
-      const int p0 = pr * 2 * w;
-      cplx acc = cmk(0.0, 0.0);
-      for (int k = 0; k <= c; ++k)
-        acc = cadd(acc, cmul(A[(p0 + r) * LDB + p0 + w + k], X[(p0 + w + k) * LDB + p0 + w + c]));
-      X[(p0 + w + r) * LDB + p0 + c] = acc;
-    }
+  // A22 -= U12^H U12 (upper)
+  if (tc >= tr) {
+    cplx acc = cmk(0.0, 0.0);
+    for (int k = 0; k < 32; ++k) acc = cadd(acc, cmulc(A[k * LDB + 32 + tr], A[k * LDB + 32 + tc]));
+    A[(32 + tr) * LDB + 32 + tc] = csub(A[(32 + tr) * LDB + 32 + tc], acc);
+  }
+  __syncthreads();
+  if (!chol32(A, rinv, 32, tr, tc, &s_fail, 32)) {
+    if (threadIdx.x == 0 && s_fail <= b) atomicCAS(&status[ST_POTRF], 0, kb + s_fail);
+    return;
+  }
+  inv32(A, X, rinv, 32, tr, tc);
+  // X12 = -X11 (U12 X22): T = U12 X22 into X's lower-left block, then X12
+  {
+    cplx acc = cmk(0.0, 0.0);
+    for (int k = 0; k <= tc; ++k) acc = cadd(acc, cmul(A[tr * LDB + 32 + k], X[(32 + k) * LDB + 32 + tc]));
+    X[(32 + tr) * LDB + tc] = acc;  // scratch: lower-left block of X
     __syncthreads();
-    // X12 = -X11 T
-    for (int t = tid; t < npair * w * w; t += DT) {
-      const int pr = t / (w * w), e = t % (w * w), r = e % w, c = e / w;
-      const int p0 = pr * 2 * w;
-      cplx acc = cmk(0.0, 0.0);
-      for (int k = r; k < w; ++k)
-        acc = cadd(acc, cmul(X[(p0 + r) * LDB + p0 + k], X[(p0 + w + k) * LDB + p0 + c]));
-      X[(p0 + r) * LDB + p0 + w + c] = cmk(-acc.x, -acc.y);
-    }
+    cplx acc2 = cmk(0.0, 0.0);
+    for (int k = tr; k < 32; ++k) acc2 = cadd(acc2, cmul(X[tr * LDB + k], X[(32 + k) * LDB + tc]));
+    X[tr * LDB + 32 + tc] = cmk(-acc2.x, -acc2.y);
     __syncthreads();
   }
-  for (int t = tid; t < NBP * NBP; t += DT) {
+  for (int t = threadIdx.x; t < NBP * NBP; t += 1024) {
     const int r = t % NBP, c = t / NBP;
     if (r < b && c < b && r <= c) {
       O[(kb + r) + ld * (kb + c)] = A[r * LDB + c];
@@ -177,13 +129,13 @@ __device__ __forceinline__ void potrf_diag_block(int n, int kb, cplx* O, long lo
   }
 }
 
-__global__ void __launch_bounds__(DT) k_potrf_diag(int n, int kb, cplx* O, long long ld, cplx* Ui,
+__global__ void __launch_bounds__(1024) k_potrf_diag(int n, int kb, cplx* O, long long ld, cplx* Ui,
                                                      int* status) {
   potrf_diag_block(n, kb, O, ld, Ui, status);
 }
 
 // Grouped form: CTA b factors diagonal block kb of problem b.
-__global__ void __launch_bounds__(DT) k_potrf_diag_grouped(const PotrfProb* __restrict__ probs, int kb) {
+__global__ void __launch_bounds__(1024) k_potrf_diag_grouped(const PotrfProb* __restrict__ probs, int kb) {
   const PotrfProb p = probs[blockIdx.x];
   potrf_diag_block(p.n, kb, p.O, p.ld, p.Ui, p.status);
 }
@@ -197,7 +149,7 @@ int potrf_diag_grouped(cudaStream_t s, const PotrfProb* d_probs, int nprob, int 
   if (nprob <= 0) return EXCFV_OK;
   const int smem = potrf_smem_bytes();
   CUDA_TRY(cudaFuncSetAttribute(k_potrf_diag_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  k_potrf_diag_grouped<<<nprob, DT, smem, s>>>(d_probs, kb); count_launch();
+  k_potrf_diag_grouped<<<nprob, 1024, smem, s>>>(d_probs, kb); count_launch();
   CUDA_TRY(cudaGetLastError());
   return EXCFV_OK;
 }
@@ -209,7 +161,7 @@ int potrf_upper(excfv_handle* h, int n, cplx* O, cplx* Ui, long long ld) {
   CUDA_TRY(cudaFuncSetAttribute(k_potrf_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   for (int kb = 0; kb < n; kb += NBP) {
     const int b = min(NBP, n - kb);
-    k_potrf_diag<<<1, DT, smem, s>>>(n, kb, O, ld, Ui, h->ws.status); count_launch();
+    k_potrf_diag<<<1, 1024, smem, s>>>(n, kb, O, ld, Ui, h->ws.status); count_launch();
     CUDA_TRY(cudaGetLastError());
     const int rest = n - kb - b;
     if (rest <= 0) break;
