@@ -241,6 +241,7 @@ def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn, prec)
         tot_eager = timed(1)
         launches_batch = fvb.launch_count() - l0
         mode = fvb.batch_mode()
+        tile_rows = fvb.group_tile() if mode != 0 else None
         # launches of the other form on the same batch (one eager, untimed run)
         fvb.set_batch_mode(1 if mode == 0 else 0)
         l0 = fvb.launch_count()
@@ -309,6 +310,7 @@ def run_batched(args, torch, np, dev, local_rank, rank, world, flush, syn, prec)
                         "as grouped launches), lanes for the rest",
                      3: "grouped front per lane (each lane's k-points' Cholesky, inverse factor and "
                         "two-sided reduction as grouped launches on its stream)"}.get(mode, str(mode)),
+            "group_tile_rows": tile_rows,
             "launches_per_batch": int(launches_batch),
             "launches_per_batch_other_form": int(launches_other),
             "lane_stage_ms_per_k": {kk: round(v[0] / nk, 3) for kk, v in bprof.items()},

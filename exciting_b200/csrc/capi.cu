@@ -1568,6 +1568,14 @@ int excfv_get_batch_mode(excfv_handle* h) { return h ? h->batch_mode : EXCFV_ERR
 
 long long excfv_group_launches(excfv_handle* h) { return h ? group_front_launches(h) : 0; }
 
+int excfv_set_group_tile(excfv_handle* h, int32_t rows) {
+  if (!h || (rows != 64 && rows != 128)) return EXCFV_ERR_ARG;
+  h->group_tbm = rows;
+  return EXCFV_OK;
+}
+
+int excfv_get_group_tile(excfv_handle* h) { return h ? h->group_tbm : EXCFV_ERR_ARG; }
+
 static std::vector<unsigned long long> batch_key(const excfv_handle* h, const BatchArgs& b, int L) {
   std::vector<unsigned long long> k = {(unsigned long long)b.nk, (unsigned long long)L,
                                        (unsigned long long)h->prec, h->static_gen,
@@ -1692,9 +1700,10 @@ int excfv_batch_info(excfv_handle* h, int32_t nk, int32_t* info) {
   return batch_info(h, nk, info);
 }
 
-// Times the batch in both forms (lanes; grouped front) with 1, 2, 4, 6, 8,
-// 12, ... lanes (those the SM budget allows) and keeps the fastest form and
-// lane count for later batched calls.  Device pointers; the outputs of
+// Times the batch in every form (lanes; grouped front over the batch or per
+// lane) with 1, 2, 4, 6, 8, 12, ... lanes (those the SM budget allows), then
+// the winning grouped form with the other GEMM tile shape, and keeps the
+// fastest form, lane count and tile shape for later batched calls.  Device pointers; the outputs of
 // the last timed run are valid.  best_ms (optional) receives the winning time.
 int excfv_autotune_lanes(excfv_handle* h, int32_t nk, const int32_t* nmatp, const int32_t* ngp,
                          int32_t ngkmax, const double* const* gpc, const double* const* tpgpc,
@@ -1713,8 +1722,9 @@ int excfv_autotune_lanes(excfv_handle* h, int32_t nk, const int32_t* nmatp, cons
   CUDA_TRY(cudaEventCreate(&e0));
   CUDA_TRY(cudaEventCreate(&e1));
   float best = 1e30f;
-  int bestL = 1, bestMode = EXCFV_BATCH_LANES;
+  int bestL = 1, bestMode = EXCFV_BATCH_LANES, bestTbm = 64;
   const int cand[] = {1, 2, 4, 6, 8, 12, 16, 24, 32};
+  h->group_tbm = 64;
   for (int mode : {EXCFV_BATCH_LANES, EXCFV_BATCH_GROUPED, EXCFV_BATCH_GROUPED_LANES}) {
     h->batch_mode = mode;
     for (int L : cand) {
@@ -1732,11 +1742,29 @@ int excfv_autotune_lanes(excfv_handle* h, int32_t nk, const int32_t* nmatp, cons
     }
     if (rc) break;
   }
+  // the grouped forms' GEMM tile shape: 128 x 64 tiles against the 64 x 64 of
+  // the search above, at the winning form and lane count
+  if (rc == EXCFV_OK && bestMode != EXCFV_BATCH_LANES) {
+    h->batch_mode = bestMode;
+    h->group_tbm = 128;
+    for (int rep = 0; rep < 2 && rc == EXCFV_OK; ++rep) {
+      CUDA_TRY(cudaEventRecord(e0, h->stream));
+      if ((rc = run_batch(h, b, bestL))) break;
+      CUDA_TRY(cudaEventRecord(e1, h->stream));
+      CUDA_TRY(cudaEventSynchronize(e1));
+    }
+    float ms = 0.f;
+    if (rc == EXCFV_OK) {
+      CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best) { best = ms; bestTbm = 128; }
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
   h->nlanes_pref = bestL;
   h->batch_mode = bestMode;
+  h->group_tbm = bestTbm;
   if (best_ms) *best_ms = best;
   rc = run_batch(h, b, bestL);
   if (rc) return rc;

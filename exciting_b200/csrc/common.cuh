@@ -106,7 +106,7 @@ const GemmCtx& gemm_ctx();
 int zgemm(cudaStream_t s, int opA, int opB, const ZgemmArgs& a);
 
 // Grouped products: many unbatched products of different sizes in one
-// launch, one CTA per 64 x 64 output tile.  The host appends each product and
+// launch, one CTA per output tile.  The host appends each product and
 // its tiles to shared lists (zgemm_group_add; tile entries carry the global
 // product index), orders one launch's tiles heaviest first
 // (zgemm_group_order), uploads both lists and launches zgemm_grouped with the
@@ -115,9 +115,12 @@ struct GroupTile {
   int prob, ti, tj;
   long long klen;  // K range of the tile: the ordering key, not uploaded
 };
-void zgemm_group_add(const ZgemmArgs& p, std::vector<ZgemmArgs>& probs, std::vector<GroupTile>& tiles);
+// Tile shapes: tbm x 64 outputs per CTA, tbm = 64 or 128.
+void zgemm_group_add(const ZgemmArgs& p, std::vector<ZgemmArgs>& probs, std::vector<GroupTile>& tiles,
+                     int tbm);
 void zgemm_group_order(std::vector<GroupTile>& tiles, size_t from);
-int zgemm_grouped(cudaStream_t s, int opA, int opB, const ZgemmArgs* d_probs, const int4* d_tiles, int ntiles);
+int zgemm_grouped(cudaStream_t s, int opA, int opB, const ZgemmArgs* d_probs, const int4* d_tiles, int ntiles,
+                  int tbm);
 
 // convenience: single (non-batched) product
 int zgemm1(cudaStream_t s, int opA, int opB, int m, int n, int k, cplx alpha,

@@ -46,6 +46,7 @@ struct GroupPlan {
   std::vector<int> seg_begin;  // ops of segment s: [seg_begin[s], seg_begin[s+1])
   std::vector<int> zero_k;     // k-points whose eigensolve status words a ZERO op clears
   long long launches = 0;
+  int tbm = 64;                // rows of the grouped GEMM tiles
 };
 
 namespace {
@@ -116,8 +117,9 @@ int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax,
                      const std::vector<std::vector<int>>& segs) {
   if (!h->gplan) h->gplan = new GroupPlan();
   GroupPlan& P = *h->gplan;
+  const int tbm = h->group_tbm;
   std::vector<unsigned long long> key = {(unsigned long long)nk, (unsigned long long)nmax,
-                                         (unsigned long long)h->prec,
+                                         (unsigned long long)h->prec, (unsigned long long)tbm,
                                          (unsigned long long)(uintptr_t)h->kinfo};
   for (int k = 0; k < nk; ++k) key.push_back((unsigned long long)nmatp[k]);
   for (const std::vector<int>& ks : segs) {
@@ -144,6 +146,7 @@ int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax,
   P.key.swap(key);
   P.nk = nk;
   P.nmax = nmax;
+  P.tbm = tbm;
   P.ops.clear();
   P.seg_begin.clear();
   P.zero_k.clear();
@@ -193,7 +196,7 @@ int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax,
         cplx* panel = Os(k) + kb + ld * (kb + b);
         zgemm_group_add(gemm(b, rest, b, one, Us(k) + kb + ld * kb, ld, panel, ld, zero, panel, ld, TRI_NONE,
                              TRI_LOWER, TRI_NONE),
-                        probs, tiles);
+                        probs, tiles, tbm);
       }
       gemm_op(OP_C, OP_N, t0);
       t0 = tiles.size();
@@ -206,7 +209,7 @@ int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax,
         const cplx* panel = Os(k) + kb + ld * (kb + b);
         zgemm_group_add(gemm(rest, rest, b, mone, panel, ld, panel, ld, one, Os(k) + (kb + b) * (ld + 1), ld,
                              TRI_UPPER),
-                        probs, tiles);
+                        probs, tiles, tbm);
       }
       gemm_op(OP_C, OP_N, t0);
     }
@@ -228,11 +231,11 @@ int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax,
             if (half == 0)  // T = U12 X22
               zgemm_group_add(gemm(bs, bs, bs, one, U + ld * bs + q * step, ld, Ui + bs * (ld + 1) + q * step, ld,
                                    zero, T + (size_t)q * bs * bs, bs, TRI_NONE, TRI_NONE, TRI_UPPER),
-                              probs, tiles);
+                              probs, tiles, tbm);
             else  // X12 = -X11 T
               zgemm_group_add(gemm(bs, bs, bs, mone, Ui + q * step, ld, T + (size_t)q * bs * bs, bs, zero,
                                    Ui + ld * bs + q * step, ld, TRI_NONE, TRI_UPPER, TRI_NONE),
-                              probs, tiles);
+                              probs, tiles, tbm);
           }
           if (rem > bs) {  // a trailing pair whose second block is shorter
             const int a0 = nfull * 2 * bs, d0 = a0 + bs, sd = n - d0;
@@ -240,11 +243,11 @@ int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax,
             if (half == 0)
               zgemm_group_add(gemm(bs, sd, sd, one, U + a0 + ld * d0, ld, Ui + d0 + ld * d0, ld, zero, Tq, bs,
                                    TRI_NONE, TRI_NONE, TRI_UPPER),
-                              probs, tiles);
+                              probs, tiles, tbm);
             else
               zgemm_group_add(gemm(bs, sd, bs, mone, Ui + a0 + ld * a0, ld, Tq, bs, zero, Ui + a0 + ld * d0, ld,
                                    TRI_NONE, TRI_UPPER, TRI_NONE),
-                              probs, tiles);
+                              probs, tiles, tbm);
           }
         }
         gemm_op(OP_N, OP_N, t0);
@@ -257,14 +260,14 @@ int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax,
     for (int k : ks) {
       const int n = nmatp[k];
       zgemm_group_add(gemm(n, n, n, one, Hs(k), n, Us(k), n, zero, Ts(k), n, TRI_NONE, TRI_NONE, TRI_UPPER), probs,
-                      tiles);
+                      tiles, tbm);
     }
     gemm_op(OP_N, OP_N, t0);
     t0 = tiles.size();
     for (int k : ks) {
       const int n = nmatp[k];
       zgemm_group_add(gemm(n, n, n, one, Us(k), n, Ts(k), n, zero, Hs(k), n, TRI_UPPER, TRI_LOWER, TRI_NONE), probs,
-                      tiles);
+                      tiles, tbm);
     }
     gemm_op(OP_C, OP_N, t0);
     const int m0 = (int)mp.size();
@@ -312,7 +315,7 @@ int group_enqueue_front(excfv_handle* h, int seg, cudaStream_t s, excfv_handle* 
         if ((rc = potrf_diag_grouped(s, P.d_potrf + op.off, op.cnt, op.kb))) return rc;
         break;
       case GroupPlan::OPK_GEMM:
-        if ((rc = zgemm_grouped(s, op.a, op.b, P.d_probs, P.d_tiles + op.off, op.cnt))) return rc;
+        if ((rc = zgemm_grouped(s, op.a, op.b, P.d_probs, P.d_tiles + op.off, op.cnt, P.tbm))) return rc;
         break;
       case GroupPlan::OPK_MIRROR:
         if ((rc = mirror_grouped(s, P.d_mirror + op.off, op.cnt, op.kb))) return rc;

@@ -185,6 +185,7 @@ struct excfv_handle {
   int batch_mode = EXCFV_BATCH_AUTO;   // whole chains on lanes, the grouped front, or auto
   int batch_form = EXCFV_BATCH_LANES;  // the form the current batch runs in
   GroupPlan* gplan = nullptr;
+  int group_tbm = 64;          // rows of the grouped front's GEMM tiles (64 or 128)
   std::vector<excfv_handle*> lanes;
   int* kinfo = nullptr;       // per-k status words of the last batch (device)
   int kinfo_cap = 0;

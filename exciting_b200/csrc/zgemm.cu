@@ -32,25 +32,37 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-typedef double SmemTile[2][2][BK][LDS];
+// Two-stage operand buffers of a TBM x 64 tile: re/im planes of A (k-major,
+// TBM rows) and of B (k-major, 64 columns).
+template <int TBM>
+struct TileSmem {
+  double A[2][2][BK][TBM + PAD];
+  double B[2][2][BK][BN + PAD];
+};
 
-// One 64 x 64 output tile (rows i0.., columns j0..) of batch entry bz and
-// split-K piece split; As / Bs are the CTA's two-stage operand buffers.
-template <int OPA, int OPB>
+// One TBM x 64 output tile (rows i0.., columns j0..) of batch entry bz and
+// split-K piece split, by 2 TBM threads: (TBM / 32) x 2 warps of 32 x 32.
+// TBM = 64 is the shape of every plain launch; the grouped launches also
+// have TBM = 128 (eight warps, half the B loads per product).
+template <int OPA, int OPB, int TBM>
 __device__ __forceinline__ void zgemm_tile(const ZgemmArgs& p, int i0, int j0, long long bz, int split,
-                                           SmemTile& As, SmemTile& Bs) {
+                                           TileSmem<TBM>& S) {
+  constexpr int TNT = 2 * TBM;            // threads
+  constexpr int BPER = BN * BK / TNT;     // B elements each thread stages
+  auto& As = S.A;
+  auto& Bs = S.B;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
   if (p.uplo_c == TRI_UPPER && i0 > j0 + BN - 1) return;
-  if (p.uplo_c == TRI_LOWER && j0 > i0 + BM - 1) return;
+  if (p.uplo_c == TRI_LOWER && j0 > i0 + TBM - 1) return;
 
   const cplx* __restrict__ A = p.A + bz * p.strideA;
   const cplx* __restrict__ B = p.B + bz * p.strideB;
   cplx* __restrict__ C = p.C + bz * p.strideC;
 
   int kbeg = 0, kend = p.k - p.kdec * (int)bz;
-  if (p.tri_a == TRI_LOWER) kend = min(kend, i0 + BM);
+  if (p.tri_a == TRI_LOWER) kend = min(kend, i0 + TBM);
   if (p.tri_a == TRI_UPPER) kbeg = max(kbeg, i0);
   if (p.tri_b == TRI_UPPER) kend = min(kend, j0 + BN);
   if (p.tri_b == TRI_LOWER) kbeg = max(kbeg, j0);
@@ -63,8 +75,8 @@ __device__ __forceinline__ void zgemm_tile(const ZgemmArgs& p, int i0, int j0, l
     kbeg = b0;
   }
 
-  const int wm = (warp & 1) * 32;
-  const int wn = (warp >> 1) * 32;
+  const int wm = (warp % (TBM / 32)) * 32;
+  const int wn = (warp / (TBM / 32)) * 32;
 
   double acc[4][4][2][2];
 #pragma unroll
@@ -74,14 +86,14 @@ __device__ __forceinline__ void zgemm_tile(const ZgemmArgs& p, int i0, int j0, l
 #pragma unroll
       for (int c = 0; c < 2; ++c) acc[a][b][c][0] = acc[a][b][c][1] = 0.0;
 
-  cplx ra[4], rb[4];
+  cplx ra[4], rb[BPER];
 
   auto load_tile = [&](int kt) {
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-      const int idx = tid + r * NT;
+      const int idx = tid + r * TNT;
       int ii, kk;
-      if (OPA == OP_N) { ii = idx & 63; kk = idx >> 6; }
+      if (OPA == OP_N) { ii = idx & (TBM - 1); kk = idx / TBM; }
       else { kk = idx & 7; ii = idx >> 3; }
       const int gi = i0 + ii, gk = kt + kk;
       bool ok = gi < p.m && gk < kend;
@@ -98,8 +110,8 @@ __device__ __forceinline__ void zgemm_tile(const ZgemmArgs& p, int i0, int j0, l
       ra[r] = v;
     }
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int idx = tid + r * NT;
+    for (int r = 0; r < BPER; ++r) {
+      const int idx = tid + r * TNT;
       int jj, kk;
       if (OPB == OP_N) { kk = idx & 7; jj = idx >> 3; }
       else { jj = idx & 63; kk = idx >> 6; }
@@ -122,16 +134,16 @@ __device__ __forceinline__ void zgemm_tile(const ZgemmArgs& p, int i0, int j0, l
   auto store_tile = [&](int st) {
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-      const int idx = tid + r * NT;
+      const int idx = tid + r * TNT;
       int ii, kk;
-      if (OPA == OP_N) { ii = idx & 63; kk = idx >> 6; }
+      if (OPA == OP_N) { ii = idx & (TBM - 1); kk = idx / TBM; }
       else { kk = idx & 7; ii = idx >> 3; }
       As[st][0][kk][ii] = ra[r].x;
       As[st][1][kk][ii] = ra[r].y;
     }
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int idx = tid + r * NT;
+    for (int r = 0; r < BPER; ++r) {
+      const int idx = tid + r * TNT;
       int jj, kk;
       if (OPB == OP_N) { kk = idx & 7; jj = idx >> 3; }
       else { jj = idx & 63; kk = idx >> 6; }
@@ -220,8 +232,7 @@ __device__ __forceinline__ void zgemm_tile(const ZgemmArgs& p, int i0, int j0, l
 
 template <int OPA, int OPB>
 __global__ void __launch_bounds__(NT) zgemm_kernel(ZgemmArgs p) {
-  __shared__ __align__(16) SmemTile As;
-  __shared__ __align__(16) SmemTile Bs;
+  __shared__ __align__(16) TileSmem<BM> S;
   // Tiles whose K range grows with the row (tri_a lower) or the column
   // (tri_b upper) index are dispatched heaviest first, so that the last wave
   // holds the short ones.
@@ -231,21 +242,21 @@ __global__ void __launch_bounds__(NT) zgemm_kernel(ZgemmArgs p) {
   const int j0 = (rev_y ? (int)(gridDim.y - 1 - blockIdx.y) : (int)blockIdx.y) * BN;
   const long long bz = (p.splitk > 1) ? blockIdx.z / p.splitk : blockIdx.z;
   const int split = (p.splitk > 1) ? (int)(blockIdx.z % p.splitk) : 0;
-  zgemm_tile<OPA, OPB>(p, i0, j0, bz, split, As, Bs);
+  zgemm_tile<OPA, OPB, BM>(p, i0, j0, bz, split, S);
 }
 
-// Grouped form: one launch over the tiles of many independent products of
-// different sizes.  tiles[b] = (problem, row tile, column tile, -) of CTA b,
+// Grouped form: one launch over the TBM x 64 tiles of many independent
+// products of different sizes.  tiles[b] = (problem, row tile, column tile, -) of CTA b,
 // listed by the host heaviest first; probs[problem] is an unbatched product
 // (batch 1, no split-K).
-template <int OPA, int OPB>
-__global__ void __launch_bounds__(NT) zgemm_grouped_kernel(const ZgemmArgs* __restrict__ probs,
-                                                           const int4* __restrict__ tiles) {
-  __shared__ __align__(16) SmemTile As;
-  __shared__ __align__(16) SmemTile Bs;
+template <int OPA, int OPB, int TBM>
+__global__ void __launch_bounds__(2 * TBM) zgemm_grouped_kernel(const ZgemmArgs* __restrict__ probs,
+                                                                const int4* __restrict__ tiles) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  TileSmem<TBM>& S = *reinterpret_cast<TileSmem<TBM>*>(gsm);
   const int4 t = tiles[blockIdx.x];
   const ZgemmArgs p = probs[t.x];
-  zgemm_tile<OPA, OPB>(p, t.y * BM, t.z * BN, 0, 0, As, Bs);
+  zgemm_tile<OPA, OPB, TBM>(p, t.y * TBM, t.z * BN, 0, 0, S);
 }
 
 // C = alpha * sum_s P_s + beta * C over the split-K slabs (fixed order).
@@ -323,29 +334,30 @@ int zgemm(cudaStream_t s, int opA, int opB, const ZgemmArgs& a_in) {
 
 // Length of the K range tile (ti, tj) of p runs over (the same rules as
 // zgemm_tile), or -1 for a tile outside the written triangle of C.
-static long long group_tile_k(const ZgemmArgs& p, int ti, int tj) {
-  const int i0 = ti * BM, j0 = tj * BN;
+static long long group_tile_k(const ZgemmArgs& p, int ti, int tj, int tbm) {
+  const int i0 = ti * tbm, j0 = tj * BN;
   if (p.uplo_c == TRI_UPPER && i0 > j0 + BN - 1) return -1;
-  if (p.uplo_c == TRI_LOWER && j0 > i0 + BM - 1) return -1;
+  if (p.uplo_c == TRI_LOWER && j0 > i0 + tbm - 1) return -1;
   int kbeg = 0, kend = p.k;
-  if (p.tri_a == TRI_LOWER) kend = std::min(kend, i0 + BM);
+  if (p.tri_a == TRI_LOWER) kend = std::min(kend, i0 + tbm);
   if (p.tri_a == TRI_UPPER) kbeg = std::max(kbeg, i0);
   if (p.tri_b == TRI_UPPER) kend = std::min(kend, j0 + BN);
   if (p.tri_b == TRI_LOWER) kbeg = std::max(kbeg, j0);
   return std::max(0, kend - (kbeg / BK) * BK);
 }
 
-void zgemm_group_add(const ZgemmArgs& p_in, std::vector<ZgemmArgs>& probs, std::vector<GroupTile>& tiles) {
+void zgemm_group_add(const ZgemmArgs& p_in, std::vector<ZgemmArgs>& probs, std::vector<GroupTile>& tiles,
+                     int tbm) {
   ZgemmArgs p = p_in;
   if (p.m <= 0 || p.n <= 0) return;
   p.batch = 1; p.splitk = 1; p.part = nullptr; p.kdec = 0;
   p.strideA = p.strideB = p.strideC = 0;
   const int pi = (int)probs.size();
   probs.push_back(p);
-  const int tm = (p.m + BM - 1) / BM, tn = (p.n + BN - 1) / BN;
+  const int tm = (p.m + tbm - 1) / tbm, tn = (p.n + BN - 1) / BN;
   for (int tj = 0; tj < tn; ++tj)
     for (int ti = 0; ti < tm; ++ti) {
-      const long long kl = group_tile_k(p, ti, tj);
+      const long long kl = group_tile_k(p, ti, tj, tbm);
       if (kl >= 0) tiles.push_back(GroupTile{pi, ti, tj, kl});
     }
 }
@@ -355,13 +367,18 @@ void zgemm_group_order(std::vector<GroupTile>& tiles, size_t from) {
                    [](const GroupTile& a, const GroupTile& b) { return a.klen > b.klen; });
 }
 
-int zgemm_grouped(cudaStream_t s, int opA, int opB, const ZgemmArgs* d_probs, const int4* d_tiles, int ntiles) {
-  if (ntiles <= 0) return 0;
+template <int TBM>
+static int launch_grouped(cudaStream_t s, int opA, int opB, const ZgemmArgs* d_probs, const int4* d_tiles,
+                          int ntiles) {
+  const int smem = (int)sizeof(TileSmem<TBM>);
   switch (opA * 3 + opB) {
-#define EXCFV_GROUPED_CASE(A_, B_)                                                     \
-  case A_ * 3 + B_:                                                                    \
-    zgemm_grouped_kernel<A_, B_><<<ntiles, NT, 0, s>>>(d_probs, d_tiles);             \
-    count_launch();                                                                    \
+#define EXCFV_GROUPED_CASE(A_, B_)                                                               \
+  case A_ * 3 + B_:                                                                              \
+    if (cudaFuncSetAttribute(zgemm_grouped_kernel<A_, B_, TBM>,                                  \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)  \
+      return EXCFV_ERR_CUDA;                                                                     \
+    zgemm_grouped_kernel<A_, B_, TBM><<<ntiles, 2 * TBM, smem, s>>>(d_probs, d_tiles);          \
+    count_launch();                                                                              \
     return cudaGetLastError() == cudaSuccess ? 0 : EXCFV_ERR_CUDA;
     EXCFV_GROUPED_CASE(OP_N, OP_N)
     EXCFV_GROUPED_CASE(OP_N, OP_C)
@@ -369,6 +386,14 @@ int zgemm_grouped(cudaStream_t s, int opA, int opB, const ZgemmArgs* d_probs, co
     EXCFV_GROUPED_CASE(OP_C, OP_C)
 #undef EXCFV_GROUPED_CASE
   }
+  return EXCFV_ERR_ARG;
+}
+
+int zgemm_grouped(cudaStream_t s, int opA, int opB, const ZgemmArgs* d_probs, const int4* d_tiles, int ntiles,
+                  int tbm) {
+  if (ntiles <= 0) return 0;
+  if (tbm == 128) return launch_grouped<128>(s, opA, opB, d_probs, d_tiles, ntiles);
+  if (tbm == 64) return launch_grouped<64>(s, opA, opB, d_probs, d_tiles, ntiles);
   return EXCFV_ERR_ARG;
 }
 

@@ -504,6 +504,13 @@ class FirstVariational:
         """Launches of the grouped front of the last grouped batch."""
         return int(self._L.excfv_group_launches(self._h))
 
+    def set_group_tile(self, rows: int) -> None:
+        """Rows of the grouped front's GEMM tiles (64 or 128)."""
+        self._check(self._L.excfv_set_group_tile(self._h, rows), "excfv_set_group_tile")
+
+    def group_tile(self) -> int:
+        return int(self._L.excfv_get_group_tile(self._h))
+
     def set_lanes(self, nlanes: int) -> None:
         self._check(self._L.excfv_set_lanes(self._h, nlanes), "excfv_set_lanes")
 

@@ -169,6 +169,8 @@ SIGNATURES = {
     "excfv_set_batch_mode": (C.c_int, [C.c_void_p, C.c_int32]),
     "excfv_get_batch_mode": (C.c_int, [C.c_void_p]),
     "excfv_group_launches": (C.c_longlong, [C.c_void_p]),
+    "excfv_set_group_tile": (C.c_int, [C.c_void_p, C.c_int32]),
+    "excfv_get_group_tile": (C.c_int, [C.c_void_p]),
     "excfv_get_lanes": (C.c_int, [C.c_void_p]),
     "excfv_autotune_lanes": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

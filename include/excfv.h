@@ -473,12 +473,17 @@ int excfv_set_batch_mode(excfv_handle* h, int32_t mode);
 int excfv_get_batch_mode(excfv_handle* h);
 /* Launches of the grouped front of the last grouped batch (0 if none). */
 long long excfv_group_launches(excfv_handle* h);
+/* Tile shape of the grouped front's GEMMs: 64 (64 x 64 tiles, 128 threads,
+ * the default) or 128 (128 x 64 tiles, 256 threads). */
+int excfv_set_group_tile(excfv_handle* h, int32_t rows);
+int excfv_get_group_tile(excfv_handle* h);
 /* Lane count for the batched calls (0 = heuristic default). */
 int excfv_set_lanes(excfv_handle* h, int32_t nlanes);
 int excfv_get_lanes(excfv_handle* h);
 /* The project's autotuner: times the batch in every form (EXCFV_BATCH_LANES,
- * EXCFV_BATCH_GROUPED, EXCFV_BATCH_GROUPED_LANES) with 1, 2, 4, ... lanes and
- * keeps the fastest form and lane count (device pointers, same arguments as
+ * EXCFV_BATCH_GROUPED, EXCFV_BATCH_GROUPED_LANES) with 1, 2, 4, ... lanes, then
+ * a winning grouped form with the other GEMM tile shape, and keeps the fastest
+ * form, lane count and tile shape (device pointers, same arguments as
  * excfv_seceqn_batched_dev). */
 int excfv_autotune_lanes(excfv_handle* h, int32_t nk, const int32_t* nmatp, const int32_t* ngp,
                          int32_t ngkmax, const double* const* gpc, const double* const* tpgpc,

@@ -54,6 +54,14 @@ def test_grouped_host_buffers(batch_problem):
                 assert np.all(info == 0)
                 _check(refs, p.kpts, outs, 1e-10, 1e-13, 1e-11)
             assert fv.group_launches() > 0
+        # the other tile shape of the grouped GEMMs (128 x 64)
+        fv.set_batch_mode(EXCFV_BATCH_GROUPED)
+        fv.set_group_tile(128)
+        assert fv.group_tile() == 128
+        fv.set_lanes(2)
+        outs, info = fv.seceqn_batched(p.kpts, p.nmatmax)
+        assert np.all(info == 0)
+        _check(refs, p.kpts, outs, 1e-10, 1e-13, 1e-11)
 
 
 def _dev(a, dtype):
