@@ -1297,7 +1297,14 @@ static int run_batch(excfv_handle* h, const BatchArgs& b, int L) {
   if (h->batch_form == EXCFV_BATCH_GROUPED || h->batch_form == EXCFV_BATCH_GROUPED_LANES) {
     std::vector<std::vector<int>> segs;
     group_segments(h, b, L, segs);
-    if ((rc = group_plan_front(h, b.nk, b.nmatp, nmax, segs))) return rc;
+    bool rebuilt = false;
+    if ((rc = group_plan_front(h, b.nk, b.nmatp, nmax, segs, &rebuilt))) return rc;
+    // the plan's descriptors (and buffers) changed: no graph of an older plan may replay
+    if (rebuilt) {
+      drop_graph(h);
+      h->gkey.clear();
+      h->gseen = 0;
+    }
   }
   if (!b.host && h->graph_on && !h->prof.on) return run_batch_graph(h, b, L);
   return enqueue_batch(h, b, L);
@@ -1580,6 +1587,7 @@ static std::vector<unsigned long long> batch_key(const excfv_handle* h, const Ba
   std::vector<unsigned long long> k = {(unsigned long long)b.nk, (unsigned long long)L,
                                        (unsigned long long)h->prec, h->static_gen,
                                        (unsigned long long)h->batch_form,
+                                       (unsigned long long)h->group_tbm,
                                        (unsigned long long)b.nmatmax, (unsigned long long)b.ngkmax,
                                        (unsigned long long)(uintptr_t)h->stream};
   for (int i = 0; i < b.nk; ++i) {

@@ -112,9 +112,11 @@ bool group_slots_hold(const excfv_handle* h, int nk, int nmax) {
 // one op sequence per segment (a list of k-points grouped together).
 // Allocates the slots and descriptors and uploads them; when the plan
 // changes, the handle's stream is synchronised first (a previous batch may
-// still read the old descriptors).  Must not run inside a stream capture.
+// still read the old descriptors) and *rebuilt is set: a CUDA graph captured
+// with the old plan must not be replayed.  Must not run inside a stream capture.
 int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax,
-                     const std::vector<std::vector<int>>& segs) {
+                     const std::vector<std::vector<int>>& segs, bool* rebuilt) {
+  *rebuilt = false;
   if (!h->gplan) h->gplan = new GroupPlan();
   GroupPlan& P = *h->gplan;
   const int tbm = h->group_tbm;
@@ -129,6 +131,7 @@ int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax,
   const size_t S = (size_t)nmax * nmax;
   const bool slots_ok = P.slot[0] && P.slot_elems == S && P.slot_k >= nk;
   if (slots_ok && key == P.key) return EXCFV_OK;
+  *rebuilt = true;
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   int rc;
   if (!slots_ok) {

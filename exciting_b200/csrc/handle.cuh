@@ -323,7 +323,7 @@ int mirror_grouped(cudaStream_t s, const MirrorProb* d_probs, int nprob, int nma
 // (segments: lists of k-points whose fronts are grouped together, each
 // enqueued on its own stream; stage events go to the profile of handle ph)
 int group_plan_front(excfv_handle* h, int nk, const int32_t* nmatp, int nmax,
-                     const std::vector<std::vector<int>>& segs);
+                     const std::vector<std::vector<int>>& segs, bool* rebuilt);
 int group_enqueue_front(excfv_handle* h, int seg, cudaStream_t s, excfv_handle* ph);
 cplx* group_slot(excfv_handle* h, int which, int k);
 long long group_front_launches(const excfv_handle* h);
