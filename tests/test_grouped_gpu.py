@@ -70,8 +70,8 @@ def _dev(a, dtype):
 
 @pytest.mark.parametrize("prec", [0, EXCFV_PREC_MIXED])
 def test_grouped_device_pointers_graph_replay(batch_problem, prec):
-    """Eager run, graph capture, replay: every run against the oracle; the
-    lanes form on the same handle afterwards still agrees."""
+    """Eager run, graph capture, replay in each form and tile shape: every run
+    against the oracle."""
     p, refs = batch_problem
     st = p.static
     etol, rtol, otol = (1e-10, 1e-13, 1e-11) if prec == 0 else (1e-8, 1e-7, 1e-9)
@@ -89,8 +89,11 @@ def test_grouped_device_pointers_graph_replay(batch_problem, prec):
                 [e.data_ptr() for e in ev], [x.data_ptr() for x in X])
         torch.cuda.synchronize()
         fv.set_lanes(2)
-        for mode in (EXCFV_BATCH_GROUPED, EXCFV_BATCH_GROUPED_LANES, EXCFV_BATCH_LANES):
+        # (a change of tile shape after a capture must not replay the old graph)
+        for mode, tile in ((EXCFV_BATCH_GROUPED, 64), (EXCFV_BATCH_GROUPED, 128),
+                           (EXCFV_BATCH_GROUPED_LANES, 64), (EXCFV_BATCH_LANES, 64)):
             fv.set_batch_mode(mode)
+            fv.set_group_tile(tile)
             for _ in range(3):
                 for e in ev:
                     e.zero_()
