@@ -170,9 +170,12 @@ int potrf_upper(excfv_handle* h, int n, cplx* O, cplx* Ui, long long ld) {
     int rc = zgemm1(s, OP_C, OP_N, b, rest, b, one, Ui + kb + ld * kb, ld, panel, ld,
                     cmk(0.0, 0.0), panel, ld, TRI_NONE, TRI_LOWER, TRI_NONE);
     if (rc) return rc;
-    // A(rest, rest) -= U(kb, rest)^H U(kb, rest), upper triangle
-    rc = zgemm1(s, OP_C, OP_N, rest, rest, b, mone, panel, ld, panel, ld, one,
-                O + (kb + b) + ld * (kb + b), ld, TRI_UPPER);
+    // A(rest, rest) -= U(kb, rest)^H U(kb, rest), upper triangle: an A^H B
+    // product with K = 64 whose operand tiles a TMA ring brings three stages
+    // ahead (zgemm_tma.cu), so the K loop is not bound by load latency
+    const cplx* Pp[1] = {panel};
+    cplx* Cp[1] = {O + (kb + b) + ld * (kb + b)};
+    rc = zgemm_cn_tma(h, rest, rest, b, mone, Pp, ld, Pp, ld, one, Cp, ld, 1, TRI_UPPER);
     if (rc) return rc;
   }
   return EXCFV_OK;
