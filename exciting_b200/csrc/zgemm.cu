@@ -2,17 +2,21 @@
 //
 // C = alpha * op(A) * op(B) + beta * C, column-major, op in {N, C, T},
 // strided batch over blockIdx.z, optional triangular structure (see
-// ZgemmArgs).  This is the workhorse of the plain-FP64 form: the muffin-tin
-// contractions A^H (aa A) / A^H A, the Cholesky trailing updates, the
-// triangular inverse, the two-sided reduction U^-H H U^-1, the her2k update
-// of the tridiagonal reduction and the eigenvector back-transforms.
+// ZgemmArgs).  This is the workhorse of the plain-FP64 form: Z = aa A, the
+// Cholesky row panels, the triangular inverse, the two-sided reduction
+// U^-H H U^-1, the her2k update of the tridiagonal reduction and the
+// eigenvector back-transforms (the A^H B products with long K — the setup
+// contractions and the Cholesky trailing updates — have their TMA-fed
+// kernel in zgemm_tma.cu).  Its grouped form runs many products of
+// different sizes in one launch from a device tile list.
 //
 // tcgen05 has no FP64 kind, so the FP64 tensor instruction on sm_100a is
 // DMMA.  A complex product is four real DMMAs on split re/im planes:
 //   Cre += Are*Bre + Aim*(-Bim),  Cim += Are*Bim + Aim*Bre.
 //
 // Tiling: 64x64 complex outputs per CTA, 4 warps (2x2), 32x32 per warp =
-// 4x4 m8n8 tiles x {re, im}; k-tile 8 complex, two shared-memory stages
+// 4x4 m8n8 tiles x {re, im} (the grouped form also has 128x64 tiles, 4x2
+// warps); k-tile 8 complex, two shared-memory stages
 // with register-staged global loads (loads of tile t+1 overlap the DMMAs of
 // tile t).  Shared rows are padded by 4 doubles so that fragment loads
 // (lane%4 -> k row, lane/4 -> column) are bank-conflict free.
